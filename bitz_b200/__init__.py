@@ -1,0 +1,151 @@
+"""bitz_b200: a B200-native BitZ SHA-256 prover.
+
+Python mirror of the reference's prover-side interfaces over the C ABI of
+libbitz_b200.so. Field elements are numpy uint64 arrays of shape (..., 2)
+holding (lo, hi) in the reference's GF(2^128) basis.
+
+- ``build_prover`` / ``ProverState``: crates/transcript/src/domain.rs:13,
+  crates/transcript/src/prover.rs:10-84.
+- ``post_gkr_prove``: crates/post_gkr/src/lib.rs:85 (post_gkr::prove).
+- ``gkr_prove``: crates/gkr/src/lib.rs:24,785 (grand_product + gpgkr_prove).
+"""
+import ctypes
+
+import numpy as np
+
+from . import _lib
+
+__all__ = ["BitzError", "ProverState", "build_prover", "post_gkr_prove", "gkr_prove",
+           "gkr_outputs", "device_count"]
+
+_ERRORS = {
+    1: "ArgumentError", 2: "ClaimDoesNotHold", 3: "Unsatisfied", 4: "Configuration",
+    5: "CudaError", 6: "Internal", 7: "Scratch", 8: "VerifyError", 9: "MalformedProof",
+    10: "NoDevice",
+}
+
+
+class BitzError(RuntimeError):
+    """A non-zero status from the C ABI; ``code`` names the reference error variant."""
+
+    def __init__(self, status, message):
+        self.status = status
+        self.code = _ERRORS.get(status, f"status{status}")
+        super().__init__(f"{self.code}: {message}")
+
+
+def _check(status):
+    if status != 0:
+        msg = _lib.load().bitz_last_error()
+        raise BitzError(status, msg.decode() if msg else "")
+
+
+def _u64(a):
+    a = np.ascontiguousarray(a, dtype=np.uint64)
+    return a, a.ctypes.data_as(ctypes.POINTER(ctypes.c_uint64))
+
+
+def device_count():
+    return _lib.load().bitz_device_count()
+
+
+class ProverState:
+    """The prover transcript (crates/transcript/src/prover.rs:10)."""
+
+    def __init__(self, session: bytes, instance: bytes):
+        lib = _lib.load()
+        self._lib = lib
+        self._h = lib.bitz_transcript_new(session, len(session), instance, len(instance))
+        if not self._h:
+            raise BitzError(6, "transcript allocation failed")
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h:
+            self._lib.bitz_transcript_free(h)
+            self._h = None
+
+    @property
+    def handle(self):
+        return self._h
+
+    def public_message(self, data: bytes):
+        _check(self._lib.bitz_transcript_public(self._h, data, len(data)))
+
+    def prover_message(self, data: bytes):
+        _check(self._lib.bitz_transcript_prover(self._h, data, len(data)))
+
+    def hint(self, data: bytes):
+        _check(self._lib.bitz_transcript_hint(self._h, data, len(data)))
+
+    def verifier_message_f128(self):
+        out = np.zeros(2, dtype=np.uint64)
+        _check(self._lib.bitz_transcript_challenge_f128(
+            self._h, out.ctypes.data_as(ctypes.POINTER(ctypes.c_uint64))))
+        return out
+
+    def grind(self, label: bytes, bits: int):
+        _check(self._lib.bitz_transcript_grind(self._h, label, bits))
+
+    def squeeze_prime(self, bits: int) -> int:
+        buf = (ctypes.c_uint8 * 16)()
+        _check(self._lib.bitz_transcript_prime(self._h, bits, buf))
+        return int.from_bytes(bytes(buf), "little")
+
+    def narg(self) -> bytes:
+        n = self._lib.bitz_transcript_narg(self._h, None, 0)
+        buf = (ctypes.c_uint8 * max(n, 1))()
+        self._lib.bitz_transcript_narg(self._h, buf, n)
+        return bytes(buf)[:n]
+
+    def hints(self) -> bytes:
+        n = self._lib.bitz_transcript_hints(self._h, None, 0)
+        buf = (ctypes.c_uint8 * max(n, 1))()
+        self._lib.bitz_transcript_hints(self._h, buf, n)
+        return bytes(buf)[:n]
+
+
+def build_prover(session: bytes, instance: bytes) -> ProverState:
+    return ProverState(session, instance)
+
+
+def post_gkr_prove(rows, cols, target, packed, security_bits, transcript: ProverState):
+    """Runs the post-GKR sumcheck on the GPU; returns (point, value)."""
+    rows, rp = _u64(rows)
+    cols, cp = _u64(cols)
+    packed, pp = _u64(packed)
+    tgt, tp = _u64(target)
+    log_rows = int(rows.shape[0]).bit_length() - 1
+    log_cols = int(cols.shape[0]).bit_length() - 1
+    point = np.zeros((log_rows + log_cols, 2), dtype=np.uint64)
+    value = np.zeros(2, dtype=np.uint64)
+    _check(_lib.load().bitz_post_gkr_prove(
+        rp, log_rows, cp, log_cols, tp, pp, security_bits, transcript.handle,
+        point.ctypes.data_as(ctypes.POINTER(ctypes.c_uint64)),
+        value.ctypes.data_as(ctypes.POINTER(ctypes.c_uint64))))
+    return point, value
+
+
+def gkr_prove(row_images, columns, zeta, security_bits, transcript: ProverState):
+    """Builds the product tree and runs the seven layer sumchecks; returns (point, claim)."""
+    img, ip = _u64(row_images)
+    cols, cp = _u64(columns)
+    z, zp = _u64(zeta)
+    log_cols = int(cols.shape[0]).bit_length() - 1
+    point = np.zeros((log_cols + 7, 2), dtype=np.uint64)
+    claim = np.zeros(2, dtype=np.uint64)
+    _check(_lib.load().bitz_gkr_prove(
+        ip, cp, log_cols, zp, security_bits, transcript.handle,
+        point.ctypes.data_as(ctypes.POINTER(ctypes.c_uint64)),
+        claim.ctypes.data_as(ctypes.POINTER(ctypes.c_uint64))))
+    return point, claim
+
+
+def gkr_outputs(row_images, columns):
+    img, ip = _u64(row_images)
+    cols, cp = _u64(columns)
+    log_cols = int(cols.shape[0]).bit_length() - 1
+    out = np.zeros((1 << log_cols, 2), dtype=np.uint64)
+    _check(_lib.load().bitz_gkr_outputs(ip, cp, log_cols,
+                                        out.ctypes.data_as(ctypes.POINTER(ctypes.c_uint64))))
+    return out

@@ -1,0 +1,57 @@
+"""ctypes binding of libbitz_b200.so (the C ABI declared in include/bitz_b200.h).
+
+The library is built in-tree by ``make -C bitz_b200`` (or ``__graft_entry__.build()``).
+Loading fails loudly when it is missing: there is no fallback implementation.
+"""
+import ctypes
+import os
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libbitz_b200.so")
+
+_u64p = ctypes.POINTER(ctypes.c_uint64)
+_u8p = ctypes.POINTER(ctypes.c_uint8)
+_vp = ctypes.c_void_p
+
+# (name, restype, argtypes) for every exported entry point.
+SIGNATURES = [
+    ("bitz_last_error", ctypes.c_char_p, []),
+    ("bitz_device_count", ctypes.c_int, []),
+    ("bitz_transcript_new", _vp, [_vp, ctypes.c_size_t, _vp, ctypes.c_size_t]),
+    ("bitz_transcript_free", None, [_vp]),
+    ("bitz_transcript_public", ctypes.c_int, [_vp, _vp, ctypes.c_size_t]),
+    ("bitz_transcript_prover", ctypes.c_int, [_vp, _vp, ctypes.c_size_t]),
+    ("bitz_transcript_hint", ctypes.c_int, [_vp, _vp, ctypes.c_size_t]),
+    ("bitz_transcript_challenge_f128", ctypes.c_int, [_vp, _u64p]),
+    ("bitz_transcript_grind", ctypes.c_int, [_vp, ctypes.c_char_p, ctypes.c_uint32]),
+    ("bitz_transcript_prime", ctypes.c_int, [_vp, ctypes.c_uint32, _u8p]),
+    ("bitz_transcript_narg", ctypes.c_size_t, [_vp, _u8p, ctypes.c_size_t]),
+    ("bitz_transcript_hints", ctypes.c_size_t, [_vp, _u8p, ctypes.c_size_t]),
+    ("bitz_post_gkr_prove", ctypes.c_int,
+     [_u64p, ctypes.c_int, _u64p, ctypes.c_int, _u64p, _u64p, ctypes.c_uint32, _vp, _u64p, _u64p]),
+    ("bitz_post_gkr_prove_dev", ctypes.c_int,
+     [_vp, ctypes.c_int, _vp, ctypes.c_int, _u64p, _vp, ctypes.c_uint32, _vp, _u64p, _u64p]),
+    ("bitz_gkr_prove", ctypes.c_int,
+     [_u64p, _u64p, ctypes.c_int, _u64p, ctypes.c_uint32, _vp, _u64p, _u64p]),
+    ("bitz_gkr_prove_dev", ctypes.c_int,
+     [_vp, _vp, ctypes.c_int, _u64p, ctypes.c_uint32, _vp, _u64p, _u64p]),
+    ("bitz_gkr_outputs", ctypes.c_int, [_u64p, _u64p, ctypes.c_int, _u64p]),
+]
+
+_lib = None
+
+
+def load():
+    """Loads the library once and attaches the argument types."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise RuntimeError(
+                f"{LIB_PATH} is not built; run `make -C bitz_b200` or __graft_entry__.build()")
+        lib = ctypes.CDLL(LIB_PATH)
+        for name, res, args in SIGNATURES:
+            fn = getattr(lib, name)
+            fn.restype = res
+            fn.argtypes = args
+        _lib = lib
+    return _lib

@@ -1,0 +1,107 @@
+// Per-process device context: one stream and the scratch buffers the stage
+// kernels reuse across calls, grown on demand and kept resident in HBM.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <vector>
+
+#include "device.cuh"
+#include "eq.cuh"
+#include "gkr.hpp"
+#include "post_gkr.hpp"
+
+namespace bz {
+
+constexpr int kMaxPointGkr = 64;
+
+template <class T>
+class DeviceBuffer {
+ public:
+  DeviceBuffer() = default;
+  explicit DeviceBuffer(size_t n) { resize(n); }
+  ~DeviceBuffer() { release(); }
+  DeviceBuffer(const DeviceBuffer &) = delete;
+  DeviceBuffer &operator=(const DeviceBuffer &) = delete;
+  DeviceBuffer(DeviceBuffer &&o) noexcept : p_(o.p_), n_(o.n_) {
+    o.p_ = nullptr;
+    o.n_ = 0;
+  }
+  void resize(size_t n) {
+    if (n <= n_) return;
+    release();
+    BZ_CUDA(cudaMalloc(&p_, (n ? n : 1) * sizeof(T)));
+    n_ = n;
+  }
+  void release() {
+    if (p_) cudaFree(p_);
+    p_ = nullptr;
+    n_ = 0;
+  }
+  void upload(const T *h, size_t n, cudaStream_t s) {
+    resize(n);
+    BZ_CUDA(cudaMemcpyAsync(p_, h, n * sizeof(T), cudaMemcpyHostToDevice, s));
+  }
+  void download(T *h, size_t n, cudaStream_t s) const {
+    BZ_CUDA(cudaMemcpyAsync(h, p_, n * sizeof(T), cudaMemcpyDeviceToHost, s));
+  }
+  T *get() const { return p_; }
+  size_t size() const { return n_; }
+
+ private:
+  T *p_ = nullptr;
+  size_t n_ = 0;
+};
+
+class Context {
+ public:
+  static Context &get();
+
+  cudaStream_t stream() const { return stream_; }
+
+  PostGkrScratch &post_gkr_scratch(size_t entries) {
+    if (pg_.capacity < entries) {
+      pg_w0_.resize(entries);
+      pg_v0_.resize(entries);
+      pg_w1_.resize(entries);
+      pg_v1_.resize(entries);
+      pg_.w0 = pg_w0_.get();
+      pg_.v0 = pg_v0_.get();
+      pg_.w1 = pg_w1_.get();
+      pg_.v1 = pg_v1_.get();
+      pg_.capacity = entries;
+    }
+    return pg_;
+  }
+
+  GkrScratch &gkr_scratch(int s) {
+    size_t leaves = (size_t)128 << s;
+    if (gk_.capacity < leaves) {
+      size_t total = 0;
+      for (int j = 0; j < 8; j++) total += leaves >> j;
+      gk_layers_.resize(total);
+      size_t off = 0;
+      for (int j = 0; j < 8; j++) {
+        gk_.layer[j] = gk_layers_.get() + off;
+        off += leaves >> j;
+      }
+      gk_eq_.resize(leaves / 4);
+      gk_eq_scratch_.resize(eq_scratch_entries(6 + s));
+      gk_.eq = gk_eq_.get();
+      gk_.eq_scratch = gk_eq_scratch_.get();
+      gk_.capacity = leaves;
+    }
+    return gk_;
+  }
+
+ private:
+  Context();
+  cudaStream_t stream_ = nullptr;
+  PostGkrScratch pg_;
+  DeviceBuffer<f128> pg_w0_, pg_v0_, pg_w1_, pg_v1_;
+  DeviceBuffer<unsigned long long> acc_;
+  uint64_t *host_ = nullptr;
+  GkrScratch gk_;
+  DeviceBuffer<f128> gk_layers_, gk_eq_, gk_eq_scratch_, gk_pair_;
+};
+
+}  // namespace bz

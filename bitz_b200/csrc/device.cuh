@@ -1,0 +1,122 @@
+// Device-side helpers shared by the kernels: block reductions of GF(2^128)
+// and prime-field partial sums, launch sizing and error checks.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include <stdio.h>
+
+#include <stdexcept>
+#include <string>
+
+#include "field.cuh"
+
+namespace bz {
+
+struct CudaError : std::runtime_error {
+  explicit CudaError(const std::string &s) : std::runtime_error(s) {}
+};
+
+#define BZ_CUDA(call)                                                                          \
+  do {                                                                                         \
+    cudaError_t e_ = (call);                                                                   \
+    if (e_ != cudaSuccess)                                                                     \
+      throw ::bz::CudaError(std::string(#call) + ": " + cudaGetErrorString(e_) + " at " +     \
+                            __FILE__ + ":" + std::to_string(__LINE__));                        \
+  } while (0)
+
+#define BZ_LAUNCH_CHECK() BZ_CUDA(cudaGetLastError())
+
+constexpr int kThreads = 256;
+// 148 SMs on B200; grids are sized in multiples of the SM count and walked
+// with grid-stride loops, so one launch shape serves every table size.
+constexpr int kSMs = 148;
+
+inline int grid_for(size_t work, int per_block = kThreads, int max_blocks = kSMs * 8) {
+  size_t b = (work + per_block - 1) / per_block;
+  if (b < 1) b = 1;
+  if (b > (size_t)max_blocks) b = max_blocks;
+  return (int)b;
+}
+
+#if defined(__CUDACC__)
+// XOR-reduce `n` 64-bit words across the block and fold the block's result
+// into `acc` with atomicXor. XOR is associative and commutative, so the total
+// is the same whatever the order the blocks land in.
+template <int N>
+__device__ __forceinline__ void block_xor_atomic(uint64_t (&v)[N], unsigned long long *acc) {
+  __shared__ uint64_t sm[N][kThreads / 32];
+#pragma unroll
+  for (int k = 0; k < N; k++) {
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) v[k] ^= __shfl_xor_sync(0xffffffffu, v[k], off);
+  }
+  int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  if (lane == 0) {
+#pragma unroll
+    for (int k = 0; k < N; k++) sm[k][warp] = v[k];
+  }
+  __syncthreads();
+  if (warp == 0) {
+    int nw = blockDim.x >> 5;
+#pragma unroll
+    for (int k = 0; k < N; k++) {
+      uint64_t x = lane < nw ? sm[k][lane] : 0;
+#pragma unroll
+      for (int off = 16; off > 0; off >>= 1) x ^= __shfl_xor_sync(0xffffffffu, x, off);
+      if (lane == 0 && x) atomicXor(acc + k, (unsigned long long)x);
+    }
+  }
+}
+
+// Sum `N` prime-field values across the block (mod q) and write the block's
+// partial sums to out[blockIdx.x * N + k]; the host (or a second pass) adds
+// the per-block partials. Modular addition is exact in any order.
+template <int N>
+__device__ __forceinline__ void block_fp_sum(fp (&v)[N], const FpCtx &c, fp *out) {
+  __shared__ fp sm[N][kThreads / 32];
+#pragma unroll
+  for (int k = 0; k < N; k++) {
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) {
+      fp o;
+      o.lo = __shfl_xor_sync(0xffffffffu, v[k].lo, off);
+      o.hi = __shfl_xor_sync(0xffffffffu, v[k].hi, off);
+      v[k] = fp_add(v[k], o, c);
+    }
+  }
+  int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  if (lane == 0) {
+#pragma unroll
+    for (int k = 0; k < N; k++) sm[k][warp] = v[k];
+  }
+  __syncthreads();
+  if (warp == 0) {
+    int nw = blockDim.x >> 5;
+#pragma unroll
+    for (int k = 0; k < N; k++) {
+      fp x = lane < nw ? sm[k][lane] : fp_zero();
+#pragma unroll
+      for (int off = 16; off > 0; off >>= 1) {
+        fp o;
+        o.lo = __shfl_xor_sync(0xffffffffu, x.lo, off);
+        o.hi = __shfl_xor_sync(0xffffffffu, x.hi, off);
+        x = fp_add(x, o, c);
+      }
+      if (lane == 0) out[blockIdx.x * N + k] = x;
+    }
+  }
+}
+
+__device__ __forceinline__ f128 ld(const f128 *p) {
+  ulonglong2 v = *reinterpret_cast<const ulonglong2 *>(p);
+  return mk(v.x, v.y);
+}
+__device__ __forceinline__ void st(f128 *p, f128 v) {
+  *reinterpret_cast<ulonglong2 *>(p) = make_ulonglong2(v.lo, v.hi);
+}
+__device__ __forceinline__ int bit128(f128 e, int v) {
+  return v < 64 ? (int)((e.lo >> v) & 1) : (int)((e.hi >> (v - 64)) & 1);
+}
+#endif
+
+}  // namespace bz

@@ -1,0 +1,166 @@
+// The grand-product GKR (crates/gkr/src/lib.rs:24-81,88-240,785-897).
+//
+// Leaf (b << s) | c of the product tree is the row image b where column c has
+// bit b set, one elsewhere (crates/prover/src/reduce.rs:1-5); node k of each
+// layer multiplies nodes k and k + half of the layer below. The reference
+// keeps layers 0-2 in 16-entry lookup tables to save CPU memory traffic;
+// here every layer is a dense device table (2^(7+s) leaves at most, 512 MiB
+// at s = 18), built by one pass per layer. Round messages are exact field
+// values, so the dense sums equal the reference's bucketed ones bit for bit.
+//
+// A layer sumcheck binds its point's top coordinate first. Round i splits
+// the children into L = C[0, 2^n) and R = C[2^n, 2^(n+1)), each into halves
+// at 2^i. One launch per round binds round i+1 in place, sums the eq table
+// down to round i's (eq_i[x] = eq_{i+1}[x] + eq_{i+1}[x + 2^i], summing out
+// coordinate i), and accumulates round i's two sums from the freshly bound
+// values; 32 bytes leave the device per round.
+#include "eq.cuh"
+#include "gkr.hpp"
+
+namespace bz {
+
+__global__ void gkr_leaves(const f128 *__restrict__ cols, int s, const f128 *__restrict__ images,
+                           f128 *__restrict__ out) {
+  const size_t total = (size_t)128 << s;
+  const size_t cmask = ((size_t)1 << s) - 1;
+  for (size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x; k < total;
+       k += (size_t)gridDim.x * blockDim.x) {
+    size_t c = k & cmask;
+    int b = (int)(k >> s);
+    f128 word = ld(cols + c);
+    st(out + k, bit128(word, b) ? ld(images + b) : mk(1, 0));
+  }
+}
+
+__global__ void gkr_parent(const f128 *__restrict__ child, size_t half, f128 *__restrict__ out) {
+  for (size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x; k < half;
+       k += (size_t)gridDim.x * blockDim.x)
+    st(out + k, gmul(ld(child + k), ld(child + half + k)));
+}
+
+// Round i's sums (round_sums, lib.rs:164-216) before any bind: the top round.
+__global__ void gkr_top_sums(const f128 *__restrict__ c, size_t n_half, size_t h,
+                             const f128 *__restrict__ eq, int at_one, unsigned long long *acc) {
+  const f128 *L = c, *R = c + n_half;
+  wide sb = wzero(), si = wzero();
+  for (size_t x = blockIdx.x * (size_t)blockDim.x + threadIdx.x; x < h;
+       x += (size_t)gridDim.x * blockDim.x) {
+    f128 l0 = ld(L + x), l1 = ld(L + h + x), r0 = ld(R + x), r1 = ld(R + h + x);
+    f128 e = ld(eq + x);
+    f128 lb = at_one ? l1 : l0, rb = at_one ? r1 : r0;
+    wacc(sb, gmul_wide(gmul(e, lb), rb));
+    wacc(si, gmul_wide(gmul(e, gadd(l1, l0)), gadd(r1, r0)));
+  }
+  f128 a = greduce(sb), b = greduce(si);
+  uint64_t v[4] = {a.lo, a.hi, b.lo, b.hi};
+  block_xor_atomic<4>(v, acc);
+}
+
+// Bind round i+1 at r (halves of 2^(i+1)), derive eq_i in place, and sum
+// round i (halves of 2^i). Thread x < 2^i owns entries x and x + 2^i.
+__global__ void gkr_bind_sums(f128 *__restrict__ c, size_t n_half, size_t h, f128 r,
+                              f128 *__restrict__ eq, int at_one, unsigned long long *acc) {
+  f128 *L = c, *R = c + n_half;
+  const size_t h2 = 2 * h;
+  wide sb = wzero(), si = wzero();
+  for (size_t x = blockIdx.x * (size_t)blockDim.x + threadIdx.x; x < h;
+       x += (size_t)gridDim.x * blockDim.x) {
+    f128 a0 = ld(L + x), a1 = ld(L + x + h2), b0 = ld(L + x + h), b1 = ld(L + x + h + h2);
+    f128 l0 = gadd(a0, gmul(r, gadd(a1, a0)));
+    f128 l1 = gadd(b0, gmul(r, gadd(b1, b0)));
+    f128 c0 = ld(R + x), c1 = ld(R + x + h2), d0 = ld(R + x + h), d1 = ld(R + x + h + h2);
+    f128 r0 = gadd(c0, gmul(r, gadd(c1, c0)));
+    f128 r1 = gadd(d0, gmul(r, gadd(d1, d0)));
+    st(L + x, l0);
+    st(L + x + h, l1);
+    st(R + x, r0);
+    st(R + x + h, r1);
+    f128 e = gadd(ld(eq + x), ld(eq + x + h));
+    st(eq + x, e);
+    f128 lb = at_one ? l1 : l0, rb = at_one ? r1 : r0;
+    wacc(sb, gmul_wide(gmul(e, lb), rb));
+    wacc(si, gmul_wide(gmul(e, gadd(l1, l0)), gadd(r1, r0)));
+  }
+  f128 a = greduce(sb), b = greduce(si);
+  uint64_t v[4] = {a.lo, a.hi, b.lo, b.hi};
+  block_xor_atomic<4>(v, acc);
+}
+
+// The bind after round 0: one pair left in each half.
+__global__ void gkr_final_bind(const f128 *__restrict__ c, size_t n_half, f128 r, f128 *out) {
+  if (threadIdx.x == 0 && blockIdx.x == 0) {
+    f128 l0 = ld(c), l1 = ld(c + 1), r0 = ld(c + n_half), r1 = ld(c + n_half + 1);
+    st(out, gadd(l0, gmul(r, gadd(l1, l0))));
+    st(out + 1, gadd(r0, gmul(r, gadd(r1, r0))));
+  }
+}
+
+void gkr_build(const f128 *cols, int s, const f128 *images, GkrScratch &sc, cudaStream_t st_) {
+  size_t total = (size_t)128 << s;
+  if (sc.capacity < total) throw CudaError("gkr_build: scratch too small");
+  gkr_leaves<<<grid_for(total), kThreads, 0, st_>>>(cols, s, images, sc.layer[0]);
+  BZ_LAUNCH_CHECK();
+  size_t len = total;
+  for (int j = 0; j < 7; j++) {
+    gkr_parent<<<grid_for(len / 2), kThreads, 0, st_>>>(sc.layer[j], len / 2, sc.layer[j + 1]);
+    BZ_LAUNCH_CHECK();
+    len /= 2;
+  }
+}
+
+static f128 eq_factor(f128 r, f128 z) { return gadd(gadd(mk(1, 0), r), z); }
+
+f128 gkr_prove(int s, const f128 *zeta, uint32_t grind_bits, Transcript &ts, GkrScratch &sc,
+               cudaStream_t st_, f128 *point_out) {
+  f128 point[kMaxPoint], next[kMaxPoint];
+  for (int i = 0; i < s; i++) point[i] = zeta[i];
+  int n = s;
+  f128 claim = mk(0, 0);
+  for (int j = 6; j >= 0; j--) {
+    f128 *c = sc.layer[j];
+    size_t n_half = (size_t)1 << n;
+    int rounds = n;
+    BZ_CUDA(cudaMemsetAsync(sc.acc, 0, sizeof(unsigned long long) * 4 * (rounds + 1), st_));
+    // eq over the coordinates below the top one: 2^(n-1) entries
+    eq_table_device(point, n - 1, sc.eq, sc.eq_scratch, st_);
+    size_t h = n_half / 2;
+    gkr_top_sums<<<grid_for(h), kThreads, 0, st_>>>(c, n_half, h, sc.eq,
+                                                    gis_zero(point[n - 1]), sc.acc);
+    BZ_LAUNCH_CHECK();
+    f128 eq_bound = mk(1, 0);
+    for (int i = n - 1; i >= 0; i--) {
+      unsigned long long *acc = sc.acc + 4 * (n - 1 - i);
+      BZ_CUDA(cudaMemcpyAsync(sc.host, acc, 32, cudaMemcpyDeviceToHost, st_));
+      BZ_CUDA(cudaStreamSynchronize(st_));
+      f128 sb = mk(sc.host[0], sc.host[1]), si = mk(sc.host[2], sc.host[3]);
+      f128 msg[2] = {gmul(eq_bound, sb), gmul(eq_bound, si)};
+      ts.prover_message(msg, 32);
+      ts.grind("gkr/cubic/v1", grind_bits);
+      f128 r = ts.challenge_f128();
+      next[i] = r;
+      eq_bound = gmul(eq_bound, eq_factor(r, point[i]));
+      if (i > 0) {
+        size_t hh = (size_t)1 << (i - 1);
+        gkr_bind_sums<<<grid_for(hh), kThreads, 0, st_>>>(c, n_half, hh, r, sc.eq,
+                                                          gis_zero(point[i - 1]), acc + 4);
+        BZ_LAUNCH_CHECK();
+      } else {
+        gkr_final_bind<<<1, 32, 0, st_>>>(c, n_half, r, sc.pair);
+        BZ_LAUNCH_CHECK();
+      }
+    }
+    f128 lr[2];
+    BZ_CUDA(cudaMemcpyAsync(lr, sc.pair, 32, cudaMemcpyDeviceToHost, st_));
+    BZ_CUDA(cudaStreamSynchronize(st_));
+    ts.prover_message(lr, 32);
+    f128 t = ts.challenge_f128();
+    next[n] = t;
+    claim = gadd(lr[0], gmul(t, gadd(lr[1], lr[0])));
+    n++;
+    for (int i = 0; i < n; i++) point[i] = next[i];
+  }
+  for (int i = 0; i < n; i++) point_out[i] = point[i];
+  return claim;
+}
+
+}  // namespace bz

@@ -1,0 +1,30 @@
+// Host interface of the grand-product GKR kernels.
+#pragma once
+#include <cuda_runtime.h>
+
+#include "status.hpp"
+#include "transcript.hpp"
+
+namespace bz {
+
+struct GkrScratch {
+  size_t capacity = 0;         // leaves the layer tables can hold: 2^(7+s)
+  f128 *layer[8] = {nullptr};  // layer j holds 2^(7+s-j) nodes; layer 7 is the output
+  f128 *eq = nullptr;          // 2^(6+s-1) entries
+  f128 *eq_scratch = nullptr;
+  f128 *pair = nullptr;               // 2 entries
+  unsigned long long *acc = nullptr;  // 4 words per round
+  uint64_t *host = nullptr;           // pinned, 4 words
+};
+
+// Builds every layer from the packed columns (2^s F128, bit b of column c is
+// row b) and the 128 row images. Layer 7 holds the column products.
+void gkr_build(const f128 *cols, int s, const f128 *images, GkrScratch &sc, cudaStream_t st);
+
+// The seven layer sumchecks from the output point zeta (s coordinates) to the
+// leaves: writes 7 + s coordinates and returns the claim on the leaves. The
+// layer tables are consumed (bound in place).
+f128 gkr_prove(int s, const f128 *zeta, uint32_t grind_bits, Transcript &ts, GkrScratch &sc,
+               cudaStream_t st, f128 *point_out);
+
+}  // namespace bz

@@ -1,0 +1,228 @@
+// The post-GKR sumcheck (crates/post_gkr/src/lib.rs:121-148, sumcheck.rs:98-215):
+// from the inner-product claim <rows (x) cols, f> = target over the committed
+// bits f to an evaluation claim MLE[f](rho) = v.
+//
+// Device layout: the packed bits stay as the committed F128 words; the two
+// tables of the quadratic rounds (weights W and values V) live in two
+// ping-pong buffers of 2^(m-1) F128 each. Every round is one launch that
+// folds both tables at the previous challenge and, from the freshly folded
+// values still in registers, accumulates the next round's (a0, a2); the two
+// sums leave the device as 32 bytes. Round 1 reads the bits directly: its
+// coefficients are XOR sums of weights with no multiplication
+// (lib.rs:189-239).
+#include "device.cuh"
+#include "post_gkr.hpp"
+
+namespace bz {
+
+// Round 1 message and the claim check, one warp per packed element: lane l
+// owns bit pairs l and l + 32, so the warp reads the element's 128 row
+// weights as one contiguous 2 KiB run.
+__global__ void pg_first_message(const f128 *__restrict__ rows, int log_rows,
+                                 const f128 *__restrict__ cols, const f128 *__restrict__ packed,
+                                 size_t npacked, unsigned long long *acc) {
+  const int lane = threadIdx.x & 31;
+  const size_t warp = (blockIdx.x * (size_t)blockDim.x + threadIdx.x) >> 5;
+  const size_t nwarps = (gridDim.x * (size_t)blockDim.x) >> 5;
+  const int shift = log_rows - 7;
+  const size_t per_col_mask = ((size_t)1 << shift) - 1;
+  wide a0 = wzero(), a2 = wzero(), ws = wzero();
+  for (size_t e = warp; e < npacked; e += nwarps) {
+    f128 word = ld(packed + e);
+    const f128 *rw = rows + ((e & per_col_mask) << 7);
+    f128 s0 = mk(0, 0), s2 = mk(0, 0), sw = mk(0, 0);
+    // Branch-free: each lane's two bits become all-ones / all-zero masks.
+#pragma unroll
+    for (int h = 0; h < 2; h++) {
+      const int p = lane + 32 * h;
+      const uint64_t w = h == 0 ? word.lo : word.hi;
+      const int sh = 2 * lane;
+      const uint64_t m0 = 0 - ((w >> sh) & 1ull);
+      const uint64_t m1 = 0 - ((w >> (sh + 1)) & 1ull);
+      const f128 w0 = ld(rw + 2 * p), w1 = ld(rw + 2 * p + 1);
+      s0.lo ^= w0.lo & m0;
+      s0.hi ^= w0.hi & m0;
+      sw.lo ^= (w0.lo & m0) ^ (w1.lo & m1);
+      sw.hi ^= (w0.hi & m0) ^ (w1.hi & m1);
+      s2.lo ^= (w0.lo ^ w1.lo) & (m0 ^ m1);
+      s2.hi ^= (w0.hi ^ w1.hi) & (m0 ^ m1);
+    }
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) {
+      s0.lo ^= __shfl_xor_sync(0xffffffffu, s0.lo, off);
+      s0.hi ^= __shfl_xor_sync(0xffffffffu, s0.hi, off);
+      s2.lo ^= __shfl_xor_sync(0xffffffffu, s2.lo, off);
+      s2.hi ^= __shfl_xor_sync(0xffffffffu, s2.hi, off);
+      sw.lo ^= __shfl_xor_sync(0xffffffffu, sw.lo, off);
+      sw.hi ^= __shfl_xor_sync(0xffffffffu, sw.hi, off);
+    }
+    if (lane == 0) {
+      f128 c = ld(cols + (e >> shift));
+      wacc(a0, gmul_wide(c, s0));
+      wacc(a2, gmul_wide(c, s2));
+      wacc(ws, gmul_wide(c, sw));
+    }
+  }
+  f128 r0 = greduce(a0), r2 = greduce(a2), rw = greduce(ws);
+  uint64_t v[6] = {r0.lo, r0.hi, r2.lo, r2.hi, rw.lo, rw.hi};
+  block_xor_atomic<6>(v, acc);
+}
+
+// Round 1's fold: W'[c * R/2 + k] = cols[c] * fold(rows)[k] and V' the bound
+// bit pairs {0, 1+r, r, 1} (lib.rs:241-283), fused with round 2's sums.
+// Thread j writes the new pair (2j, 2j+1) of both tables.
+__global__ void pg_first_fold(const f128 *__restrict__ rows, int log_rows,
+                              const f128 *__restrict__ cols, const f128 *__restrict__ packed,
+                              f128 r, f128 *__restrict__ w_out, f128 *__restrict__ v_out,
+                              size_t npairs_out, unsigned long long *acc) {
+  const size_t half_rows = (size_t)1 << (log_rows - 1);
+  const f128 vals[4] = {mk(0, 0), mk(r.lo ^ 1, r.hi), r, mk(1, 0)};
+  wide a0 = wzero(), a2 = wzero();
+  for (size_t j = blockIdx.x * (size_t)blockDim.x + threadIdx.x; j < npairs_out;
+       j += (size_t)gridDim.x * blockDim.x) {
+    size_t i0 = 2 * j;
+    size_t c = i0 / half_rows, k = i0 % half_rows;
+    f128 col = ld(cols + c);
+    f128 x0 = ld(rows + 2 * k), x1 = ld(rows + 2 * k + 1);
+    f128 x2 = ld(rows + 2 * k + 2), x3 = ld(rows + 2 * k + 3);
+    f128 w0 = gmul(col, gadd(x0, gmul(r, gadd(x0, x1))));
+    f128 w1 = gmul(col, gadd(x2, gmul(r, gadd(x2, x3))));
+    f128 word = ld(packed + (i0 >> 6));
+    int p = (int)(i0 & 63);
+    int t0 = bit128(word, 2 * p) | (bit128(word, 2 * p + 1) << 1);
+    int t1 = bit128(word, 2 * p + 2) | (bit128(word, 2 * p + 3) << 1);
+    f128 v0 = vals[t0], v1 = vals[t1];
+    st(w_out + i0, w0);
+    st(w_out + i0 + 1, w1);
+    st(v_out + i0, v0);
+    st(v_out + i0 + 1, v1);
+    wacc(a0, gmul_wide(w0, v0));
+    wacc(a2, gmul_wide(gadd(w0, w1), gadd(v0, v1)));
+  }
+  f128 r0 = greduce(a0), r2 = greduce(a2);
+  uint64_t v[4] = {r0.lo, r0.hi, r2.lo, r2.hi};
+  block_xor_atomic<4>(v, acc);
+}
+
+// A quadratic round (sumcheck.rs:63-95,198-215): fold W and V at r (entry =
+// t0 + r (t0 + t1)) and accumulate the next round's (a0, a2) over the folded
+// pairs. With emit == 0 only the fold runs (the last round).
+__global__ void pg_round(const f128 *__restrict__ w_in, const f128 *__restrict__ v_in, f128 r,
+                         f128 *__restrict__ w_out, f128 *__restrict__ v_out, size_t nout,
+                         int emit, unsigned long long *acc) {
+  wide a0 = wzero(), a2 = wzero();
+  const size_t npairs = (nout + 1) / 2;
+  for (size_t j = blockIdx.x * (size_t)blockDim.x + threadIdx.x; j < npairs;
+       j += (size_t)gridDim.x * blockDim.x) {
+    size_t o = 2 * j;
+    f128 w0 = ld(w_in + 2 * o), w1 = ld(w_in + 2 * o + 1);
+    f128 v0 = ld(v_in + 2 * o), v1 = ld(v_in + 2 * o + 1);
+    f128 fw0 = gadd(w0, gmul(r, gadd(w0, w1)));
+    f128 fv0 = gadd(v0, gmul(r, gadd(v0, v1)));
+    st(w_out + o, fw0);
+    st(v_out + o, fv0);
+    if (o + 1 < nout) {
+      f128 w2 = ld(w_in + 2 * o + 2), w3 = ld(w_in + 2 * o + 3);
+      f128 v2 = ld(v_in + 2 * o + 2), v3 = ld(v_in + 2 * o + 3);
+      f128 fw1 = gadd(w2, gmul(r, gadd(w2, w3)));
+      f128 fv1 = gadd(v2, gmul(r, gadd(v2, v3)));
+      st(w_out + o + 1, fw1);
+      st(v_out + o + 1, fv1);
+      if (emit) {
+        wacc(a0, gmul_wide(fw0, fv0));
+        wacc(a2, gmul_wide(gadd(fw0, fw1), gadd(fv0, fv1)));
+      }
+    }
+  }
+  if (emit) {
+    f128 r0 = greduce(a0), r2 = greduce(a2);
+    uint64_t v[4] = {r0.lo, r0.hi, r2.lo, r2.hi};
+    block_xor_atomic<4>(v, acc);
+  }
+}
+
+// h' = p(rho) with a1 = h + a2 (lib.rs:320-323).
+static f128 advance(f128 claim, f128 a0, f128 a2, f128 r) {
+  return gadd(a0, gmul(r, gadd(gadd(claim, a2), gmul(r, a2))));
+}
+
+static void read_acc(const unsigned long long *d_acc, uint64_t *h_pinned, int words,
+                     cudaStream_t s) {
+  BZ_CUDA(cudaMemcpyAsync(h_pinned, d_acc, words * 8, cudaMemcpyDeviceToHost, s));
+  BZ_CUDA(cudaStreamSynchronize(s));
+}
+
+int post_gkr_prove(const PostGkrArgs &a, Transcript &ts, PostGkrScratch &sc, cudaStream_t s,
+                   f128 *point_out, f128 *value_out) {
+  const int log_rows = a.log_rows, log_cols = a.log_cols;
+  const size_t npacked = ((size_t)1 << (log_rows - 7)) << log_cols;
+  const int m = log_rows + log_cols;
+  const size_t n1 = (size_t)1 << (m - 1);  // table length after round 1
+  if (sc.capacity < n1) return BZ_ERR_SCRATCH;
+  unsigned long long *acc = sc.acc;
+  BZ_CUDA(cudaMemsetAsync(acc, 0, sizeof(unsigned long long) * 8 * (m + 2), s));
+
+  pg_first_message<<<grid_for(npacked * 32), kThreads, 0, s>>>(a.rows, log_rows, a.cols,
+                                                                 a.packed, npacked, acc);
+  BZ_LAUNCH_CHECK();
+  read_acc(acc, sc.host, 6, s);
+  f128 a0 = mk(sc.host[0], sc.host[1]), a2 = mk(sc.host[2], sc.host[3]);
+  f128 wsum = mk(sc.host[4], sc.host[5]);
+  if (!geq(wsum, a.target)) {
+    sc.claim_seen = wsum;
+    return BZ_ERR_CLAIM;
+  }
+
+  uint64_t msg[4] = {a0.lo, a0.hi, a2.lo, a2.hi};
+  ts.prover_message(msg, 32);
+  ts.grind("bitz/pcs/sumcheck/v1", a.grind_bits);
+  f128 r = ts.challenge_f128();
+  f128 claim = advance(a.target, a0, a2, r);
+  point_out[0] = r;
+
+  // Round 1's fold fused with round 2's message.
+  f128 *w = sc.w0, *v = sc.v0, *w2 = sc.w1, *v2 = sc.v1;
+  const int rounds = m - 1;
+  {
+    unsigned long long *acc1 = acc + 8;
+    size_t npairs = n1 / 2;
+    if (rounds >= 1) {
+      pg_first_fold<<<grid_for(npairs), kThreads, 0, s>>>(a.rows, log_rows, a.cols, a.packed, r,
+                                                          w, v, npairs, acc1);
+      BZ_LAUNCH_CHECK();
+    }
+  }
+  size_t len = n1;
+  for (int k = 0; k < rounds; k++) {
+    unsigned long long *ak = acc + 8 * (k + 1);
+    read_acc(ak, sc.host, 4, s);
+    f128 m0 = mk(sc.host[0], sc.host[1]), m2 = mk(sc.host[2], sc.host[3]);
+    uint64_t mm[4] = {m0.lo, m0.hi, m2.lo, m2.hi};
+    ts.prover_message(mm, 32);
+    ts.grind("bitz/pcs/sumcheck/v1", a.grind_bits);
+    f128 rr = ts.challenge_f128();
+    claim = advance(claim, m0, m2, rr);
+    point_out[1 + k] = rr;
+    size_t nout = len / 2;
+    int emit = nout >= 2;
+    pg_round<<<grid_for((nout + 1) / 2), kThreads, 0, s>>>(w, v, rr, w2, v2, nout, emit,
+                                                           acc + 8 * (k + 2));
+    BZ_LAUNCH_CHECK();
+    f128 *t = w;
+    w = w2;
+    w2 = t;
+    t = v;
+    v = v2;
+    v2 = t;
+    len = nout;
+  }
+  f128 fin[2];
+  BZ_CUDA(cudaMemcpyAsync(fin, w, 16, cudaMemcpyDeviceToHost, s));
+  BZ_CUDA(cudaMemcpyAsync(fin + 1, v, 16, cudaMemcpyDeviceToHost, s));
+  BZ_CUDA(cudaStreamSynchronize(s));
+  *value_out = fin[1];
+  ts.prover_f128(fin[1]);
+  return geq(gmul(fin[0], fin[1]), claim) ? BZ_OK : BZ_ERR_INTERNAL;
+}
+
+}  // namespace bz

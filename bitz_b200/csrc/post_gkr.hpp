@@ -1,0 +1,35 @@
+// Host interface of the post-GKR sumcheck kernels.
+#pragma once
+#include <cuda_runtime.h>
+
+#include "status.hpp"
+#include "transcript.hpp"
+
+namespace bz {
+
+struct PostGkrArgs {
+  const f128 *rows;  // device, 2^log_rows weights
+  int log_rows;      // t >= 7
+  const f128 *cols;  // device, 2^log_cols weights
+  int log_cols;      // s
+  const f128 *packed;  // device, 2^(t+s-7) committed words
+  f128 target;
+  uint32_t grind_bits;
+};
+
+// Device scratch, reusable across proofs: four tables of `capacity` entries,
+// a round-accumulator array and a pinned host staging buffer.
+struct PostGkrScratch {
+  size_t capacity = 0;
+  f128 *w0 = nullptr, *v0 = nullptr, *w1 = nullptr, *v1 = nullptr;
+  unsigned long long *acc = nullptr;  // 8 words per round, 64 rounds
+  uint64_t *host = nullptr;           // pinned, 8 words
+  f128 claim_seen{0, 0};              // the weighted sum found when a claim fails
+};
+
+// Runs the whole reduction: writes t+s challenges to point_out and the
+// closing evaluation to value_out, appending every message to `ts`.
+int post_gkr_prove(const PostGkrArgs &a, Transcript &ts, PostGkrScratch &sc, cudaStream_t s,
+                   f128 *point_out, f128 *value_out);
+
+}  // namespace bz

@@ -1,0 +1,145 @@
+// Host Fiat-Shamir transcript: the prover side of crates/transcript.
+//
+// Framing follows crates/transcript/src/lib.rs:7-27 (rules F1-F6): the
+// protocol id "bitz/v1", the session and the instance are absorbed as domain
+// tags at construction (domain.rs:13-26); prover messages are absorbed and
+// appended to the narg string; public messages are absorbed only; hints ride
+// in a second byte string the sponge never sees. The sponge is a
+// Keccak-f[1600] duplex with a 136-byte rate, standing in for spongefish
+// 0.7.4's std sponge (not vendored in the reference), so the byte-level sponge
+// framing is this library's own.
+#pragma once
+#include <stdint.h>
+#include <string.h>
+
+#include <string>
+#include <vector>
+
+#include "field.cuh"
+#include "hash.cuh"
+
+namespace bz {
+
+typedef unsigned __int128 u128;
+
+void keccak_f1600(uint64_t st[25]);
+
+class Transcript {
+ public:
+  static constexpr int RATE = 136;
+
+  Transcript(const uint8_t *session, size_t slen, const uint8_t *instance, size_t ilen) {
+    memset(st_, 0, sizeof st_);
+    uint8_t pid[64];
+    memset(pid, 0, sizeof pid);
+    memcpy(pid, "bitz/v1", 7);
+    absorb(pid, 64);
+    absorb_len_prefixed(session, slen);
+    absorb_len_prefixed(instance, ilen);
+  }
+
+  void public_message(const void *msg, size_t len) { absorb((const uint8_t *)msg, len); }
+  void public_u64(uint64_t v) {
+    uint8_t b[8];
+    for (int i = 0; i < 8; i++) b[i] = (uint8_t)(v >> (8 * i));
+    absorb(b, 8);
+  }
+  void public_f128(f128 v) { public_message(&v, 16); }
+
+  void prover_message(const void *msg, size_t len) {
+    absorb((const uint8_t *)msg, len);
+    const uint8_t *p = (const uint8_t *)msg;
+    narg_.insert(narg_.end(), p, p + len);
+  }
+  void prover_f128(f128 v) { prover_message(&v, 16); }
+
+  void hint(const void *msg, size_t len) {
+    const uint8_t *p = (const uint8_t *)msg;
+    hints_.insert(hints_.end(), p, p + len);
+  }
+
+  void squeeze(uint8_t *out, size_t n) {
+    for (size_t i = 0; i < n; i++) {
+      if (squeeze_pos_ == RATE) {
+        keccak_f1600(st_);
+        squeeze_pos_ = 0;
+        absorb_pos_ = 0;
+      }
+      out[i] = (uint8_t)(st_[squeeze_pos_ / 8] >> (8 * (squeeze_pos_ % 8)));
+      squeeze_pos_++;
+    }
+  }
+
+  // crates/field/src/codec.rs:24-35: 16 bytes little endian, lo then hi.
+  f128 challenge_f128() {
+    uint8_t b[16];
+    squeeze(b, 16);
+    f128 r;
+    memcpy(&r.lo, b, 8);
+    memcpy(&r.hi, b + 8, 8);
+    return r;
+  }
+  u128 challenge_u128() {
+    f128 f = challenge_f128();
+    return (u128)f.lo | ((u128)f.hi << 64);
+  }
+  // crates/transcript/src/challenge.rs:59-86: uniform residue by rejection.
+  u128 challenge_fp(u128 q) {
+    u128 maxv = ~(u128)0;
+    u128 rej = (maxv % q + 1) % q;
+    u128 max_accepted = maxv - rej;
+    for (;;) {
+      u128 c = challenge_u128();
+      if (c <= max_accepted) return c % q;
+    }
+  }
+
+  // crates/transcript/src/prover.rs:29-41, pow.rs:11-36.
+  void grind(const char *label, uint32_t bits);
+  // crates/transcript/src/challenge/prime.rs:33-61.
+  u128 prime(uint32_t bits);
+
+  const std::vector<uint8_t> &narg() const { return narg_; }
+  const std::vector<uint8_t> &hints() const { return hints_; }
+
+ private:
+  void absorb(const uint8_t *in, size_t n) {
+    for (size_t i = 0; i < n; i++) {
+      if (absorb_pos_ == RATE) {
+        keccak_f1600(st_);
+        absorb_pos_ = 0;
+      }
+      st_[absorb_pos_ / 8] ^= (uint64_t)in[i] << (8 * (absorb_pos_ % 8));
+      absorb_pos_++;
+    }
+    squeeze_pos_ = RATE;
+  }
+  void absorb_len_prefixed(const uint8_t *msg, size_t len) {
+    public_u64((uint64_t)len);
+    absorb(msg, len);
+  }
+
+  uint64_t st_[25];
+  int absorb_pos_ = 0;
+  int squeeze_pos_ = RATE;
+  std::vector<uint8_t> narg_;
+  std::vector<uint8_t> hints_;
+};
+
+// crates/transcript/src/pow.rs:38-50
+bool pow_valid(const uint8_t seed[16], uint64_t nonce, uint32_t bits);
+
+// crates/common/src/security.rs:25-31
+inline uint32_t grinding_bits(uint32_t security_bits, uint64_t coefficient) {
+  if (coefficient == 0) return 0;
+  uint32_t log_c = 0;
+  uint64_t c = coefficient - 1;
+  while (c) {
+    log_c++;
+    c >>= 1;
+  }
+  uint32_t need = security_bits + log_c;
+  return need > 128 ? need - 128 : 0;
+}
+
+}  // namespace bz

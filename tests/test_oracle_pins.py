@@ -1,0 +1,108 @@
+"""Pins the CPU oracle to answers computed outside this repository.
+
+- GF(2^128): the NIST CAVP GCM vectors the reference ships
+  (crates/field/tests/ghash_vectors.rs), via tests/golden/ghash_nist.json.
+- SHA-256 / SHA3-256 (Keccak-f): Python hashlib; FIPS 180-4 "abc".
+- BLAKE3: the published digests of "" and "abc".
+- The narg layout of the reference's golden transcript (crates/transcript/tests/golden.rs:14).
+"""
+import ctypes
+import hashlib
+import json
+import os
+
+import numpy as np
+import pytest
+
+import oracle_ffi as of
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+
+
+def _rb(b):
+    return bytes(int(f"{x:08b}"[::-1], 2) for x in b)
+
+
+def _from_nist(b):
+    b = _rb(b)
+    return np.array([int.from_bytes(b[:8], "little"), int.from_bytes(b[8:], "little")], dtype=np.uint64)
+
+
+def _to_nist(f):
+    return _rb(int(f[0]).to_bytes(8, "little") + int(f[1]).to_bytes(8, "little"))
+
+
+@pytest.mark.parametrize("mode", [0, 1])
+def test_ghash_matches_nist_gcm_vectors(mode):
+    of.lib().o_set_clmul_mode(mode)
+    fx = json.load(open(os.path.join(HERE, "golden", "ghash_nist.json")))
+    assert len(fx["cases"]) == 525
+    for i, c in enumerate(fx["cases"]):
+        h = _from_nist(bytes.fromhex(c["h"]))
+        x = np.zeros(2, dtype=np.uint64)
+
+        def absorb(data, x):
+            for k in range(0, len(data), 16):
+                y = _from_nist(data[k:k + 16].ljust(16, b"\0"))
+                x = of.gf_mul(x ^ y, h)
+            return x
+
+        aad, ct = bytes.fromhex(c["aad"]), bytes.fromhex(c["ct"])
+        x = absorb(aad, x)
+        x = absorb(ct, x)
+        lengths = (len(aad) * 8).to_bytes(8, "big") + (len(ct) * 8).to_bytes(8, "big")
+        x = of.gf_mul(x ^ _from_nist(lengths), h)
+        want = c["ghash_prefix"]
+        assert _to_nist(x)[: len(want) // 2].hex() == want, f"case {i}"
+    of.lib().o_set_clmul_mode(0)
+
+
+def test_inverse_and_reduction_boundary():
+    rng = np.random.default_rng(7)
+    one = np.array([1, 0], dtype=np.uint64)
+    for _ in range(20):
+        a = rng.integers(0, 2**64, size=2, dtype=np.uint64)
+        r = of.lib().o_gf_inv(of.F128(int(a[0]), int(a[1])))
+        assert np.array_equal(of.gf_mul(a, np.array([r.lo, r.hi], dtype=np.uint64)), one)
+    # X^127 * X = X^128 = X^7 + X^2 + X + 1 (crates/field/src/gf128.rs:453-462)
+    x127 = np.array([0, 1 << 63], dtype=np.uint64)
+    x = np.array([2, 0], dtype=np.uint64)
+    assert np.array_equal(of.gf_mul(x127, x), np.array([0x87, 0], dtype=np.uint64))
+
+
+@pytest.mark.parametrize("msg", [b"", b"abc", b"a" * 55, b"a" * 56, b"a" * 64, bytes(range(256)) * 5])
+def test_sha256_and_sha3_match_hashlib(msg):
+    buf = ctypes.create_string_buffer(32)
+    of.lib().o_sha256(msg, len(msg), buf)
+    assert buf.raw == hashlib.sha256(msg).digest()
+    of.lib().o_sha3_256(msg, len(msg), buf)
+    assert buf.raw == hashlib.sha3_256(msg).digest()
+
+
+def test_sha256_fips_abc():
+    buf = ctypes.create_string_buffer(32)
+    of.lib().o_sha256(b"abc", 3, buf)
+    # FIPS 180-4 "abc" digest (crates/circuit/src/sha256.rs:34-37)
+    assert buf.raw.hex() == "ba7816bf8f01cfea414140de5dae2223b00361a396177a9cb410ff61f20015ad"
+
+
+def test_blake3_published_digests():
+    buf = ctypes.create_string_buffer(32)
+    of.lib().o_blake3(b"", 0, buf)
+    assert buf.raw.hex() == "af1349b9f5f9a1a6a0404dea36dcc9499bcb25c9adc112b7cc9a93cae41f3262"
+    of.lib().o_blake3(b"abc", 3, buf)
+    assert buf.raw.hex() == "6437b3ac38465133ffb63b75273a8db548c558465d79db03fd359c6cd5bd9d85"
+
+
+def test_golden_transcript_narg_layout():
+    """crates/transcript/tests/golden.rs:7-38: the narg string is the F128 message
+    (16 B LE, lo then hi) then the Fq message (16 B LE canonical); the hint stays out.
+    The challenges C1/C2 depend on spongefish's byte framing, which is not in the
+    reference tree: they are parity unpinned."""
+    t = of.Transcript(b"golden-session", b"golden-instance")
+    msg = (0x0123456789ABCDEF).to_bytes(8, "little") + (0xFEDCBA9876543210).to_bytes(8, "little")
+    t.prover_message(msg)
+    t.verifier_message_f128()
+    t.prover_message((12345).to_bytes(16, "little"))
+    t.verifier_message_f128()
+    assert t.narg().hex() == "efcdab89674523011032547698badcfe39300000000000000000000000000000"

@@ -1,0 +1,56 @@
+"""The product's host transcript (libbitz_b200.so) against the oracle's, byte for byte.
+
+Runs on CPU: the transcript is host code (Fiat-Shamir stays on the host)."""
+import numpy as np
+import pytest
+
+import bitz_b200 as bz
+import oracle_ffi as of
+
+
+@pytest.mark.parametrize("seed", [0, 1, 2])
+def test_random_event_sequences_agree(seed):
+    rng = np.random.default_rng(seed)
+    p = bz.build_prover(b"bitz/circuit-e2e/v2", b"sha256-chain")
+    o = of.Transcript(b"bitz/circuit-e2e/v2", b"sha256-chain")
+    for _ in range(60):
+        kind = rng.integers(0, 4)
+        if kind == 0:
+            msg = rng.bytes(int(rng.integers(0, 400)))
+            p.public_message(msg)
+            o.public_message(msg)
+        elif kind == 1:
+            msg = rng.bytes(int(rng.integers(1, 300)))
+            p.prover_message(msg)
+            o.prover_message(msg)
+        elif kind == 2:
+            assert np.array_equal(p.verifier_message_f128(), o.verifier_message_f128())
+        else:
+            bits = int(rng.integers(0, 9))
+            p.grind(b"gkr/cubic/v1", bits)
+            o.grind(b"gkr/cubic/v1", bits)
+    assert p.narg() == o.narg()
+    assert np.array_equal(p.verifier_message_f128(), o.verifier_message_f128())
+
+
+def test_prime_sampling_agrees_and_is_prime():
+    import ctypes
+    p = bz.build_prover(b"s", b"prime")
+    o = of.Transcript(b"s", b"prime")
+    for bits in (20, 64, 121):
+        q = p.squeeze_prime(bits)
+        buf = ctypes.create_string_buffer(16)
+        of.lib().o_ts_prime_le(ctypes.c_void_p(o.h), bits, buf)
+        assert q == int.from_bytes(buf.raw, "little")
+        assert q.bit_length() == bits and q % 2 == 1
+        # Fermat check with Python big integers
+        for base in (2, 3, 5, 7, 11):
+            assert pow(base, q - 1, q) == 1
+
+
+def test_hints_bypass_the_sponge():
+    a = bz.build_prover(b"s", b"i")
+    b = bz.build_prover(b"s", b"i")
+    a.hint(b"\xaa" * 5)
+    assert np.array_equal(a.verifier_message_f128(), b.verifier_message_f128())
+    assert a.hints() == b"\xaa" * 5 and a.narg() == b""
