@@ -131,3 +131,86 @@ def weighted_sum(rows, cols, packed):
     lc = cols.shape[0].bit_length() - 1
     r = L.o_weighted_sum(p64(rows), lr, p64(cols), lc, p64(packed))
     return np.array([r.lo, r.hi], dtype=np.uint64)
+
+
+class Circuit:
+    """The oracle's replay of one SHA-256 circuit statement."""
+
+    def __init__(self, kind: int, inputs, expected):
+        L = lib()
+        L.o_circuit_build.restype = _vp
+        L.o_circuit_build.argtypes = [ctypes.c_int, _vp, ctypes.c_size_t, _vp]
+        L.o_circuit_free.argtypes = [_vp]
+        inputs = np.ascontiguousarray(inputs, dtype=np.uint8)
+        expected = np.ascontiguousarray(expected, dtype=np.uint8)
+        self.h = L.o_circuit_build(kind, inputs.ctypes.data, inputs.size, expected.ctypes.data)
+        sizes = np.zeros(7, dtype=np.uint64)
+        L.o_circuit_sizes(ctypes.c_void_p(self.h), sizes.ctypes.data_as(_u64p))
+        (self.f_len, self.h_len, self.rows, self.m_nnz, self.a_nnz, self.b_nnz,
+         self.c_nnz) = [int(x) for x in sizes]
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            lib().o_circuit_free(self.h)
+            self.h = None
+
+    def _bytes(self, fn, n, dtype=np.uint8):
+        out = np.zeros(n, dtype=dtype)
+        getattr(lib(), fn)(ctypes.c_void_p(self.h), out.ctypes.data_as(ctypes.c_void_p))
+        return out
+
+    def outputs(self):
+        return self._bytes("o_circuit_outputs", 256)
+
+    def f(self):
+        return self._bytes("o_circuit_f", self.f_len)
+
+    def hbits(self):
+        return self._bytes("o_circuit_h", self.h_len)
+
+    def products(self):
+        a = np.zeros(self.rows, dtype=np.int64)
+        b = np.zeros(self.rows, dtype=np.int64)
+        c = np.zeros(self.rows, dtype=np.int64)
+        lib().o_circuit_products(ctypes.c_void_p(self.h), a.ctypes.data_as(_vp),
+                                 b.ctypes.data_as(_vp), c.ctypes.data_as(_vp))
+        return a, b, c
+
+    def m_rows(self):
+        off = np.zeros(self.h_len + 1, dtype=np.uint32)
+        pos = np.zeros(max(self.m_nnz, 1), dtype=np.uint32)
+        lib().o_circuit_m(ctypes.c_void_p(self.h), off.ctypes.data_as(_vp), pos.ctypes.data_as(_vp))
+        return off, pos[: self.m_nnz]
+
+    def matrix(self, which):
+        nnz = [self.a_nnz, self.b_nnz, self.c_nnz][which]
+        off = np.zeros(self.rows + 1, dtype=np.uint32)
+        cols = np.zeros(max(nnz, 1), dtype=np.uint32)
+        coef = np.zeros(max(nnz, 1), dtype=np.int64)
+        lib().o_circuit_matrix(ctypes.c_void_p(self.h), which, off.ctypes.data_as(_vp),
+                               cols.ctypes.data_as(_vp), coef.ctypes.data_as(_vp))
+        return off, cols[:nnz], coef[:nnz]
+
+
+def prove(kind: int, inputs, expected, security: int):
+    """Runs the oracle's end-to-end prover; returns (status, proof bytes, times)."""
+    L = lib()
+    L.o_prover_run.restype = _vp
+    L.o_prover_run.argtypes = [ctypes.c_int, _vp, ctypes.c_size_t, _vp, ctypes.c_int,
+                               ctypes.POINTER(ctypes.c_int)]
+    L.o_prover_proof.restype = ctypes.c_size_t
+    L.o_prover_proof.argtypes = [_vp, _vp, ctypes.c_size_t]
+    L.o_prover_times.argtypes = [_vp, _vp]
+    L.o_prover_free.argtypes = [_vp]
+    inputs = np.ascontiguousarray(inputs, dtype=np.uint8)
+    expected = np.ascontiguousarray(expected, dtype=np.uint8)
+    st = ctypes.c_int(-1)
+    h = L.o_prover_run(kind, inputs.ctypes.data, inputs.size, expected.ctypes.data, security,
+                       ctypes.byref(st))
+    n = L.o_prover_proof(h, None, 0)
+    buf = ctypes.create_string_buffer(max(n, 1))
+    L.o_prover_proof(h, buf, n)
+    times = np.zeros(3, dtype=np.float64)
+    L.o_prover_times(h, times.ctypes.data)
+    L.o_prover_free(h)
+    return st.value, buf.raw[:n], times
