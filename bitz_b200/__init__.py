@@ -141,6 +141,58 @@ def gkr_prove(row_images, columns, zeta, security_bits, transcript: ProverState)
     return point, claim
 
 
+CIRCUITS = {"sha256-compression": 0, "sha256-chain": 1, "sha256-block-aligned": 2, "sha256-2kb": 3}
+
+
+class CircuitProofSystem:
+    """A prepared SHA-256 statement (tooling/cli/src/end_to_end.rs:150-336).
+
+    ``inputs`` and ``outputs`` are 0/1 sequences in the statement's bit order
+    (tooling/cli/src/circuits.rs:58-160); ``security_bits`` is 100 or 128.
+    """
+
+    def __init__(self, circuit: str, inputs, outputs, security_bits: int = 100):
+        lib = _lib.load()
+        self._lib = lib
+        self._h = None
+        inp = np.ascontiguousarray(inputs, dtype=np.uint8)
+        out = np.ascontiguousarray(outputs, dtype=np.uint8)
+        h = ctypes.c_void_p()
+        _check(lib.bitz_system_new(CIRCUITS[circuit], inp.ctypes.data, inp.size, out.ctypes.data,
+                                   security_bits, ctypes.byref(h)))
+        self._h = h
+
+    def __del__(self):
+        if getattr(self, "_h", None):
+            self._lib.bitz_system_free(self._h)
+            self._h = None
+
+    def stats(self):
+        out = np.zeros(8, dtype=np.uint64)
+        _check(self._lib.bitz_system_stats(self._h, out.ctypes.data_as(ctypes.POINTER(ctypes.c_uint64))))
+        keys = ["constraints", "assignment_bits", "committed_bits", "padded_committed_bits",
+                "prime_bits", "pcs_security", "claim_log_cols", "compressions"]
+        return dict(zip(keys, (int(x) for x in out)))
+
+    def prove(self):
+        """witness + commit + prove; returns (proof bytes, stage times in ms)."""
+        p = ctypes.POINTER(ctypes.c_uint8)()
+        n = ctypes.c_size_t(0)
+        times = (ctypes.c_double * 3)()
+        _check(self._lib.bitz_system_prove(self._h, ctypes.byref(p), ctypes.byref(n), times))
+        data = ctypes.string_at(p, n.value)
+        self._lib.bitz_free(p)
+        return data, {"witness_ms": times[0], "commit_ms": times[1], "prove_ms": times[2]}
+
+    def witness(self, f_words: int, h_words: int, rows: int):
+        f = np.zeros(f_words, dtype=np.uint32)
+        h = np.zeros(h_words, dtype=np.uint32)
+        pr = np.zeros(3 * rows, dtype=np.int64)
+        _check(self._lib.bitz_system_witness(self._h, f.ctypes.data, f.size, h.ctypes.data, h.size,
+                                             pr.ctypes.data, pr.size))
+        return f, h, pr
+
+
 def gkr_outputs(row_images, columns):
     img, ip = _u64(row_images)
     cols, cp = _u64(columns)

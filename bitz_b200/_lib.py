@@ -36,6 +36,17 @@ SIGNATURES = [
     ("bitz_gkr_prove_dev", ctypes.c_int,
      [_vp, _vp, ctypes.c_int, _u64p, ctypes.c_uint32, _vp, _u64p, _u64p]),
     ("bitz_gkr_outputs", ctypes.c_int, [_u64p, _u64p, ctypes.c_int, _u64p]),
+    ("bitz_system_new", ctypes.c_int,
+     [ctypes.c_int, _vp, ctypes.c_size_t, _vp, ctypes.c_uint32, ctypes.POINTER(_vp)]),
+    ("bitz_system_free", None, [_vp]),
+    ("bitz_system_stats", ctypes.c_int, [_vp, _u64p]),
+    ("bitz_system_prove", ctypes.c_int,
+     [_vp, ctypes.POINTER(_u8p), ctypes.POINTER(ctypes.c_size_t), ctypes.POINTER(ctypes.c_double)]),
+    ("bitz_free", None, [_vp]),
+    ("bitz_system_witness", ctypes.c_int,
+     [_vp, _vp, ctypes.c_size_t, _vp, ctypes.c_size_t, _vp, ctypes.c_size_t]),
+    ("bitz_circuit_layout", ctypes.c_int,
+     [ctypes.c_int, ctypes.c_size_t, _u64p, _u8p, _vp, _vp, _vp, _vp, _vp]),
 ]
 
 _lib = None

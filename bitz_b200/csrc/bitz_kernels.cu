@@ -1,0 +1,377 @@
+// The BitZ virtual opening's device stages and the PCS kernels.
+//
+// - Column fold (crates/common/src/fold.rs:29-63) and the comb exponentiation
+//   of the row images (fold.rs:72-104, crates/field/src/gf128/pow.rs:137-199).
+// - M^T gather (crates/circuit/src/matrix_transpose.rs:377-416).
+// - BLAKE3 derive-key digest of the inner-product weights
+//   (crates/pcs/src/opening.rs:337-368) as a chunk-parallel tree.
+// - Ring switch (crates/pcs/src/mle.rs:63-123), OOD evaluation and basis
+//   (crates/pcs/src/ood.rs:44-95).
+// - Interleaved Reed-Solomon encoding by the additive FFT, BLAKE3 Merkle tree
+//   and the Ligerito query glue (the PCS restatement; flock-core is not in
+//   the reference tree).
+#include "bitz_kernels.hpp"
+#include "device.cuh"
+#include "hash.cuh"
+
+namespace bz {
+
+// --------------------------------------------------------------- the fold
+
+__global__ void k_fold_columns(const f128 *__restrict__ cols, size_t ncols,
+                               const u128 *__restrict__ exps, u128 *__restrict__ folds) {
+  __shared__ u128 e[128];
+  for (int i = threadIdx.x; i < 128; i += blockDim.x) e[i] = exps[i];
+  __syncthreads();
+  for (size_t c = blockIdx.x * (size_t)blockDim.x + threadIdx.x; c < ncols;
+       c += (size_t)gridDim.x * blockDim.x) {
+    f128 w = ld(cols + c);
+    u128 s = 0;
+    uint64_t lo = w.lo, hi = w.hi;
+    while (lo) {
+      s += e[__ffsll((long long)lo) - 1];
+      lo &= lo - 1;
+    }
+    while (hi) {
+      s += e[64 + __ffsll((long long)hi) - 1];
+      hi &= hi - 1;
+    }
+    folds[c] = s;
+  }
+}
+
+// comb.pow(e): one multiply per non-zero 8-bit window (pow.rs:177-199)
+__global__ void k_comb_pow(const f128 *__restrict__ table, const u128 *__restrict__ exps, int n,
+                           f128 *__restrict__ out) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  u128 e = exps[i];
+  f128 acc = mk(1, 0);
+  for (int w = 0; w < 16 && e; w++, e >>= 8) {
+    int d = (int)(e & 0xff);
+    if (d) acc = gmul(acc, ld(table + w * 256 + d));
+  }
+  st(out + i, acc);
+}
+
+void fold_columns(const f128 *cols, size_t ncols, const u128 *exps, u128 *folds, cudaStream_t s) {
+  k_fold_columns<<<grid_for(ncols), kThreads, 0, s>>>(cols, ncols, exps, folds);
+  BZ_LAUNCH_CHECK();
+}
+
+void comb_pow(const f128 *table, const u128 *exps, int n, f128 *out, cudaStream_t s) {
+  k_comb_pow<<<(n + 127) / 128, 128, 0, s>>>(table, exps, n, out);
+  BZ_LAUNCH_CHECK();
+}
+
+// -------------------------------------------------------------------- M^T
+
+// w[c] = sum over the rows of column c of u1[row & 127] * u2[row >> 7]; one
+// reduction per column. Column 0 (the constant) goes to w0, the others to
+// weights[c - 1]; weights beyond the last column are zero.
+__global__ void k_mt_transpose(const uint32_t *__restrict__ off, const uint32_t *__restrict__ row,
+                               size_t ncols, const f128 *__restrict__ u1,
+                               const f128 *__restrict__ u2, f128 *__restrict__ weights,
+                               size_t padded, f128 *w0) {
+  __shared__ f128 su1[128];
+  for (int i = threadIdx.x; i < 128; i += blockDim.x) su1[i] = u1[i];
+  __syncthreads();
+  for (size_t c = blockIdx.x * (size_t)blockDim.x + threadIdx.x; c <= padded;
+       c += (size_t)gridDim.x * blockDim.x) {
+    f128 v = mk(0, 0);
+    if (c < ncols) {
+      wide acc = wzero();
+      for (uint32_t e = off[c]; e < off[c + 1]; e++) {
+        uint32_t r = row[e];
+        wacc(acc, gmul_wide(su1[r & 127], ld(u2 + (r >> 7))));
+      }
+      v = greduce(acc);
+    }
+    if (c == 0)
+      *w0 = v;
+    else
+      st(weights + (c - 1), v);
+  }
+}
+
+void mt_transpose(const uint32_t *off, const uint32_t *row, size_t ncols, const f128 *u1,
+                  const f128 *u2, f128 *weights, size_t padded, f128 *w0, cudaStream_t s) {
+  k_mt_transpose<<<grid_for(padded + 1), kThreads, 0, s>>>(off, row, ncols, u1, u2, weights,
+                                                           padded, w0);
+  BZ_LAUNCH_CHECK();
+}
+
+// ------------------------------------------------------------ BLAKE3 tree
+
+struct Key8 {
+  uint32_t k[8];
+};
+
+// Chaining value of every full 1 KiB chunk of `data` (16 blocks each).
+__global__ void k_b3_chunks(const uint8_t *__restrict__ data, size_t nchunks, Key8 key,
+                            uint32_t flags, uint32_t *__restrict__ cvs) {
+  for (size_t ch = blockIdx.x * (size_t)blockDim.x + threadIdx.x; ch < nchunks;
+       ch += (size_t)gridDim.x * blockDim.x) {
+    uint32_t cv[8];
+    for (int i = 0; i < 8; i++) cv[i] = key.k[i];
+    const uint32_t *p = reinterpret_cast<const uint32_t *>(data + ch * 1024);
+    for (int b = 0; b < 16; b++) {
+      uint32_t m[16];
+      for (int i = 0; i < 16; i++) m[i] = p[16 * b + i];
+      uint32_t fl = flags | (b == 0 ? B3_CHUNK_START : 0) | (b == 15 ? B3_CHUNK_END : 0);
+      b3_compress(cv, m, ch, 64, fl, cv);
+    }
+    for (int i = 0; i < 8; i++) cvs[8 * ch + i] = cv[i];
+  }
+}
+
+__global__ void k_b3_parents(const uint32_t *__restrict__ in, size_t nout, Key8 key,
+                             uint32_t flags, uint32_t *__restrict__ out) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < nout;
+       i += (size_t)gridDim.x * blockDim.x) {
+    uint32_t m[16], cv[8];
+    for (int j = 0; j < 16; j++) m[j] = in[16 * i + j];
+    b3_compress(key.k, m, 0, 64, flags | B3_PARENT, cv);
+    for (int j = 0; j < 8; j++) out[8 * i + j] = cv[j];
+  }
+}
+
+// The non-root chaining value of a power-of-two number of whole chunks.
+void blake3_tree_cv(const uint8_t *data, size_t nchunks, const uint32_t key[8], uint32_t flags,
+                    uint32_t *scratch, uint32_t cv_out[8], cudaStream_t s) {
+  Key8 k;
+  for (int i = 0; i < 8; i++) k.k[i] = key[i];
+  uint32_t *a = scratch, *b = scratch + 8 * nchunks;
+  k_b3_chunks<<<grid_for(nchunks), kThreads, 0, s>>>(data, nchunks, k, flags, a);
+  BZ_LAUNCH_CHECK();
+  size_t n = nchunks;
+  while (n > 1) {
+    k_b3_parents<<<grid_for(n / 2), kThreads, 0, s>>>(a, n / 2, k, flags, b);
+    BZ_LAUNCH_CHECK();
+    std::swap(a, b);
+    n /= 2;
+  }
+  BZ_CUDA(cudaMemcpyAsync(cv_out, a, 32, cudaMemcpyDeviceToHost, s));
+  BZ_CUDA(cudaStreamSynchronize(s));
+}
+
+// ----------------------------------------------------------- ring switch
+
+// claims[v] = sum over y with bit v of f[y] set of suffix[y]; block b covers
+// 64 consecutive y, thread v one bit position.
+__global__ void k_ring_claims(const f128 *__restrict__ f, const f128 *__restrict__ suffix,
+                              size_t n, unsigned long long *claims) {
+  int v = threadIdx.x;
+  uint64_t lo = 0, hi = 0;
+  for (size_t y0 = blockIdx.x * (size_t)64; y0 < n; y0 += (size_t)gridDim.x * 64) {
+    size_t y1 = y0 + 64 < n ? y0 + 64 : n;
+    for (size_t y = y0; y < y1; y++) {
+      f128 w = ld(f + y);
+      if (bit128(w, v)) {
+        f128 e = ld(suffix + y);
+        lo ^= e.lo;
+        hi ^= e.hi;
+      }
+    }
+  }
+  if (lo) atomicXor(claims + 2 * v, (unsigned long long)lo);
+  if (hi) atomicXor(claims + 2 * v + 1, (unsigned long long)hi);
+}
+
+// B(y) = sum over u with bit u of suffix[y] set of bw[u] (the packed basis of
+// the batched ring-switch claim), plus coef * eq_ood[y] when eq_ood is given.
+__global__ void k_packed_basis(const f128 *__restrict__ suffix, size_t n,
+                               const f128 *__restrict__ bw, const f128 *__restrict__ eq_ood,
+                               f128 coef, f128 *__restrict__ basis) {
+  __shared__ f128 w[128];
+  for (int i = threadIdx.x; i < 128; i += blockDim.x) w[i] = bw[i];
+  __syncthreads();
+  for (size_t y = blockIdx.x * (size_t)blockDim.x + threadIdx.x; y < n;
+       y += (size_t)gridDim.x * blockDim.x) {
+    f128 e = ld(suffix + y);
+    f128 acc = mk(0, 0);
+    uint64_t lo = e.lo, hi = e.hi;
+    while (lo) {
+      acc = gadd(acc, w[__ffsll((long long)lo) - 1]);
+      lo &= lo - 1;
+    }
+    while (hi) {
+      acc = gadd(acc, w[64 + __ffsll((long long)hi) - 1]);
+      hi &= hi - 1;
+    }
+    if (eq_ood) acc = gadd(acc, gmul(coef, ld(eq_ood + y)));
+    st(basis + y, acc);
+  }
+}
+
+// sum_y a[y] * b[y], XOR-reduced into acc[0..2).
+__global__ void k_dot(const f128 *__restrict__ a, const f128 *__restrict__ b, size_t n,
+                      unsigned long long *acc) {
+  wide s = wzero();
+  for (size_t y = blockIdx.x * (size_t)blockDim.x + threadIdx.x; y < n;
+       y += (size_t)gridDim.x * blockDim.x)
+    wacc(s, gmul_wide(ld(a + y), ld(b + y)));
+  f128 r = greduce(s);
+  uint64_t v[2] = {r.lo, r.hi};
+  block_xor_atomic<2>(v, acc);
+}
+
+__global__ void k_axpy(f128 *__restrict__ y, f128 a, const f128 *__restrict__ x, size_t n) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
+       i += (size_t)gridDim.x * blockDim.x)
+    st(y + i, gadd(ld(y + i), gmul(a, ld(x + i))));
+}
+
+void axpy(f128 *y, f128 a, const f128 *x, size_t n, cudaStream_t s) {
+  k_axpy<<<grid_for(n), kThreads, 0, s>>>(y, a, x, n);
+  BZ_LAUNCH_CHECK();
+}
+
+void ring_claims(const f128 *f, const f128 *suffix, size_t n, unsigned long long *claims,
+                 cudaStream_t s) {
+  int blocks = (int)((n + 63) / 64);
+  if (blocks > kSMs * 4) blocks = kSMs * 4;
+  k_ring_claims<<<blocks, 128, 0, s>>>(f, suffix, n, claims);
+  BZ_LAUNCH_CHECK();
+}
+
+void packed_basis(const f128 *suffix, size_t n, const f128 *bw, const f128 *eq_ood, f128 coef,
+                  f128 *basis, cudaStream_t s) {
+  k_packed_basis<<<grid_for(n), kThreads, 0, s>>>(suffix, n, bw, eq_ood, coef, basis);
+  BZ_LAUNCH_CHECK();
+}
+
+void dot(const f128 *a, const f128 *b, size_t n, unsigned long long *acc, cudaStream_t s) {
+  k_dot<<<grid_for(n), kThreads, 0, s>>>(a, b, n, acc);
+  BZ_LAUNCH_CHECK();
+}
+
+// ----------------------------------------------------- Reed-Solomon encode
+
+// Copies the message into every 2^l-row repetition of the codeword: levels
+// t >= l of the additive FFT only copy, the upper coefficients being zero.
+__global__ void k_rs_spread(const f128 *__restrict__ msg, int k, int l, int d,
+                            f128 *__restrict__ cw) {
+  size_t total = (size_t)1 << (d + k);
+  size_t mmask = ((size_t)1 << (l + k)) - 1;
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < total;
+       i += (size_t)gridDim.x * blockDim.x)
+    st(cw + i, ld(msg + (i & mmask)));
+}
+
+// One additive-FFT level t over every column: rows q and q + 2^t of a block
+// based at q0 become (u + lam w, u + (lam + 1) w), lam = Wh_t(x_q0) summed from
+// the basis table wh[t][s] = Wh_t(X^s).
+__global__ void k_rs_level(f128 *__restrict__ cw, int k, int d, int t,
+                           const f128 *__restrict__ wh) {
+  size_t pairs = (size_t)1 << (d - 1 + k);
+  size_t cmask = ((size_t)1 << k) - 1;
+  size_t half = (size_t)1 << t;
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < pairs;
+       i += (size_t)gridDim.x * blockDim.x) {
+    size_t c = i & cmask, p = i >> k;
+    size_t base = (p >> t) << (t + 1);
+    size_t j = p & (half - 1);
+    f128 lam = mk(0, 0);
+    for (int sb = t + 1; sb < d; sb++)
+      if ((base >> sb) & 1) lam = gadd(lam, wh[t * kMaxRsDim + sb]);
+    size_t iu = ((base + j) << k) + c, iw = ((base + half + j) << k) + c;
+    f128 u = ld(cw + iu), w = ld(cw + iw);
+    f128 u2 = gadd(u, gmul(lam, w));
+    st(cw + iu, u2);
+    st(cw + iw, gadd(u2, w));
+  }
+}
+
+void rs_encode(const f128 *msg, int log_n, int k, int rate, const f128 *wh, f128 *cw,
+               cudaStream_t s) {
+  int l = log_n - k, d = l + rate;
+  size_t total = (size_t)1 << (d + k);
+  k_rs_spread<<<grid_for(total), kThreads, 0, s>>>(msg, k, l, d, cw);
+  BZ_LAUNCH_CHECK();
+  for (int t = l - 1; t >= 0; t--) {
+    k_rs_level<<<grid_for(total / 2), kThreads, 0, s>>>(cw, k, d, t, wh);
+    BZ_LAUNCH_CHECK();
+  }
+}
+
+// ------------------------------------------------------------------ Merkle
+
+// Leaf i = BLAKE3 of codeword row i (2^k elements, at most 1 KiB: one chunk).
+__global__ void k_merkle_leaves(const f128 *__restrict__ cw, size_t rows, int k,
+                                uint32_t *__restrict__ nodes) {
+  const uint32_t IV[8] = {0x6A09E667, 0xBB67AE85, 0x3C6EF372, 0xA54FF53A,
+                          0x510E527F, 0x9B05688C, 0x1F83D9AB, 0x5BE0CD19};
+  int nbytes = 16 << k;
+  int nblk = (nbytes + 63) / 64;
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < rows;
+       i += (size_t)gridDim.x * blockDim.x) {
+    const uint32_t *p = reinterpret_cast<const uint32_t *>(cw + (i << k));
+    uint32_t cv[8];
+    for (int j = 0; j < 8; j++) cv[j] = IV[j];
+    for (int b = 0; b < nblk; b++) {
+      uint32_t m[16];
+      int len = nbytes - 64 * b < 64 ? nbytes - 64 * b : 64;
+      for (int j = 0; j < 16; j++) m[j] = 4 * j < len ? p[16 * b + j] : 0;
+      uint32_t fl = (b == 0 ? B3_CHUNK_START : 0) | (b == nblk - 1 ? B3_CHUNK_END | B3_ROOT : 0);
+      b3_compress(cv, m, 0, (uint32_t)len, fl, cv);
+    }
+    for (int j = 0; j < 8; j++) nodes[8 * (rows + i) + j] = cv[j];
+  }
+}
+
+// Parents lo..hi-1: node i = BLAKE3(node 2i || node 2i+1).
+__global__ void k_merkle_parents(uint32_t *nodes, size_t lo, size_t hi) {
+  const uint32_t IV[8] = {0x6A09E667, 0xBB67AE85, 0x3C6EF372, 0xA54FF53A,
+                          0x510E527F, 0x9B05688C, 0x1F83D9AB, 0x5BE0CD19};
+  for (size_t i = lo + blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < hi;
+       i += (size_t)gridDim.x * blockDim.x) {
+    uint32_t m[16], cv[8];
+    for (int j = 0; j < 16; j++) m[j] = nodes[16 * i + j];
+    b3_compress(IV, m, 0, 64, B3_CHUNK_START | B3_CHUNK_END | B3_ROOT, cv);
+    for (int j = 0; j < 8; j++) nodes[8 * i + j] = cv[j];
+  }
+}
+
+void merkle_build(const f128 *cw, size_t rows, int k, uint32_t *nodes, cudaStream_t s) {
+  k_merkle_leaves<<<grid_for(rows), kThreads, 0, s>>>(cw, rows, k, nodes);
+  BZ_LAUNCH_CHECK();
+  for (size_t lo = rows / 2; lo >= 1; lo /= 2) {
+    k_merkle_parents<<<grid_for(lo), kThreads, 0, s>>>(nodes, lo, 2 * lo);
+    BZ_LAUNCH_CHECK();
+  }
+}
+
+// ----------------------------------------------------- Ligerito query glue
+
+// basis[j] += sum_q s_q prod_{t in j} w[q][t]: block q builds its tensor table
+// in shared memory by doubling and XORs it into the basis.
+__global__ void k_query_basis(const f128 *__restrict__ w, const f128 *__restrict__ scale, int l,
+                              unsigned long long *basis) {
+  extern __shared__ f128 tab[];
+  int q = blockIdx.x;
+  if (threadIdx.x == 0) tab[0] = scale[q];
+  __syncthreads();
+  for (int t = 0; t < l; t++) {
+    int h = 1 << t;
+    f128 wt = w[q * kMaxRsDim + t];
+    for (int j = threadIdx.x; j < h; j += blockDim.x) tab[h + j] = gmul(tab[j], wt);
+    __syncthreads();
+  }
+  for (int j = threadIdx.x; j < (1 << l); j += blockDim.x) {
+    f128 v = tab[j];
+    if (v.lo) atomicXor(basis + 2 * j, (unsigned long long)v.lo);
+    if (v.hi) atomicXor(basis + 2 * j + 1, (unsigned long long)v.hi);
+  }
+}
+
+void query_basis(const f128 *w, const f128 *scale, int nq, int l, f128 *basis, cudaStream_t s) {
+  size_t smem = sizeof(f128) << l;
+  if (smem > 48 * 1024)
+    BZ_CUDA(cudaFuncSetAttribute(k_query_basis, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)smem));
+  k_query_basis<<<nq, kThreads, smem, s>>>(w, scale, l, (unsigned long long *)basis);
+  BZ_LAUNCH_CHECK();
+}
+
+}  // namespace bz

@@ -1,0 +1,39 @@
+// Host interface of the BitZ opening and PCS kernels.
+#pragma once
+#include <cuda_runtime.h>
+
+#include "transcript.hpp"
+
+namespace bz {
+
+constexpr int kMaxRsDim = 40;  // largest additive-FFT dimension (row bits of a codeword)
+
+void fold_columns(const f128 *cols, size_t ncols, const u128 *exps, u128 *folds, cudaStream_t s);
+void comb_pow(const f128 *table, const u128 *exps, int n, f128 *out, cudaStream_t s);
+void mt_transpose(const uint32_t *off, const uint32_t *row, size_t ncols, const f128 *u1,
+                  const f128 *u2, f128 *weights, size_t padded, f128 *w0, cudaStream_t s);
+void blake3_tree_cv(const uint8_t *data, size_t nchunks, const uint32_t key[8], uint32_t flags,
+                    uint32_t *scratch, uint32_t cv_out[8], cudaStream_t s);
+void ring_claims(const f128 *f, const f128 *suffix, size_t n, unsigned long long *claims,
+                 cudaStream_t s);
+void packed_basis(const f128 *suffix, size_t n, const f128 *bw, const f128 *eq_ood, f128 coef,
+                  f128 *basis, cudaStream_t s);
+// y += a * x
+void axpy(f128 *y, f128 a, const f128 *x, size_t n, cudaStream_t s);
+void dot(const f128 *a, const f128 *b, size_t n, unsigned long long *acc, cudaStream_t s);
+void rs_encode(const f128 *msg, int log_n, int k, int rate, const f128 *wh, f128 *cw,
+               cudaStream_t s);
+void merkle_build(const f128 *cw, size_t rows, int k, uint32_t *nodes, cudaStream_t s);
+void query_basis(const f128 *w, const f128 *scale, int nq, int l, f128 *basis, cudaStream_t s);
+
+// Host helpers (GF(2^128) on the CPU for the few scalar steps).
+f128 gf_inv_host(f128 a);
+// wh[t * kMaxRsDim + s] = Wh_t(X^s): the normalised subspace polynomial of
+// span(X^0..X^(t-1)) at X^s, for t, s < d.
+void subspace_table(int d, f128 *wh);
+// The comb table of `base` with 8-bit windows: 16 x 256 entries.
+void comb_table(f128 base, f128 *out);
+f128 smallest_generator_host();
+void eq_table_host(const f128 *r, int n, f128 *out);
+
+}  // namespace bz

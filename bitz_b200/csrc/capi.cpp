@@ -25,6 +25,10 @@ static int fail(int code, const std::string &msg) {
   return code;
 }
 
+namespace bz {
+int capi_fail(int code, const std::string &msg) { return fail(code, msg); }
+}  // namespace bz
+
 template <class F>
 static int guarded(F &&f) {
   try {

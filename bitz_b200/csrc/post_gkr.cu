@@ -141,6 +141,34 @@ __global__ void pg_round(const f128 *__restrict__ w_in, const f128 *__restrict__
   }
 }
 
+// (a0, a2) over the pairs of W and V as they are (no fold).
+__global__ void pg_sums(const f128 *__restrict__ w, const f128 *__restrict__ v, size_t n,
+                        unsigned long long *acc) {
+  wide a0 = wzero(), a2 = wzero();
+  for (size_t j = blockIdx.x * (size_t)blockDim.x + threadIdx.x; j < n / 2;
+       j += (size_t)gridDim.x * blockDim.x) {
+    f128 w0 = ld(w + 2 * j), w1 = ld(w + 2 * j + 1), v0 = ld(v + 2 * j), v1 = ld(v + 2 * j + 1);
+    wacc(a0, gmul_wide(w0, v0));
+    wacc(a2, gmul_wide(gadd(w0, w1), gadd(v0, v1)));
+  }
+  f128 r0 = greduce(a0), r2 = greduce(a2);
+  uint64_t o[4] = {r0.lo, r0.hi, r2.lo, r2.hi};
+  block_xor_atomic<4>(o, acc);
+}
+
+void quad_sums(const f128 *w, const f128 *v, size_t n, unsigned long long *acc, cudaStream_t s) {
+  pg_sums<<<grid_for(n / 2), kThreads, 0, s>>>(w, v, n, acc);
+  BZ_LAUNCH_CHECK();
+}
+
+void quad_fold(const f128 *w, const f128 *v, f128 r, f128 *w2, f128 *v2, size_t n, int emit,
+               unsigned long long *acc, cudaStream_t s) {
+  size_t nout = n / 2;
+  pg_round<<<grid_for((nout + 1) / 2), kThreads, 0, s>>>(w, v, r, w2, v2, nout, emit && nout >= 2,
+                                                         acc);
+  BZ_LAUNCH_CHECK();
+}
+
 // h' = p(rho) with a1 = h + a2 (lib.rs:320-323).
 static f128 advance(f128 claim, f128 a0, f128 a2, f128 r) {
   return gadd(a0, gmul(r, gadd(gadd(claim, a2), gmul(r, a2))));

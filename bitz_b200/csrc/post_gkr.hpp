@@ -27,6 +27,13 @@ struct PostGkrScratch {
   f128 claim_seen{0, 0};              // the weighted sum found when a claim fails
 };
 
+// The quadratic sumcheck round of <W, V> (shared with the Ligerito folds):
+// quad_sums accumulates (a0, a2) over the pairs as they are; quad_fold folds
+// both tables at r and, with emit, accumulates the next round's sums.
+void quad_sums(const f128 *w, const f128 *v, size_t n, unsigned long long *acc, cudaStream_t s);
+void quad_fold(const f128 *w, const f128 *v, f128 r, f128 *w2, f128 *v2, size_t n, int emit,
+               unsigned long long *acc, cudaStream_t s);
+
 // Runs the whole reduction: writes t+s challenges to point_out and the
 // closing evaluation to value_out, appending every message to `ts`.
 int post_gkr_prove(const PostGkrArgs &a, Transcript &ts, PostGkrScratch &sc, cudaStream_t s,

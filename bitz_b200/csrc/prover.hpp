@@ -1,0 +1,95 @@
+// The end-to-end prover: CircuitProofSystem's setup, witness, commit and
+// prove (tooling/cli/src/end_to_end.rs:161-336) on one device stream.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "circuit.hpp"
+#include "context.hpp"
+#include "spartan.hpp"
+#include "transcript.hpp"
+
+namespace bz {
+
+// One Ligerito level (crates/pcs/src/profiles.rs:66-126).
+struct PcsLevel {
+  int k, log_inv_rate, log_msg_cols, queries, fold_grinding, grinding, ood_samples;
+};
+
+struct PcsConfig {
+  int m = 0, log_n = 0, security = 0, nlevels = 0, final_log_n = 0;
+  PcsLevel levels[8];
+};
+
+bool pcs_config(int m, int security_bits, PcsConfig &cfg);
+
+// Device copies of one circuit's setup, shared by every statement of that
+// circuit and size.
+struct DeviceSetup {
+  std::shared_ptr<CircuitSetup> host;
+  DeviceBuffer<uint32_t> m_off, m_pos, csc_off, csc_row;
+  DeviceBuffer<uint32_t> abc_off[3], abc_col[3];
+  DeviceBuffer<int64_t> abc_coef[3];
+  // column-major copy of A, B, C for the Spartan bind
+  DeviceBuffer<uint32_t> sp_off, sp_row;
+  DeviceBuffer<uint16_t> sp_idx;
+  DeviceBuffer<int64_t> tab_vals;
+  DeviceBuffer<uint8_t> tab_which;
+  int ntab = 0;
+};
+
+struct StageTimes {
+  double witness_ms = 0, commit_ms = 0, prove_ms = 0;
+};
+
+class ProofSystem {
+ public:
+  // CircuitProofSystem::new (end_to_end.rs:161-197): one statement (its input
+  // and expected output bits, one byte each) at a PCS security level.
+  ProofSystem(int kind, const uint8_t *inputs, size_t n_inputs, const uint8_t *outputs,
+              int security_bits);
+
+  // witness + commit + prove (benchmark.rs:28-79), returning the proof bytes:
+  // root || Spartan section || bitzPCS wire container.
+  int prove(std::vector<uint8_t> &proof, StageTimes *times);
+
+  const CircuitSetup &setup() const { return *dev_->host; }
+  int security() const { return security_; }
+  std::string error;
+
+  // Witness-stage products for inspection (valid after prove()).
+  void download_witness(std::vector<uint32_t> &f, std::vector<uint32_t> &h,
+                        std::vector<int64_t> &prod);
+
+ private:
+  int witness(cudaStream_t s);
+  int commit(cudaStream_t s);
+  int prove_after_commit(cudaStream_t s, std::vector<uint8_t> &proof);
+  std::vector<uint8_t> ligerito(cudaStream_t s, f128 target);
+
+  int kind_, security_;
+  std::vector<uint8_t> inputs_, outputs_;
+  std::shared_ptr<DeviceSetup> dev_;
+  PcsConfig pcs_;
+  uint8_t matrix_digest_[32];
+  std::vector<uint8_t> public_bytes_, pcs_enc_;
+  std::vector<uint32_t> bit_rows_;  // bit constraints whose expected value is one
+  f128 generator_;
+
+  // per-proof device state
+  DeviceBuffer<uint32_t> f_, h_;
+  DeviceBuffer<int64_t> prod_;
+  DeviceBuffer<uint8_t> bit_c_;
+  DeviceBuffer<uint32_t> d_bit_rows_;
+  DeviceBuffer<f128> codeword0_;
+  DeviceBuffer<uint32_t> nodes0_;
+  std::unique_ptr<Transcript> ts_;
+  uint8_t root_[32];
+  std::vector<f128> ood_point_;
+  f128 ood_value_;
+};
+
+}  // namespace bz

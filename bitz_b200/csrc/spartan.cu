@@ -1,0 +1,400 @@
+// Spartan's outer and inner sumchecks and the matrix bind over the
+// transcript-drawn prime (crates/spartan/src/piop.rs:67-113,
+// sumcheck.rs:252-553, matrix.rs:336-467).
+//
+// Tables hold Montgomery residues. Each round is one launch that folds the
+// previous round's challenge into every table and accumulates the next
+// round's coefficients from the folded values in registers (the reference's
+// fold/round fusion, sumcheck.rs:963-1026), then one single-block launch adds
+// the per-block partial sums; 48 (outer) or 32 (inner) bytes go to the host.
+#include "device.cuh"
+#include "spartan.hpp"
+
+namespace bz {
+
+__global__ void k_fp_eq_factor(FpPoint p, int first, int n, FpCtx c, fp *out) {
+  if (threadIdx.x == 0) out[0] = c.one;
+  __syncthreads();
+  for (int i = 0; i < n; i++) {
+    fp z = p.c[first + i];
+    int half = 1 << i;
+    for (int k = threadIdx.x; k < half; k += blockDim.x) {
+      fp par = out[k];
+      fp one = fp_mul(par, z, c);
+      out[k] = fp_sub(par, one, c);
+      out[k + half] = one;
+    }
+    __syncthreads();
+  }
+}
+
+__global__ void k_fp_eq_expand(const fp *__restrict__ lo, int a, const fp *__restrict__ hi,
+                               FpCtx c, fp *__restrict__ out, size_t total) {
+  size_t mask = ((size_t)1 << a) - 1;
+  for (size_t x = blockIdx.x * (size_t)blockDim.x + threadIdx.x; x < total;
+       x += (size_t)gridDim.x * blockDim.x)
+    out[x] = fp_mul(lo[x & mask], hi[x >> a], c);
+}
+
+void fp_eq_table(const fp *point, int n, const FpCtx &c, fp *out, fp *scratch, cudaStream_t s) {
+  FpPoint p;
+  for (int i = 0; i < n; i++) p.c[i] = point[i];
+  int a = n / 2, b = n - a;
+  fp *lo = scratch, *hi = scratch + ((size_t)1 << a);
+  k_fp_eq_factor<<<1, kThreads, 0, s>>>(p, 0, a, c, lo);
+  BZ_LAUNCH_CHECK();
+  k_fp_eq_factor<<<1, kThreads, 0, s>>>(p, a, b, c, hi);
+  BZ_LAUNCH_CHECK();
+  size_t total = (size_t)1 << n;
+  k_fp_eq_expand<<<grid_for(total), kThreads, 0, s>>>(lo, a, hi, c, out, total);
+  BZ_LAUNCH_CHECK();
+}
+
+__device__ __forceinline__ fp fp_from_i64(int64_t v, const FpCtx &c) {
+  fp x;
+  if (v >= 0) {
+    x = fp{(uint64_t)v, 0};
+  } else {
+    uint64_t m = (uint64_t)(-(v + 1)) + 1;  // |v|, which is below q
+    x.lo = c.q0 - m;
+    x.hi = c.q1 - (c.q0 < m);
+  }
+  return fp_mul(x, c.r2, c);
+}
+
+// build_product_mles (matrix.rs:336-370): A h, B h, C h mod q, zero padded.
+__global__ void k_products_to_fp(const int64_t *__restrict__ prod, size_t rows, size_t padded,
+                                 FpCtx c, fp *__restrict__ A, fp *__restrict__ B,
+                                 fp *__restrict__ C) {
+  for (size_t r = blockIdx.x * (size_t)blockDim.x + threadIdx.x; r < padded;
+       r += (size_t)gridDim.x * blockDim.x) {
+    if (r < rows) {
+      A[r] = fp_from_i64(prod[r], c);
+      B[r] = fp_from_i64(prod[rows + r], c);
+      C[r] = fp_from_i64(prod[2 * rows + r], c);
+    } else {
+      A[r] = B[r] = C[r] = fp_zero();
+    }
+  }
+}
+
+__device__ __forceinline__ fp interp(fp a, fp b, fp r, const FpCtx &c) {
+  return fp_add(a, fp_mul(r, fp_sub(b, a, c), c), c);
+}
+
+// cubic_contribution (sumcheck.rs:724-746): [e0 r0, e0 rq + ed rl, ed rq]
+__device__ __forceinline__ void cubic(fp e0, fp e1, fp a0, fp a1, fp b0, fp b1, fp c0, fp c1,
+                                      const FpCtx &c, fp (&acc)[3]) {
+  fp ed = fp_sub(e1, e0, c), ad = fp_sub(a1, a0, c), bd = fp_sub(b1, b0, c), cd = fp_sub(c1, c0, c);
+  fp r0 = fp_sub(fp_mul(a0, b0, c), c0, c);
+  fp rl = fp_sub(fp_add(fp_mul(a0, bd, c), fp_mul(ad, b0, c), c), cd, c);
+  fp rq = fp_mul(ad, bd, c);
+  acc[0] = fp_add(acc[0], fp_mul(e0, r0, c), c);
+  acc[1] = fp_add(acc[1], fp_add(fp_mul(e0, rq, c), fp_mul(ed, rl, c), c), c);
+  acc[2] = fp_add(acc[2], fp_mul(ed, rq, c), c);
+}
+
+// One outer round. fold = 0: sums over the pairs of the tables as they are.
+// fold = 1: fold every table at r (output at half length) and sum over the
+// folded pairs. emit = 0 only folds (the last fold).
+__global__ void k_outer_round(const fp *E, const fp *A, const fp *B, const fp *C, fp *E2, fp *A2,
+                              fp *B2, fp *C2, size_t n, int fold, int emit, fp r, FpCtx c,
+                              fp *partial) {
+  fp acc[3] = {fp_zero(), fp_zero(), fp_zero()};
+  size_t npairs = fold ? (n / 2 + 1) / 2 : n / 2;
+  for (size_t j = blockIdx.x * (size_t)blockDim.x + threadIdx.x; j < npairs;
+       j += (size_t)gridDim.x * blockDim.x) {
+    fp e[2], a[2], b[2], cc[2];
+    if (fold) {
+      for (int t = 0; t < 2; t++) {
+        size_t o = 2 * j + t;
+        if (o >= n / 2) {
+          e[t] = a[t] = b[t] = cc[t] = fp_zero();
+          continue;
+        }
+        e[t] = interp(E[2 * o], E[2 * o + 1], r, c);
+        a[t] = interp(A[2 * o], A[2 * o + 1], r, c);
+        b[t] = interp(B[2 * o], B[2 * o + 1], r, c);
+        cc[t] = interp(C[2 * o], C[2 * o + 1], r, c);
+        E2[o] = e[t];
+        A2[o] = a[t];
+        B2[o] = b[t];
+        C2[o] = cc[t];
+      }
+    } else {
+      for (int t = 0; t < 2; t++) {
+        e[t] = E[2 * j + t];
+        a[t] = A[2 * j + t];
+        b[t] = B[2 * j + t];
+        cc[t] = C[2 * j + t];
+      }
+    }
+    if (emit) cubic(e[0], e[1], a[0], a[1], b[0], b[1], cc[0], cc[1], c, acc);
+  }
+  if (emit) block_fp_sum<3>(acc, c, partial);
+}
+
+// One inner round over D and the assignment W. W is read from the packed h
+// bits while w_bits is set (round 0, and the input of round 1's fold).
+__global__ void k_inner_round(const fp *D, const fp *W, const uint32_t *hbits, int w_bits, fp *D2,
+                              fp *W2, size_t n, int fold, int emit, fp r, FpCtx c, fp *partial) {
+  fp acc[2] = {fp_zero(), fp_zero()};
+  size_t npairs = fold ? (n / 2 + 1) / 2 : n / 2;
+  for (size_t j = blockIdx.x * (size_t)blockDim.x + threadIdx.x; j < npairs;
+       j += (size_t)gridDim.x * blockDim.x) {
+    fp d[2], w[2];
+    for (int t = 0; t < 2; t++) {
+      size_t o = 2 * j + t;
+      if (fold) {
+        if (o >= n / 2) {
+          d[t] = w[t] = fp_zero();
+          continue;
+        }
+        fp w0, w1;
+        if (w_bits) {
+          size_t i0 = 2 * o;
+          w0 = ((hbits[i0 >> 5] >> (i0 & 31)) & 1) ? c.one : fp_zero();
+          w1 = ((hbits[(i0 + 1) >> 5] >> ((i0 + 1) & 31)) & 1) ? c.one : fp_zero();
+        } else {
+          w0 = W[2 * o];
+          w1 = W[2 * o + 1];
+        }
+        d[t] = interp(D[2 * o], D[2 * o + 1], r, c);
+        w[t] = interp(w0, w1, r, c);
+        D2[o] = d[t];
+        W2[o] = w[t];
+      } else {
+        d[t] = D[o];
+        w[t] = ((hbits[o >> 5] >> (o & 31)) & 1) ? c.one : fp_zero();
+      }
+    }
+    if (emit) {
+      acc[0] = fp_add(acc[0], fp_mul(d[0], w[0], c), c);
+      acc[1] = fp_add(acc[1], fp_mul(fp_sub(d[1], d[0], c), fp_sub(w[1], w[0], c), c), c);
+    }
+  }
+  if (emit) block_fp_sum<2>(acc, c, partial);
+}
+
+template <int N>
+__global__ void k_fp_finalize(const fp *partial, int nblocks, FpCtx c, fp *out) {
+  fp acc[N];
+  for (int k = 0; k < N; k++) acc[k] = fp_zero();
+  for (int b = threadIdx.x; b < nblocks; b += blockDim.x)
+    for (int k = 0; k < N; k++) acc[k] = fp_add(acc[k], partial[b * N + k], c);
+  block_fp_sum<N>(acc, c, out);
+}
+
+// The coefficient table of the bind: scale_k * coefficient for every distinct
+// (matrix, coefficient) pair.
+__global__ void k_bind_table(const int64_t *__restrict__ vals, const uint8_t *__restrict__ which,
+                             int n, fp rho, fp rho2, FpCtx c, fp *tab) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  fp v = fp_from_i64(vals[i], c);
+  fp s = which[i] == 0 ? c.one : which[i] == 1 ? rho : rho2;
+  tab[i] = fp_mul(v, s, c);
+}
+
+// bind_and_batch (matrix.rs:429-467) as a gather over the column-major copy of
+// A, B and C: D(y) = sum over column y's entries of eq(r_x, row) * table[idx].
+__global__ void k_bind(const uint32_t *__restrict__ off, const uint32_t *__restrict__ row,
+                       const uint16_t *__restrict__ idx, const fp *__restrict__ tab,
+                       const fp *__restrict__ eq, size_t cols, size_t padded, FpCtx c, fp *D) {
+  for (size_t y = blockIdx.x * (size_t)blockDim.x + threadIdx.x; y < padded;
+       y += (size_t)gridDim.x * blockDim.x) {
+    fp acc = fp_zero();
+    if (y < cols)
+      for (uint32_t e = off[y]; e < off[y + 1]; e++) acc = fp_add(acc, fp_mul(eq[row[e]], tab[idx[e]], c), c);
+    D[y] = acc;
+  }
+}
+
+// The statement-dependent part of C: the bit constraints whose expected value
+// is one put rho^2 eq(r_x, row) on column 0.
+__global__ void k_bind_bits(const uint32_t *__restrict__ rows, int n, const fp *__restrict__ eq,
+                            fp rho2, FpCtx c, fp *D) {
+  fp acc[1] = {fp_zero()};
+  for (int i = threadIdx.x; i < n; i += blockDim.x) acc[0] = fp_add(acc[0], eq[rows[i]], c);
+  __shared__ fp out[1];
+  block_fp_sum<1>(acc, c, out);
+  __syncthreads();
+  if (threadIdx.x == 0) D[0] = fp_add(D[0], fp_mul(out[0], rho2, c), c);
+}
+
+// ------------------------------------------------------------------- host
+
+static fp host_partial_sum(const fp *d_partial, int nblocks, int N, fp *d_out, fp *h_out,
+                           const FpCtx &c, cudaStream_t s) {
+  if (N == 3)
+    k_fp_finalize<3><<<1, kThreads, 0, s>>>(d_partial, nblocks, c, d_out);
+  else
+    k_fp_finalize<2><<<1, kThreads, 0, s>>>(d_partial, nblocks, c, d_out);
+  BZ_LAUNCH_CHECK();
+  BZ_CUDA(cudaMemcpyAsync(h_out, d_out, N * sizeof(fp), cudaMemcpyDeviceToHost, s));
+  BZ_CUDA(cudaStreamSynchronize(s));
+  return h_out[0];
+}
+
+static void put_canonical(uint8_t *b, fp mont, const FpCtx &c) {
+  fp v = fp_mul(mont, fp{1, 0}, c);
+  memcpy(b, &v.lo, 8);
+  memcpy(b + 8, &v.hi, 8);
+}
+
+// recover_full_round_polynomial_and_sample_next_challenge (sumcheck.rs:787-811)
+static fp round_message(Transcript &ts, const FpCtx &c, fp &claim, const fp *wl, int ncoef,
+                        u128 q, fp *coefs_out) {
+  fp co[4];
+  co[0] = wl[0];
+  co[1] = fp_zero();
+  for (int i = 2; i < ncoef; i++) co[i] = wl[i - 1];
+  fp at_one = fp_zero();
+  for (int i = 0; i < ncoef; i++) at_one = fp_add(at_one, co[i], c);
+  co[1] = fp_sub(fp_sub(claim, co[0], c), at_one, c);
+  uint8_t msg[64];
+  for (int i = 0; i < ncoef; i++) put_canonical(msg + 16 * i, co[i], c);
+  ts.public_message(msg, 16 * (size_t)ncoef);
+  u128 rc = ts.challenge_fp(q);
+  fp r = fp_mul(fp{(uint64_t)rc, (uint64_t)(rc >> 64)}, c.r2, c);
+  fp v = fp_zero();
+  for (int i = ncoef - 1; i >= 0; i--) v = fp_add(fp_mul(v, r, c), co[i], c);
+  claim = v;
+  for (int i = 0; i < ncoef; i++) coefs_out[i] = co[i];
+  return r;
+}
+
+void spartan_prove(const SpartanArgs &a, Transcript &ts, SpartanScratch &sc, cudaStream_t s,
+                   SpartanOut &out) {
+  const FpCtx &c = a.ctx;
+  const int nr = a.num_row_vars, nc = a.num_col_vars;
+  const size_t R = (size_t)1 << nr, Cn = (size_t)1 << nc;
+  ts.public_message(a.digest, 32);
+  fp tau[kMaxFpPoint];
+  for (int i = 0; i < nr; i++) {
+    u128 t = ts.challenge_fp(a.q);
+    tau[i] = fp_mul(fp{(uint64_t)t, (uint64_t)(t >> 64)}, c.r2, c);
+  }
+  fp *E = sc.t[0], *A = sc.t[1], *B = sc.t[2], *C = sc.t[3];
+  fp *E2 = sc.t[4], *A2 = sc.t[5], *B2 = sc.t[6], *C2 = sc.t[7];
+  fp_eq_table(tau, nr, c, E, sc.eq_scratch, s);
+  k_products_to_fp<<<grid_for(R), kThreads, 0, s>>>(a.prod, a.rows, R, c, A, B, C);
+  BZ_LAUNCH_CHECK();
+  fp claim = fp_zero();
+  out.outer.resize(4 * (size_t)nr);
+  out.rx.resize(nr);
+  size_t len = R;
+  fp r = fp_zero();
+  for (int round = 0; round < nr; round++) {
+    int fold = round > 0;
+    size_t npairs = fold ? (len / 2 + 1) / 2 : len / 2;
+    int g = grid_for(npairs);
+    k_outer_round<<<g, kThreads, 0, s>>>(E, A, B, C, E2, A2, B2, C2, len, fold, 1, r, c, sc.partial);
+    BZ_LAUNCH_CHECK();
+    host_partial_sum(sc.partial, g, 3, sc.sums, sc.host, c, s);
+    if (fold) {
+      std::swap(E, E2);
+      std::swap(A, A2);
+      std::swap(B, B2);
+      std::swap(C, C2);
+      len /= 2;
+    }
+    fp co[4];
+    r = round_message(ts, c, claim, sc.host, 4, a.q, co);
+    for (int i = 0; i < 4; i++) out.outer[4 * round + i] = co[i];
+    out.rx[round] = r;
+  }
+  // the last fold leaves one entry per table
+  k_outer_round<<<1, kThreads, 0, s>>>(E, A, B, C, E2, A2, B2, C2, len, 1, 0, r, c, sc.partial);
+  BZ_LAUNCH_CHECK();
+  fp fin[3];
+  BZ_CUDA(cudaMemcpyAsync(&fin[0], A2, sizeof(fp), cudaMemcpyDeviceToHost, s));
+  BZ_CUDA(cudaMemcpyAsync(&fin[1], B2, sizeof(fp), cudaMemcpyDeviceToHost, s));
+  BZ_CUDA(cudaMemcpyAsync(&fin[2], C2, sizeof(fp), cudaMemcpyDeviceToHost, s));
+  BZ_CUDA(cudaStreamSynchronize(s));
+  uint8_t msg[48];
+  for (int k = 0; k < 3; k++) {
+    out.abc[k] = fin[k];
+    put_canonical(msg + 16 * k, fin[k], c);
+  }
+  ts.public_message(msg, 48);
+  u128 rhoc = ts.challenge_fp(a.q);
+  fp rho = fp_mul(fp{(uint64_t)rhoc, (uint64_t)(rhoc >> 64)}, c.r2, c);
+  fp rho2 = fp_mul(rho, rho, c);
+  claim = fp_add(fp_add(fin[0], fp_mul(rho, fin[1], c), c), fp_mul(rho2, fin[2], c), c);
+  // bind: eq(r_x) over the rows, then the column gather
+  fp *eq = sc.t[0];
+  fp_eq_table(out.rx.data(), nr, c, eq, sc.eq_scratch, s);
+  k_bind_table<<<(a.ntab + 127) / 128, 128, 0, s>>>(a.tab_vals, a.tab_which, a.ntab, rho, rho2, c,
+                                                     sc.tab);
+  BZ_LAUNCH_CHECK();
+  fp *D = sc.d[0], *W = sc.d[1], *D2 = sc.d[2], *W2 = sc.d[3];
+  k_bind<<<grid_for(Cn), kThreads, 0, s>>>(a.csc_off, a.csc_row, a.csc_idx, sc.tab, eq, a.cols, Cn,
+                                           c, D);
+  BZ_LAUNCH_CHECK();
+  if (a.n_bit_rows) {
+    k_bind_bits<<<1, kThreads, 0, s>>>(a.bit_rows, a.n_bit_rows, eq, rho2, c, D);
+    BZ_LAUNCH_CHECK();
+  }
+  // inner sumcheck
+  out.inner.resize(3 * (size_t)nc);
+  out.ry.resize(nc);
+  len = Cn;
+  int w_bits = 1;
+  for (int round = 0; round < nc; round++) {
+    int fold = round > 0;
+    size_t npairs = fold ? (len / 2 + 1) / 2 : len / 2;
+    int g = grid_for(npairs);
+    k_inner_round<<<g, kThreads, 0, s>>>(D, W, a.hbits, w_bits, D2, W2, len, fold, 1, r, c,
+                                         sc.partial);
+    BZ_LAUNCH_CHECK();
+    host_partial_sum(sc.partial, g, 2, sc.sums, sc.host, c, s);
+    if (fold) {
+      std::swap(D, D2);
+      std::swap(W, W2);
+      len /= 2;
+      w_bits = 0;
+    }
+    fp co[3];
+    r = round_message(ts, c, claim, sc.host, 3, a.q, co);
+    for (int i = 0; i < 3; i++) out.inner[3 * round + i] = co[i];
+    out.ry[round] = r;
+  }
+  k_inner_round<<<1, kThreads, 0, s>>>(D, W, a.hbits, w_bits, D2, W2, len, 1, 0, r, c, sc.partial);
+  BZ_LAUNCH_CHECK();
+  fp dw[2];
+  BZ_CUDA(cudaMemcpyAsync(&dw[0], D2, sizeof(fp), cudaMemcpyDeviceToHost, s));
+  BZ_CUDA(cudaMemcpyAsync(&dw[1], W2, sizeof(fp), cudaMemcpyDeviceToHost, s));
+  BZ_CUDA(cudaStreamSynchronize(s));
+  out.d_at_ry = dw[0];
+  out.final_claim = claim;
+  out.ok = fp_mul(dw[0], dw[1], c).lo == claim.lo && fp_mul(dw[0], dw[1], c).hi == claim.hi;
+}
+
+FpCtx make_fp_ctx(u128 q) {
+  FpCtx c;
+  c.q0 = (uint64_t)q;
+  c.q1 = (uint64_t)(q >> 64);
+  // -q^{-1} mod 2^64 by Newton iteration on the odd low word
+  uint64_t inv = 1;
+  for (int i = 0; i < 7; i++) inv *= 2 - c.q0 * inv;
+  c.qinv = (uint64_t)0 - inv;
+  u128 one = ((~(u128)0) % q + 1) % q;  // 2^128 mod q
+  c.one = fp{(uint64_t)one, (uint64_t)(one >> 64)};
+  u128 x = one;
+  for (int i = 0; i < 128; i++) {
+    x <<= 1;  // x < q < 2^126: no overflow
+    if (x >= q) x -= q;
+  }
+  c.r2 = fp{(uint64_t)x, (uint64_t)(x >> 64)};
+  return c;
+}
+
+u128 fp_canonical(fp mont, const FpCtx &c) {
+  fp v = fp_mul(mont, fp{1, 0}, c);
+  return (u128)v.lo | ((u128)v.hi << 64);
+}
+
+fp fp_to_mont(u128 v, const FpCtx &c) { return fp_mul(fp{(uint64_t)v, (uint64_t)(v >> 64)}, c.r2, c); }
+
+}  // namespace bz

@@ -79,6 +79,47 @@ int bitz_gkr_prove_dev(const uint64_t *row_images_dev, const uint64_t *columns_d
 int bitz_gkr_outputs(const uint64_t *row_images, const uint64_t *columns, int log_cols,
                      uint64_t *out);
 
+/* ----------------------------------------------------- end-to-end prover
+ * A prepared statement of one of the four SHA-256 circuits.
+ * Replaces CircuitProofSystem::new(statement, SecurityLevel)
+ * (tooling/cli/src/end_to_end.rs:161-197) with the statement of
+ * tooling/cli/src/circuits.rs:58-210: circuit_kind 0 sha256-compression
+ * (768 input bits), 1 sha256-chain (512 n), 2 sha256-block-aligned (512 k),
+ * 3 sha256-2kb (16384); input_bits and the 256 output_bits one byte (0/1)
+ * per bit in the statement's order. security_bits is the PCS profile (100 or
+ * 128). The circuit's structure is built once per (kind, size) and cached. */
+typedef struct bitz_system bitz_system;
+int bitz_system_new(int circuit_kind, const uint8_t *input_bits, size_t n_inputs,
+                    const uint8_t *output_bits, uint32_t security_bits, bitz_system **out);
+void bitz_system_free(bitz_system *sys);
+/* CircuitProofSystem::stats (end_to_end.rs:199-212): [0] constraints, [1]
+ * assignment entries, [2] committed bits, [3] padded committed bits, [4]
+ * prime bits, [5] PCS security, [6] claim column bits s, [7] compressions. */
+int bitz_system_stats(const bitz_system *sys, uint64_t out[8]);
+/* witness + commit + prove (end_to_end.rs:215-336; the stages
+ * benchmark::run times, tooling/cli/src/benchmark.rs:28-79). Returns the
+ * proof bytes root || Spartan section || bitzPCS wire container
+ * (crates/host/src/wire_proof.rs:88-104) in a buffer freed with bitz_free,
+ * and the stage times in milliseconds (witness, commit, prove).
+ * BZ_ERR_UNSATISFIED when the statement is false (Error::Unsatisfied). */
+int bitz_system_prove(bitz_system *sys, uint8_t **proof, size_t *proof_len, double times_ms[3]);
+void bitz_free(void *p);
+/* Diagnostic (no reference counterpart): the last proof's packed witness f,
+ * packed h = M (1 || f) and the exact products (A h, B h, C h per row). */
+int bitz_system_witness(bitz_system *sys, uint32_t *f_words, size_t f_cap, uint32_t *h_words,
+                        size_t h_cap, int64_t *products, size_t prod_cap);
+
+/* Diagnostic (no reference counterpart): the structural setup of a circuit
+ * size, as ConstraintGenerator and MTransposeGenerator build it
+ * (crates/circuit/src/constraints.rs:678-880,
+ * crates/circuit/src/matrix_transpose.rs:475-560). sizes: [0] f bits, [1] h
+ * entries, [2] rows, [3] M nonzeros, [4] C nonzeros without the statement's
+ * bit constants, [5] compressions, [6] claim column bits, [7] committed m.
+ * The array outputs are filled when non-null. Needs no GPU. */
+int bitz_circuit_layout(int circuit_kind, size_t n_inputs, uint64_t sizes[8],
+                        uint8_t map_digest[32], uint32_t *m_off, uint32_t *m_pos,
+                        uint32_t *c_off, uint32_t *c_col, int64_t *c_coef);
+
 #ifdef __cplusplus
 }
 #endif
