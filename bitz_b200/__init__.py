@@ -49,6 +49,14 @@ def device_count():
     return _lib.load().bitz_device_count()
 
 
+def set_device(device: int):
+    _check(_lib.load().bitz_set_device(device))
+
+
+def launch_count() -> int:
+    return int(_lib.load().bitz_launch_count())
+
+
 class ProverState:
     """The prover transcript (crates/transcript/src/prover.rs:10)."""
 
@@ -174,15 +182,19 @@ class CircuitProofSystem:
                 "prime_bits", "pcs_security", "claim_log_cols", "compressions"]
         return dict(zip(keys, (int(x) for x in out)))
 
-    def prove(self):
-        """witness + commit + prove; returns (proof bytes, stage times in ms)."""
+    def prove(self, restage: bool = True):
+        """witness + commit + prove; returns (proof bytes, times in ms).
+
+        restage=False reuses the statement staged on the device at creation."""
         p = ctypes.POINTER(ctypes.c_uint8)()
         n = ctypes.c_size_t(0)
-        times = (ctypes.c_double * 3)()
-        _check(self._lib.bitz_system_prove(self._h, ctypes.byref(p), ctypes.byref(n), times))
+        times = (ctypes.c_double * 4)()
+        _check(self._lib.bitz_system_prove_ex(self._h, int(restage), ctypes.byref(p),
+                                              ctypes.byref(n), times))
         data = ctypes.string_at(p, n.value)
         self._lib.bitz_free(p)
-        return data, {"witness_ms": times[0], "commit_ms": times[1], "prove_ms": times[2]}
+        return data, {"witness_ms": times[0], "commit_ms": times[1], "prove_ms": times[2],
+                      "device_ms": times[3]}
 
     def witness(self, f_words: int, h_words: int, rows: int):
         f = np.zeros(f_words, dtype=np.uint32)

@@ -17,6 +17,7 @@ _vp = ctypes.c_void_p
 SIGNATURES = [
     ("bitz_last_error", ctypes.c_char_p, []),
     ("bitz_device_count", ctypes.c_int, []),
+    ("bitz_set_device", ctypes.c_int, [ctypes.c_int]),
     ("bitz_transcript_new", _vp, [_vp, ctypes.c_size_t, _vp, ctypes.c_size_t]),
     ("bitz_transcript_free", None, [_vp]),
     ("bitz_transcript_public", ctypes.c_int, [_vp, _vp, ctypes.c_size_t]),
@@ -42,7 +43,11 @@ SIGNATURES = [
     ("bitz_system_stats", ctypes.c_int, [_vp, _u64p]),
     ("bitz_system_prove", ctypes.c_int,
      [_vp, ctypes.POINTER(_u8p), ctypes.POINTER(ctypes.c_size_t), ctypes.POINTER(ctypes.c_double)]),
+    ("bitz_system_prove_ex", ctypes.c_int,
+     [_vp, ctypes.c_int, ctypes.POINTER(_u8p), ctypes.POINTER(ctypes.c_size_t),
+      ctypes.POINTER(ctypes.c_double)]),
     ("bitz_free", None, [_vp]),
+    ("bitz_launch_count", ctypes.c_ulonglong, []),
     ("bitz_system_witness", ctypes.c_int,
      [_vp, _vp, ctypes.c_size_t, _vp, ctypes.c_size_t, _vp, ctypes.c_size_t]),
     ("bitz_circuit_layout", ctypes.c_int,

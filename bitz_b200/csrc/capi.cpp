@@ -52,6 +52,12 @@ int bitz_device_count(void) {
   return n;
 }
 
+int bitz_set_device(int device) {
+  cudaError_t e = cudaSetDevice(device);
+  if (e != cudaSuccess) return fail(BZ_ERR_CUDA, cudaGetErrorString(e));
+  return BZ_OK;
+}
+
 bitz_transcript *bitz_transcript_new(const uint8_t *session, size_t slen, const uint8_t *instance,
                                      size_t ilen) {
   try {

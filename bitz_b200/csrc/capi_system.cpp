@@ -74,14 +74,19 @@ int bitz_system_stats(const bitz_system *sys, uint64_t out[8]) {
   return BZ_OK;
 }
 
-int bitz_system_prove(bitz_system *sys, uint8_t **proof, size_t *proof_len, double times_ms[3]) {
+int bitz_system_prove(bitz_system *sys, uint8_t **proof, size_t *proof_len, double times_ms[4]) {
+  return bitz_system_prove_ex(sys, 1, proof, proof_len, times_ms);
+}
+
+int bitz_system_prove_ex(bitz_system *sys, int restage, uint8_t **proof, size_t *proof_len,
+                         double times_ms[4]) {
   if (!sys || !proof || !proof_len) return capi_fail(BZ_ERR_ARGUMENT, "null argument");
   *proof = nullptr;
   *proof_len = 0;
   try {
     std::vector<uint8_t> p;
     StageTimes t;
-    int rc = sys->ps->prove(p, &t);
+    int rc = sys->ps->prove(p, &t, restage != 0);
     if (rc) return capi_fail(rc, sys->ps->error);
     *proof = (uint8_t *)malloc(p.size());
     if (!*proof) return capi_fail(BZ_ERR_INTERNAL, "out of host memory");
@@ -91,6 +96,7 @@ int bitz_system_prove(bitz_system *sys, uint8_t **proof, size_t *proof_len, doub
       times_ms[0] = t.witness_ms;
       times_ms[1] = t.commit_ms;
       times_ms[2] = t.prove_ms;
+      times_ms[3] = t.device_ms;
     }
     return BZ_OK;
   } catch (const CudaError &e) {
@@ -101,6 +107,8 @@ int bitz_system_prove(bitz_system *sys, uint8_t **proof, size_t *proof_len, doub
 }
 
 void bitz_free(void *p) { free(p); }
+
+unsigned long long bitz_launch_count(void) { return launch_counter(); }
 
 int bitz_system_witness(bitz_system *sys, uint32_t *f_words, size_t f_cap, uint32_t *h_words,
                         size_t h_cap, int64_t *products, size_t prod_cap) {

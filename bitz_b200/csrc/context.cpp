@@ -14,6 +14,11 @@ Context::Context() {
   gk_.pair = gk_pair_.get();
 }
 
+unsigned long long &launch_counter() {
+  static unsigned long long n = 0;
+  return n;
+}
+
 Context &Context::get() {
   // One context per process, created on first use on the current device.
   static Context *ctx = new Context();

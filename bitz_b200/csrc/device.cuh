@@ -24,7 +24,14 @@ struct CudaError : std::runtime_error {
                             __FILE__ + ":" + std::to_string(__LINE__));                        \
   } while (0)
 
-#define BZ_LAUNCH_CHECK() BZ_CUDA(cudaGetLastError())
+// Every launch site ends in BZ_LAUNCH_CHECK(), which also counts the launch
+// (read through bitz_launch_count()).
+unsigned long long &launch_counter();
+#define BZ_LAUNCH_CHECK()           \
+  do {                              \
+    ++::bz::launch_counter();       \
+    BZ_CUDA(cudaGetLastError());    \
+  } while (0)
 
 constexpr int kThreads = 256;
 // 148 SMs on B200; grids are sized in multiples of the SM count and walked

@@ -107,6 +107,23 @@ double ms_since(std::chrono::steady_clock::time_point t) {
   return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t).count();
 }
 
+// Phase timer: with BITZ_PHASES set, each phase's host time (after a stream
+// sync) is printed to stderr.
+struct Phases {
+  cudaStream_t s;
+  bool on;
+  std::chrono::steady_clock::time_point t;
+  explicit Phases(cudaStream_t st) : s(st), on(getenv("BITZ_PHASES") != nullptr) {
+    t = std::chrono::steady_clock::now();
+  }
+  void mark(const char *name) {
+    if (!on) return;
+    cudaStreamSynchronize(s);
+    fprintf(stderr, "[phase] %-22s %8.3f ms\n", name, ms_since(t));
+    t = std::chrono::steady_clock::now();
+  }
+};
+
 // Setup cache: one device copy per (circuit, input size).
 std::mutex g_setup_mu;
 std::map<std::pair<int, size_t>, std::shared_ptr<DeviceSetup>> g_setups;
@@ -168,6 +185,7 @@ std::shared_ptr<DeviceSetup> device_setup(int kind, size_t n_inputs, cudaStream_
   d->tab_vals.upload(vals.data(), vals.size(), s);
   d->tab_which.upload(which.data(), which.size(), s);
   d->ntab = (int)vals.size();
+  d->col0_nnz = cnt[1];
   BZ_CUDA(cudaStreamSynchronize(s));
   g_setups[key] = d;
   return d;
@@ -228,6 +246,11 @@ Workspace &workspace() {
 
 // ----------------------------------------------------------- ProofSystem
 
+static void prepare_statement(int kind, const CircuitSetup &S, const std::vector<uint8_t> &inputs_,
+                              const std::vector<uint8_t> &outputs_, std::vector<uint32_t> &states,
+                              std::vector<uint32_t> &msgs, std::vector<uint32_t> &fin,
+                              std::vector<uint8_t> &bitc);
+
 ProofSystem::ProofSystem(int kind, const uint8_t *inputs, size_t n_inputs, const uint8_t *outputs,
                          int security_bits)
     : kind_(kind), security_(security_bits), inputs_(inputs, inputs + n_inputs),
@@ -257,6 +280,24 @@ ProofSystem::ProofSystem(int kind, const uint8_t *inputs, size_t n_inputs, const
   pcs_enc_.insert(pcs_enc_.end(), v, v + strlen(v));
   put_u64(pcs_enc_, (uint64_t)1 << S.committed_m);
   for (int i = 0; i < 4; i++) pcs_enc_.push_back((uint8_t)((uint32_t)security_bits >> (8 * i)));
+  prepare_statement(kind, S, inputs_, outputs_, states_h_, msgs_h_, fin_h_, bitc_h_);
+  stage_statement(s);
+  BZ_CUDA(cudaEventCreate(&ev_start_));
+  BZ_CUDA(cudaEventCreate(&ev_stop_));
+  BZ_CUDA(cudaStreamSynchronize(s));
+}
+
+ProofSystem::~ProofSystem() {
+  if (ev_start_) cudaEventDestroy(ev_start_);
+  if (ev_stop_) cudaEventDestroy(ev_stop_);
+}
+
+void ProofSystem::stage_statement(cudaStream_t s) {
+  states_.upload(states_h_.data(), states_h_.size(), s);
+  msgs_.upload(msgs_h_.data(), msgs_h_.size(), s);
+  offsets_.upload(dev_->host->block_f_offset.data(), dev_->host->block_f_offset.size(), s);
+  fin_.upload(fin_h_.data(), std::max<size_t>(fin_h_.size(), 1), s);
+  bit_c_.upload(bitc_h_.data(), bitc_h_.size(), s);
 }
 
 int ProofSystem::witness(cudaStream_t s) {
@@ -264,9 +305,59 @@ int ProofSystem::witness(cudaStream_t s) {
   Workspace &W = workspace();
   W.acc.resize(512);
   size_t n_in = inputs_.size();
-  // chaining values and message words of every compression (host: a few
-  // hundred nanoseconds per block), then the device expands each block
-  std::vector<uint32_t> states(8 * S.n_blocks), msgs(16 * S.n_blocks);
+  size_t fwords = ((size_t)1 << S.committed_m) / 32;
+  size_t hwords = ((size_t)1 << (S.claim_log_cols + 7)) / 32;
+  f_.resize(fwords);
+  h_.resize(hwords);
+  BZ_CUDA(cudaMemsetAsync(f_.get(), 0, fwords * 4, s));
+  BZ_CUDA(cudaMemsetAsync(h_.get(), 0, hwords * 4, s));
+  if (n_in)
+    BZ_CUDA(cudaMemcpyAsync(f_.get(), fin_.get(), fin_h_.size() * 4, cudaMemcpyDeviceToDevice, s));
+  prod_.resize(3 * S.rows);
+  W.flag.resize(1);
+  BZ_CUDA(cudaMemsetAsync(W.flag.get(), 0, sizeof(int), s));
+  WitnessArgs a;
+  a.states = states_.get();
+  a.msgs = msgs_.get();
+  a.offsets = offsets_.get();
+  a.nblocks = (int)S.n_blocks;
+  a.f = f_.get();
+  a.h_len = S.h_len;
+  a.m_off = dev_->m_off.get();
+  a.m_pos = dev_->m_pos.get();
+  a.h = h_.get();
+  a.rows = S.rows;
+  a.n_inputs = n_in;
+  for (int k = 0; k < 3; k++) {
+    a.abc_off[k] = dev_->abc_off[k].get();
+    a.abc_col[k] = dev_->abc_col[k].get();
+    a.abc_coef[k] = dev_->abc_coef[k].get();
+  }
+  a.bit_c = bit_c_.get();
+  a.prod = prod_.get();
+  a.unsat = W.flag.get();
+  witness_generate(a, s);
+  int unsat = 0;
+  BZ_CUDA(cudaMemcpyAsync(&unsat, W.flag.get(), sizeof(int), cudaMemcpyDeviceToHost, s));
+  BZ_CUDA(cudaStreamSynchronize(s));
+  if (unsat) {
+    error = "circuit witness does not satisfy the constraints";
+    return BZ_ERR_UNSATISFIED;
+  }
+  return BZ_OK;
+}
+
+// The statement's chaining values and message words for every compression
+// (the chain is sequential, a few hundred nanoseconds per block on the host);
+// the device expands each block's hints in parallel.
+static void prepare_statement(int kind, const CircuitSetup &S, const std::vector<uint8_t> &inputs_,
+                              const std::vector<uint8_t> &outputs_, std::vector<uint32_t> &states,
+                              std::vector<uint32_t> &msgs, std::vector<uint32_t> &fin,
+                              std::vector<uint8_t> &bitc) {
+  const int kind_ = kind;
+  size_t n_in = inputs_.size();
+  states.assign(8 * S.n_blocks, 0);
+  msgs.assign(16 * S.n_blocks, 0);
   static const uint32_t IV[8] = {0x6a09e667, 0xbb67ae85, 0x3c6ef372, 0xa54ff53a,
                                  0x510e527f, 0x9b05688c, 0x1f83d9ab, 0x5be0cd19};
   uint32_t st[8];
@@ -299,54 +390,11 @@ int ProofSystem::witness(cudaStream_t s) {
     for (int i = 0; i < 16; i++) msgs[16 * b + i] = m[i];
     sha256_compress_host(st, m);
   }
-  size_t fwords = ((size_t)1 << S.committed_m) / 32;
-  size_t hwords = ((size_t)1 << (S.claim_log_cols + 7)) / 32;
-  std::vector<uint32_t> fin((n_in + 31) / 32, 0);
+  fin.assign((n_in + 31) / 32, 0);
   for (size_t i = 0; i < n_in; i++) fin[i / 32] |= (uint32_t)inputs_[i] << (i % 32);
-  f_.resize(fwords);
-  h_.resize(hwords);
-  BZ_CUDA(cudaMemsetAsync(f_.get(), 0, fwords * 4, s));
-  BZ_CUDA(cudaMemsetAsync(h_.get(), 0, hwords * 4, s));
-  BZ_CUDA(cudaMemcpyAsync(f_.get(), fin.data(), fin.size() * 4, cudaMemcpyHostToDevice, s));
-  W.states.upload(states.data(), states.size(), s);
-  W.msgs_u32.upload(msgs.data(), msgs.size(), s);
-  W.offsets.upload(S.block_f_offset.data(), S.block_f_offset.size(), s);
-  std::vector<uint8_t> bitc(n_in + 256);
+  bitc.assign(n_in + 256, 0);
   for (size_t i = 0; i < n_in; i++) bitc[i] = inputs_[i];
   for (int i = 0; i < 256; i++) bitc[n_in + i] = outputs_[i];
-  bit_c_.upload(bitc.data(), bitc.size(), s);
-  prod_.resize(3 * S.rows);
-  W.flag.resize(1);
-  BZ_CUDA(cudaMemsetAsync(W.flag.get(), 0, sizeof(int), s));
-  WitnessArgs a;
-  a.states = W.states.get();
-  a.msgs = W.msgs_u32.get();
-  a.offsets = W.offsets.get();
-  a.nblocks = (int)S.n_blocks;
-  a.f = f_.get();
-  a.h_len = S.h_len;
-  a.m_off = dev_->m_off.get();
-  a.m_pos = dev_->m_pos.get();
-  a.h = h_.get();
-  a.rows = S.rows;
-  a.n_inputs = n_in;
-  for (int k = 0; k < 3; k++) {
-    a.abc_off[k] = dev_->abc_off[k].get();
-    a.abc_col[k] = dev_->abc_col[k].get();
-    a.abc_coef[k] = dev_->abc_coef[k].get();
-  }
-  a.bit_c = bit_c_.get();
-  a.prod = prod_.get();
-  a.unsat = W.flag.get();
-  witness_generate(a, s);
-  int unsat = 0;
-  BZ_CUDA(cudaMemcpyAsync(&unsat, W.flag.get(), sizeof(int), cudaMemcpyDeviceToHost, s));
-  BZ_CUDA(cudaStreamSynchronize(s));
-  if (unsat) {
-    error = "circuit witness does not satisfy the constraints";
-    return BZ_ERR_UNSATISFIED;
-  }
-  return BZ_OK;
 }
 
 int ProofSystem::commit(cudaStream_t s) {
@@ -577,6 +625,7 @@ int ProofSystem::prove_after_commit(cudaStream_t s, std::vector<uint8_t> &proof)
   Tables &T = tables(s);
   Context &ctx = Context::get();
   Transcript &t = *ts_;
+  Phases ph(s);
   // bind (end_to_end.rs:442-455)
   t.public_u64(public_bytes_.size());
   t.public_message(public_bytes_.data(), public_bytes_.size());
@@ -600,6 +649,7 @@ int ProofSystem::prove_after_commit(cudaStream_t s, std::vector<uint8_t> &proof)
   const uint8_t *gb = reinterpret_cast<const uint8_t *>(&generator_);
   params.insert(params.end(), gb, gb + 16);
   t.public_message(params.data(), params.size());
+  ph.mark("bind+prime");
   // Spartan
   int nr = ceil_log2(S.rows ? S.rows : 1), nc = ceil_log2(S.h_len);
   size_t R = (size_t)1 << nr, Cn = (size_t)1 << nc;
@@ -631,6 +681,7 @@ int ProofSystem::prove_after_commit(cudaStream_t s, std::vector<uint8_t> &proof)
   sa.csc_off = dev_->sp_off.get();
   sa.csc_row = dev_->sp_row.get();
   sa.csc_idx = dev_->sp_idx.get();
+  sa.col0_nnz = dev_->col0_nnz;
   sa.tab_vals = dev_->tab_vals.get();
   sa.tab_which = dev_->tab_which.get();
   sa.ntab = dev_->ntab;
@@ -638,6 +689,7 @@ int ProofSystem::prove_after_commit(cudaStream_t s, std::vector<uint8_t> &proof)
   sa.n_bit_rows = (int)bit_rows_.size();
   SpartanOut so;
   spartan_prove(sa, t, sc, s, so);
+  ph.mark("spartan");
   if (!so.ok) {
     error = "Spartan closing check failed";
     return BZ_ERR_INTERNAL;
@@ -689,6 +741,7 @@ int ProofSystem::prove_after_commit(cudaStream_t s, std::vector<uint8_t> &proof)
     t.public_message(ce.data(), ce.size());
   }
   t.public_message(pcs_enc_.data(), pcs_enc_.size());
+  ph.mark("claim");
   // send_fold (crates/prover/src/fold.rs:38-75)
   W.exps.upload(rows_w.data(), 128, s);
   W.folds.resize(ncol);
@@ -705,6 +758,7 @@ int ProofSystem::prove_after_commit(cudaStream_t s, std::vector<uint8_t> &proof)
   t.grind("bitz/columns/v1", grinding_bits((uint32_t)security_, (uint64_t)sc_cols));
   std::vector<f128> zeta(sc_cols);
   for (auto &z : zeta) z = t.challenge_f128();
+  ph.mark("fold");
   // gkr_reduce (crates/prover/src/reduce.rs:17-47)
   GkrScratch &gs = ctx.gkr_scratch(sc_cols);
   gkr_build(hpk, sc_cols, W.images.get(), gs, s);
@@ -712,6 +766,7 @@ int ProofSystem::prove_after_commit(cudaStream_t s, std::vector<uint8_t> &proof)
   f128 gclaim = gkr_prove(sc_cols, zeta.data(), grinding_bits((uint32_t)security_, 3), t, gs, s,
                           gpt.data());
   f128 ip_target = gadd(gclaim, mk(1, 0));
+  ph.mark("gkr");
   std::vector<f128> eqb(128), u1(128);
   eq_table_host(gpt.data() + sc_cols, 7, eqb.data());
   for (int b = 0; b < 128; b++) u1[b] = gmul(gadd(row_images[b], mk(1, 0)), eqb[b]);
@@ -757,6 +812,7 @@ int ProofSystem::prove_after_commit(cudaStream_t s, std::vector<uint8_t> &proof)
   t.public_message(digest, 32);
   t.public_f128(target2);
   t.public_message("bitz/pcs/inner-product-sumcheck/v2", 34);
+  ph.mark("transpose+digest");
   // post-GKR sumcheck
   W.ones.resize(1);
   f128 one = mk(1, 0);
@@ -777,6 +833,7 @@ int ProofSystem::prove_after_commit(cudaStream_t s, std::vector<uint8_t> &proof)
     error = "post-GKR claim does not hold";
     return rc;
   }
+  ph.mark("post_gkr");
   // prove(Mle) with binding (opening.rs:119-135, 323-335)
   t.public_message("bitz/pcs/mle-opening/v1", 23);
   t.public_message(root_, 32);
@@ -840,7 +897,9 @@ int ProofSystem::prove_after_commit(cudaStream_t s, std::vector<uint8_t> &proof)
   packed_basis(W.suffix.get(), np, W.bw.get(), security_ == 100 ? W.eq_ood.get() : nullptr, coef,
                W.lb.get(), s);
   BZ_CUDA(cudaMemcpyAsync(W.lf.get(), f_.get(), np * 16, cudaMemcpyDeviceToDevice, s));
+  ph.mark("ring_switch");
   std::vector<uint8_t> lproof = ligerito(s, ptarget);
+  ph.mark("ligerito");
   if (lproof.empty()) {
     error = "Ligerito closing check failed";
     return BZ_ERR_INTERNAL;
@@ -868,9 +927,11 @@ int ProofSystem::prove_after_commit(cudaStream_t s, std::vector<uint8_t> &proof)
   return BZ_OK;
 }
 
-int ProofSystem::prove(std::vector<uint8_t> &proof, StageTimes *times) {
+int ProofSystem::prove(std::vector<uint8_t> &proof, StageTimes *times, bool restage) {
   cudaStream_t s = Context::get().stream();
   auto t0 = std::chrono::steady_clock::now();
+  BZ_CUDA(cudaEventRecord(ev_start_, s));
+  if (restage) stage_statement(s);
   int rc = witness(s);
   if (rc) return rc;
   double tw = ms_since(t0);
@@ -880,10 +941,15 @@ int ProofSystem::prove(std::vector<uint8_t> &proof, StageTimes *times) {
   double tc = ms_since(t1);
   auto t2 = std::chrono::steady_clock::now();
   rc = prove_after_commit(s, proof);
+  BZ_CUDA(cudaEventRecord(ev_stop_, s));
+  BZ_CUDA(cudaEventSynchronize(ev_stop_));
   if (times) {
     times->witness_ms = tw;
     times->commit_ms = tc;
     times->prove_ms = ms_since(t2);
+    float dm = 0;
+    BZ_CUDA(cudaEventElapsedTime(&dm, ev_start_, ev_stop_));
+    times->device_ms = dm;
   }
   return rc;
 }

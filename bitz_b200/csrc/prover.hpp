@@ -39,10 +39,12 @@ struct DeviceSetup {
   DeviceBuffer<int64_t> tab_vals;
   DeviceBuffer<uint8_t> tab_which;
   int ntab = 0;
+  uint32_t col0_nnz = 0;
 };
 
 struct StageTimes {
   double witness_ms = 0, commit_ms = 0, prove_ms = 0;
+  double device_ms = 0;  // CUDA-event span on the prover's stream, first to last launch
 };
 
 class ProofSystem {
@@ -51,10 +53,15 @@ class ProofSystem {
   // and expected output bits, one byte each) at a PCS security level.
   ProofSystem(int kind, const uint8_t *inputs, size_t n_inputs, const uint8_t *outputs,
               int security_bits);
+  ~ProofSystem();
+  ProofSystem(const ProofSystem &) = delete;
+  ProofSystem &operator=(const ProofSystem &) = delete;
 
   // witness + commit + prove (benchmark.rs:28-79), returning the proof bytes:
-  // root || Spartan section || bitzPCS wire container.
-  int prove(std::vector<uint8_t> &proof, StageTimes *times);
+  // root || Spartan section || bitzPCS wire container. With restage set the
+  // statement (input bits, chaining values, message words) is copied from
+  // host memory first; otherwise the copy made at construction is reused.
+  int prove(std::vector<uint8_t> &proof, StageTimes *times, bool restage = true);
 
   const CircuitSetup &setup() const { return *dev_->host; }
   int security() const { return security_; }
@@ -65,6 +72,7 @@ class ProofSystem {
                         std::vector<int64_t> &prod);
 
  private:
+  void stage_statement(cudaStream_t s);
   int witness(cudaStream_t s);
   int commit(cudaStream_t s);
   int prove_after_commit(cudaStream_t s, std::vector<uint8_t> &proof);
@@ -78,6 +86,14 @@ class ProofSystem {
   std::vector<uint8_t> public_bytes_, pcs_enc_;
   std::vector<uint32_t> bit_rows_;  // bit constraints whose expected value is one
   f128 generator_;
+
+  // the statement on the device: chaining values, message words, hint
+  // offsets, the packed input bits and every bit constraint's expected value
+  std::vector<uint32_t> states_h_, msgs_h_, fin_h_;
+  std::vector<uint8_t> bitc_h_;
+  DeviceBuffer<uint32_t> states_, msgs_, fin_;
+  DeviceBuffer<uint64_t> offsets_;
+  cudaEvent_t ev_start_ = nullptr, ev_stop_ = nullptr;
 
   // per-proof device state
   DeviceBuffer<uint32_t> f_, h_;

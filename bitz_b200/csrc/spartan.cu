@@ -198,16 +198,38 @@ __global__ void k_bind_table(const int64_t *__restrict__ vals, const uint8_t *__
 
 // bind_and_batch (matrix.rs:429-467) as a gather over the column-major copy of
 // A, B and C: D(y) = sum over column y's entries of eq(r_x, row) * table[idx].
+// Column 0 (the constant, one entry per round constant and bit constraint)
+// is left to k_bind_col0, which spreads it over a whole grid.
 __global__ void k_bind(const uint32_t *__restrict__ off, const uint32_t *__restrict__ row,
                        const uint16_t *__restrict__ idx, const fp *__restrict__ tab,
                        const fp *__restrict__ eq, size_t cols, size_t padded, FpCtx c, fp *D) {
   for (size_t y = blockIdx.x * (size_t)blockDim.x + threadIdx.x; y < padded;
        y += (size_t)gridDim.x * blockDim.x) {
     fp acc = fp_zero();
-    if (y < cols)
+    if (y > 0 && y < cols)
       for (uint32_t e = off[y]; e < off[y + 1]; e++) acc = fp_add(acc, fp_mul(eq[row[e]], tab[idx[e]], c), c);
     D[y] = acc;
   }
+}
+
+// Column 0's entries [0, n) split across blocks; per-block partial sums.
+__global__ void k_bind_col0(const uint32_t *__restrict__ row, const uint16_t *__restrict__ idx,
+                            const fp *__restrict__ tab, const fp *__restrict__ eq, uint32_t n,
+                            FpCtx c, fp *partial) {
+  fp acc[1] = {fp_zero()};
+  for (uint32_t e = blockIdx.x * blockDim.x + threadIdx.x; e < n; e += gridDim.x * blockDim.x)
+    acc[0] = fp_add(acc[0], fp_mul(eq[row[e]], tab[idx[e]], c), c);
+  block_fp_sum<1>(acc, c, partial);
+}
+
+// D[0] = the column-0 partial sums.
+__global__ void k_bind_col0_finish(const fp *partial, int nblocks, FpCtx c, fp *D) {
+  fp acc[1] = {fp_zero()};
+  for (int b = threadIdx.x; b < nblocks; b += blockDim.x) acc[0] = fp_add(acc[0], partial[b], c);
+  __shared__ fp out[1];
+  block_fp_sum<1>(acc, c, out);
+  __syncthreads();
+  if (threadIdx.x == 0) D[0] = out[0];
 }
 
 // The statement-dependent part of C: the bit constraints whose expected value
@@ -332,6 +354,13 @@ void spartan_prove(const SpartanArgs &a, Transcript &ts, SpartanScratch &sc, cud
   k_bind<<<grid_for(Cn), kThreads, 0, s>>>(a.csc_off, a.csc_row, a.csc_idx, sc.tab, eq, a.cols, Cn,
                                            c, D);
   BZ_LAUNCH_CHECK();
+  {
+    int g = grid_for(a.col0_nnz);
+    k_bind_col0<<<g, kThreads, 0, s>>>(a.csc_row, a.csc_idx, sc.tab, eq, a.col0_nnz, c, sc.partial);
+    BZ_LAUNCH_CHECK();
+    k_bind_col0_finish<<<1, kThreads, 0, s>>>(sc.partial, g, c, D);
+    BZ_LAUNCH_CHECK();
+  }
   if (a.n_bit_rows) {
     k_bind_bits<<<1, kThreads, 0, s>>>(a.bit_rows, a.n_bit_rows, eq, rho2, c, D);
     BZ_LAUNCH_CHECK();

@@ -24,6 +24,7 @@ struct SpartanArgs {
   // column-major A, B, C: entries (row, coefficient-table index)
   const uint32_t *csc_off, *csc_row;
   const uint16_t *csc_idx;
+  uint32_t col0_nnz;  // entries of column 0 (the first col0_nnz of csc_row/csc_idx)
   const int64_t *tab_vals;    // device: distinct coefficients
   const uint8_t *tab_which;   // device: 0 = A, 1 = B, 2 = C
   int ntab;

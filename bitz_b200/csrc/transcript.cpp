@@ -3,47 +3,8 @@
 
 namespace bz {
 
-static const uint64_t KRC[24] = {
-    0x0000000000000001ull, 0x0000000000008082ull, 0x800000000000808aull, 0x8000000080008000ull,
-    0x000000000000808bull, 0x0000000080000001ull, 0x8000000080008081ull, 0x8000000000008009ull,
-    0x000000000000008aull, 0x0000000000000088ull, 0x0000000080008009ull, 0x000000008000000aull,
-    0x000000008000808bull, 0x800000000000008bull, 0x8000000000008089ull, 0x8000000000008003ull,
-    0x8000000000008002ull, 0x8000000000000080ull, 0x000000000000800aull, 0x800000008000000aull,
-    0x8000000080008081ull, 0x8000000000008080ull, 0x0000000080000001ull, 0x8000000080008008ull};
 
-static inline uint64_t rol(uint64_t x, int n) { return (x << n) | (x >> ((64 - n) & 63)); }
 
-// FIPS 202 section 3.3 with the rho/pi lane walk unrolled.
-void keccak_f1600(uint64_t a[25]) {
-  static const int PI[24] = {10, 7, 11, 17, 18, 3, 5, 16, 8, 21, 24, 4,
-                             15, 23, 19, 13, 12, 2, 20, 14, 22, 9, 6, 1};
-  static const int RHO[24] = {1, 3, 6, 10, 15, 21, 28, 36, 45, 55, 2, 14,
-                              27, 41, 56, 8, 25, 43, 62, 18, 39, 61, 20, 44};
-  for (int round = 0; round < 24; round++) {
-    uint64_t c[5];
-    for (int x = 0; x < 5; x++) c[x] = a[x] ^ a[x + 5] ^ a[x + 10] ^ a[x + 15] ^ a[x + 20];
-    for (int x = 0; x < 5; x++) {
-      uint64_t d = c[(x + 4) % 5] ^ rol(c[(x + 1) % 5], 1);
-      for (int y = 0; y < 25; y += 5) a[y + x] ^= d;
-    }
-    uint64_t t = a[1];
-    for (int i = 0; i < 24; i++) {
-      int j = PI[i];
-      uint64_t tmp = a[j];
-      a[j] = rol(t, RHO[i]);
-      t = tmp;
-    }
-    for (int y = 0; y < 25; y += 5) {
-      uint64_t b0 = a[y], b1 = a[y + 1], b2 = a[y + 2], b3 = a[y + 3], b4 = a[y + 4];
-      a[y] = b0 ^ (~b1 & b2);
-      a[y + 1] = b1 ^ (~b2 & b3);
-      a[y + 2] = b2 ^ (~b3 & b4);
-      a[y + 3] = b3 ^ (~b4 & b0);
-      a[y + 4] = b4 ^ (~b0 & b1);
-    }
-    a[0] ^= KRC[round];
-  }
-}
 
 bool pow_valid(const uint8_t seed[16], uint64_t nonce, uint32_t bits) {
   if (bits > 32) return false;
@@ -84,50 +45,47 @@ void Transcript::grind(const char *label, uint32_t bits) {
 
 // --------------------------------------------------------- prime sampling
 
-static void mulw(u128 a, u128 b, u128 &lo, u128 &hi) {
-  u128 al = (uint64_t)a, ah = a >> 64, bl = (uint64_t)b, bh = b >> 64;
-  u128 ll = al * bl, hh = ah * bh, m1 = al * bh, m2 = ah * bl;
-  u128 mid = m1 + m2;
-  u128 mc = mid < m1;
-  u128 l = ll + (mid << 64);
-  lo = l;
-  hi = hh + (mid >> 64) + (mc << 64) + (l < ll);
-}
 
-// (a*b) mod q by binary long division of the 256-bit product (q < 2^126).
-static u128 mulmod(u128 a, u128 b, u128 q) {
-  u128 lo, hi;
-  mulw(a, b, lo, hi);
-  u128 r = 0;
-  for (int i = 255; i >= 0; i--) {
-    u128 bit = i >= 128 ? (hi >> (i - 128)) & 1 : (lo >> i) & 1;
-    r = (r << 1) | bit;  // r < 2q < 2^127: no overflow
-    if (r >= q) r -= q;
+// Montgomery context of an odd candidate q < 2^126 (R = 2^128).
+static FpCtx candidate_ctx(u128 q) {
+  FpCtx c;
+  c.q0 = (uint64_t)q;
+  c.q1 = (uint64_t)(q >> 64);
+  uint64_t inv = 1;
+  for (int i = 0; i < 7; i++) inv *= 2 - c.q0 * inv;  // Newton: q0 * inv = 1 mod 2^64
+  c.qinv = (uint64_t)0 - inv;
+  u128 one = ((~(u128)0) % q + 1) % q;
+  c.one = fp{(uint64_t)one, (uint64_t)(one >> 64)};
+  u128 x = one;
+  for (int i = 0; i < 128; i++) {
+    x <<= 1;
+    if (x >= q) x -= q;
   }
-  return r;
+  c.r2 = fp{(uint64_t)x, (uint64_t)(x >> 64)};
+  return c;
 }
 
-static u128 powmod(u128 b, u128 e, u128 q) {
-  u128 r = 1 % q;
-  b %= q;
-  while (e) {
-    if (e & 1) r = mulmod(r, b, q);
-    b = mulmod(b, b, q);
-    e >>= 1;
-  }
-  return r;
-}
+static inline u128 to_u128(fp v) { return (u128)v.lo | ((u128)v.hi << 64); }
 
-// crates/field/src/helpers.rs:198-215
-static bool strong_round(u128 q, u128 base) {
+// crates/field/src/helpers.rs:198-215: base^odd is 1 or -1, or one of its
+// next shift - 1 squares is -1. Arithmetic in Montgomery form; the results
+// compare against R and -R.
+static bool strong_round(const FpCtx &c, u128 q, u128 base) {
   u128 qm1 = q - 1;
   int shift = 0;
   while (((qm1 >> shift) & 1) == 0) shift++;
-  u128 w = powmod(base, qm1 >> shift, q);
-  if (w == 1 || w == qm1) return true;
+  u128 e = qm1 >> shift;
+  fp b = fp_mul(fp{(uint64_t)(base % q), (uint64_t)((base % q) >> 64)}, c.r2, c);
+  fp w = c.one;
+  for (int i = 127; i >= 0; i--) {
+    w = fp_mul(w, w, c);
+    if ((e >> i) & 1) w = fp_mul(w, b, c);
+  }
+  u128 one = to_u128(c.one), minus_one = q - one;
+  if (to_u128(w) == one || to_u128(w) == minus_one) return true;
   for (int r = 1; r < shift; r++) {
-    w = mulmod(w, w, q);
-    if (w == qm1) return true;
+    w = fp_mul(w, w, c);
+    if (to_u128(w) == minus_one) return true;
   }
   return false;
 }
@@ -153,6 +111,7 @@ u128 Transcript::prime(uint32_t bits) {
     }
     if (!decided) {
       prime = true;
+      FpCtx ctx = candidate_ctx(cand);
       u128 bound = cand - 3;
       u128 b = bound - 1;
       int lz = 0;
@@ -163,7 +122,7 @@ u128 Transcript::prime(uint32_t bits) {
         do {
           c = challenge_u128() & mask;
         } while (c >= bound);
-        if (!strong_round(cand, 2 + c)) prime = false;
+        if (!strong_round(ctx, cand, 2 + c)) prime = false;
       }
     }
     if (prime) return cand;

@@ -103,14 +103,31 @@ class Transcript {
   const std::vector<uint8_t> &hints() const { return hints_; }
 
  private:
+  // Duplex absorb: XOR into the rate, permuting when it fills. Whole
+  // little-endian lanes go in eight bytes at a time once aligned.
   void absorb(const uint8_t *in, size_t n) {
-    for (size_t i = 0; i < n; i++) {
+    while (n) {
       if (absorb_pos_ == RATE) {
         keccak_f1600(st_);
         absorb_pos_ = 0;
       }
-      st_[absorb_pos_ / 8] ^= (uint64_t)in[i] << (8 * (absorb_pos_ % 8));
+      if ((absorb_pos_ & 7) == 0 && n >= 8) {
+        size_t lanes = (size_t)(RATE - absorb_pos_) / 8;
+        if (lanes > n / 8) lanes = n / 8;
+        for (size_t i = 0; i < lanes; i++) {
+          uint64_t v;
+          memcpy(&v, in, 8);
+          st_[absorb_pos_ / 8] ^= v;
+          absorb_pos_ += 8;
+          in += 8;
+        }
+        n -= lanes * 8;
+        continue;
+      }
+      st_[absorb_pos_ / 8] ^= (uint64_t)*in << (8 * (absorb_pos_ % 8));
       absorb_pos_++;
+      in++;
+      n--;
     }
     squeeze_pos_ = RATE;
   }

@@ -25,6 +25,10 @@ extern "C" {
 /* ------------------------------------------------------------------ errors */
 const char *bitz_last_error(void);
 int bitz_device_count(void);
+/* Selects the device this library's calls use (one process per GPU); call it
+ * before the first other call. No reference counterpart: the reference is
+ * CPU-only. */
+int bitz_set_device(int device);
 
 /* -------------------------------------------------------------- transcript
  * The prover half of the Fiat-Shamir transcript.
@@ -100,10 +104,19 @@ int bitz_system_stats(const bitz_system *sys, uint64_t out[8]);
  * benchmark::run times, tooling/cli/src/benchmark.rs:28-79). Returns the
  * proof bytes root || Spartan section || bitzPCS wire container
  * (crates/host/src/wire_proof.rs:88-104) in a buffer freed with bitz_free,
- * and the stage times in milliseconds (witness, commit, prove).
- * BZ_ERR_UNSATISFIED when the statement is false (Error::Unsatisfied). */
-int bitz_system_prove(bitz_system *sys, uint8_t **proof, size_t *proof_len, double times_ms[3]);
+ * and the times in milliseconds: witness, commit, prove (host clock) and the
+ * CUDA-event span of the whole proof on the prover's stream.
+ * BZ_ERR_UNSATISFIED when the statement is false (Error::Unsatisfied).
+ * The statement is copied from host memory on every call. */
+int bitz_system_prove(bitz_system *sys, uint8_t **proof, size_t *proof_len, double times_ms[4]);
+/* As bitz_system_prove; with restage = 0 the statement staged on the device
+ * when the system was created is reused instead of copied again. */
+int bitz_system_prove_ex(bitz_system *sys, int restage, uint8_t **proof, size_t *proof_len,
+                         double times_ms[4]);
 void bitz_free(void *p);
+/* Diagnostic (no reference counterpart): kernel launches issued by this
+ * library since the process started. */
+unsigned long long bitz_launch_count(void);
 /* Diagnostic (no reference counterpart): the last proof's packed witness f,
  * packed h = M (1 || f) and the exact products (A h, B h, C h per row). */
 int bitz_system_witness(bitz_system *sys, uint32_t *f_words, size_t f_cap, uint32_t *h_words,

@@ -10,8 +10,8 @@ import numpy as np
 import pytest
 
 from bitz_b200 import _lib
-import circuit_inputs as ci
-import oracle_ffi as of
+from bitz_b200 import statements as ci
+from oracle import ffi as of
 
 CASES = [("sha256-compression", 1), ("sha256-chain", 1), ("sha256-chain", 3),
          ("sha256-block-aligned", 0), ("sha256-block-aligned", 2)]

@@ -7,8 +7,8 @@ import numpy as np
 import pytest
 
 import bitz_b200 as bz
-import circuit_inputs as ci
-import oracle_ffi as of
+from bitz_b200 import statements as ci
+from oracle import ffi as of
 
 pytestmark = pytest.mark.gpu
 

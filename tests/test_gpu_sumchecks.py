@@ -6,7 +6,7 @@ import numpy as np
 import pytest
 
 import bitz_b200 as bz
-import oracle_ffi as of
+from oracle import ffi as of
 
 pytestmark = pytest.mark.gpu
 

@@ -14,7 +14,7 @@ import os
 import numpy as np
 import pytest
 
-import oracle_ffi as of
+from oracle import ffi as of
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 

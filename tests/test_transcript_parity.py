@@ -5,7 +5,7 @@ import numpy as np
 import pytest
 
 import bitz_b200 as bz
-import oracle_ffi as of
+from oracle import ffi as of
 
 
 @pytest.mark.parametrize("seed", [0, 1, 2])
