@@ -296,7 +296,7 @@ void ProofSystem::stage_statement(cudaStream_t s) {
   states_.upload(states_h_.data(), states_h_.size(), s);
   msgs_.upload(msgs_h_.data(), msgs_h_.size(), s);
   offsets_.upload(dev_->host->block_f_offset.data(), dev_->host->block_f_offset.size(), s);
-  fin_.upload(fin_h_.data(), std::max<size_t>(fin_h_.size(), 1), s);
+  if (!fin_h_.empty()) fin_.upload(fin_h_.data(), fin_h_.size(), s);  // empty message: no inputs
   bit_c_.upload(bitc_h_.data(), bitc_h_.size(), s);
 }
 
@@ -659,7 +659,10 @@ int ProofSystem::prove_after_commit(cudaStream_t s, std::vector<uint8_t> &proof)
   W.sp_part.resize(3 * kSMs * 8 + 16);
   W.sp_sums.resize(4);
   W.sp_tab.resize(dev_->ntab + 1);
-  d_bit_rows_.upload(bit_rows_.data(), std::max<size_t>(bit_rows_.size(), 1), s);
+  if (bit_rows_.empty())
+    d_bit_rows_.resize(1);
+  else
+    d_bit_rows_.upload(bit_rows_.data(), bit_rows_.size(), s);
   SpartanScratch sc;
   for (int i = 0; i < 8; i++) sc.t[i] = W.sp_t.get() + i * R;
   for (int i = 0; i < 4; i++) sc.d[i] = W.sp_d.get() + i * Cn;
