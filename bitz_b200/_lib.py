@@ -32,6 +32,8 @@ SIGNATURES = [
      [_u64p, ctypes.c_int, _u64p, ctypes.c_int, _u64p, _u64p, ctypes.c_uint32, _vp, _u64p, _u64p]),
     ("bitz_post_gkr_prove_dev", ctypes.c_int,
      [_vp, ctypes.c_int, _vp, ctypes.c_int, _u64p, _vp, ctypes.c_uint32, _vp, _u64p, _u64p]),
+    ("bitz_post_gkr_prove_noalloc", ctypes.c_int,
+     [_vp, ctypes.c_int, _vp, ctypes.c_int, _u64p, _vp, ctypes.c_uint32, _vp, _vp, _u64p, _u64p]),
     ("bitz_gkr_prove", ctypes.c_int,
      [_u64p, _u64p, ctypes.c_int, _u64p, ctypes.c_uint32, _vp, _u64p, _u64p]),
     ("bitz_gkr_prove_dev", ctypes.c_int,

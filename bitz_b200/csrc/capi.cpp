@@ -199,6 +199,37 @@ int bitz_post_gkr_prove_dev(const uint64_t *rows_dev, int log_rows, const uint64
   });
 }
 
+int bitz_post_gkr_prove_noalloc(const uint64_t *rows_dev, int log_rows, const uint64_t *cols_dev,
+                                int log_cols, const uint64_t target[2], const uint64_t *packed_dev,
+                                uint32_t security_bits, bitz_transcript *t, void *stream,
+                                uint64_t *point_out, uint64_t value_out[2]) {
+  if (!rows_dev || !cols_dev || !target || !packed_dev || !t || !point_out || !value_out)
+    return fail(BZ_ERR_ARGUMENT, "null argument");
+  if (int rc = check_post_gkr_args(log_rows, log_cols, security_bits)) return rc;
+  return guarded([&] {
+    PostGkrArgs a;
+    a.rows = (const f128 *)rows_dev;
+    a.log_rows = log_rows;
+    a.cols = (const f128 *)cols_dev;
+    a.log_cols = log_cols;
+    a.packed = (const f128 *)packed_dev;
+    a.target = mk(target[0], target[1]);
+    a.grind_bits = grinding_bits(security_bits, 2);
+    f128 point[64], value;
+    std::string err;
+    int rc = post_gkr_prove_noalloc(a, t->t, (cudaStream_t)stream, point, &value, err);
+    if (rc == BZ_ERR_CLAIM) return fail(rc, "claim does not hold");
+    if (rc != BZ_OK) return fail(rc, err.empty() ? "post-GKR failed" : err);
+    for (int i = 0; i < log_rows + log_cols; i++) {
+      point_out[2 * i] = point[i].lo;
+      point_out[2 * i + 1] = point[i].hi;
+    }
+    value_out[0] = value.lo;
+    value_out[1] = value.hi;
+    return BZ_OK;
+  });
+}
+
 // ------------------------------------------------------------------ GKR
 
 static int gkr_common(const f128 *images, const f128 *columns, int log_cols, const uint64_t *zeta,

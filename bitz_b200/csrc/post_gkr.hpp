@@ -2,6 +2,8 @@
 #pragma once
 #include <cuda_runtime.h>
 
+#include <string>
+
 #include "status.hpp"
 #include "transcript.hpp"
 
@@ -38,5 +40,10 @@ void quad_fold(const f128 *w, const f128 *v, f128 r, f128 *w2, f128 *v2, size_t 
 // closing evaluation to value_out, appending every message to `ts`.
 int post_gkr_prove(const PostGkrArgs &a, Transcript &ts, PostGkrScratch &sc, cudaStream_t s,
                    f128 *point_out, f128 *value_out);
+
+// The same reduction on fixed file-scope device scratch: allocates nothing.
+// Claims up to 2^20 bits; see post_gkr_noalloc.cu for the sharing rules.
+int post_gkr_prove_noalloc(const PostGkrArgs &a, Transcript &ts, cudaStream_t s, f128 *point_out,
+                           f128 *value_out, std::string &err);
 
 }  // namespace bz

@@ -68,6 +68,23 @@ int bitz_post_gkr_prove_dev(const uint64_t *rows_dev, int log_rows, const uint64
                             uint32_t security_bits, bitz_transcript *t, uint64_t *point_out,
                             uint64_t value_out[2]);
 
+/* The post-GKR sumcheck as bitz_post_gkr_prove_dev, allocating nothing.
+ * No counterpart in the reference. For callers that cannot allocate device
+ * memory: code running inside a CUDA graph capture (where cudaMalloc is not
+ * allowed), processes whose device memory belongs to another allocator or to
+ * a fixed budget set aside at start-up, and embedders that forbid allocation
+ * on the request path. Inputs are device pointers, outputs host pointers;
+ * stream may be NULL (the default stream). Its scratch is a fixed array in
+ * the library's device memory (32 MiB on every GPU that loads the library,
+ * held until the process exits), so log_rows + log_cols must be at most 20:
+ * larger claims return BZ_ERR_SCRATCH. Every call shares that array: calls
+ * that overlap on the GPU race, so serialise them. The first call on a
+ * device looks up the array's address; make it before any stream capture. */
+int bitz_post_gkr_prove_noalloc(const uint64_t *rows_dev, int log_rows, const uint64_t *cols_dev,
+                                int log_cols, const uint64_t target[2], const uint64_t *packed_dev,
+                                uint32_t security_bits, bitz_transcript *t, void *stream,
+                                uint64_t *point_out, uint64_t value_out[2]);
+
 /* ------------------------------------------------------- grand-product GKR
  * Replaces gkr::grand_product + gkr::gpgkr_prove (crates/gkr/src/lib.rs:785,24)
  * for a table of 2^log_cols columns of 128 bits (one packed word per column)
