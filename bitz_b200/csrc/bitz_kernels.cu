@@ -206,14 +206,14 @@ __global__ void k_packed_basis(const f128 *__restrict__ suffix, size_t n,
 
 // sum_y a[y] * b[y], XOR-reduced into acc[0..2).
 __global__ void k_dot(const f128 *__restrict__ a, const f128 *__restrict__ b, size_t n,
-                      unsigned long long *acc) {
+                      unsigned long long *acc, Publish pub) {
   wide s = wzero();
   for (size_t y = blockIdx.x * (size_t)blockDim.x + threadIdx.x; y < n;
        y += (size_t)gridDim.x * blockDim.x)
     wacc(s, gmul_wide(ld(a + y), ld(b + y)));
   f128 r = greduce(s);
   uint64_t v[2] = {r.lo, r.hi};
-  block_xor_atomic<2>(v, acc);
+  block_xor_publish<2>(v, acc, pub);
 }
 
 __global__ void k_axpy(f128 *__restrict__ y, f128 a, const f128 *__restrict__ x, size_t n) {
@@ -241,8 +241,9 @@ void packed_basis(const f128 *suffix, size_t n, const f128 *bw, const f128 *eq_o
   BZ_LAUNCH_CHECK();
 }
 
-void dot(const f128 *a, const f128 *b, size_t n, unsigned long long *acc, cudaStream_t s) {
-  k_dot<<<grid_for(n), kThreads, 0, s>>>(a, b, n, acc);
+void dot(const f128 *a, const f128 *b, size_t n, unsigned long long *acc, Publish pub,
+         cudaStream_t s) {
+  k_dot<<<grid_for(n), kThreads, 0, s>>>(a, b, n, acc, pub);
   BZ_LAUNCH_CHECK();
 }
 

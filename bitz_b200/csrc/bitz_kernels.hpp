@@ -2,6 +2,7 @@
 #pragma once
 #include <cuda_runtime.h>
 
+#include "device.cuh"
 #include "transcript.hpp"
 
 namespace bz {
@@ -20,7 +21,8 @@ void packed_basis(const f128 *suffix, size_t n, const f128 *bw, const f128 *eq_o
                   f128 *basis, cudaStream_t s);
 // y += a * x
 void axpy(f128 *y, f128 a, const f128 *x, size_t n, cudaStream_t s);
-void dot(const f128 *a, const f128 *b, size_t n, unsigned long long *acc, cudaStream_t s);
+void dot(const f128 *a, const f128 *b, size_t n, unsigned long long *acc, Publish pub,
+         cudaStream_t s);
 void rs_encode(const f128 *msg, int log_n, int k, int rate, const f128 *wh, f128 *cw,
                cudaStream_t s);
 void merkle_build(const f128 *cw, size_t rows, int k, uint32_t *nodes, cudaStream_t s);

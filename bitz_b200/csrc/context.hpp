@@ -57,6 +57,7 @@ class Context {
   static Context &get();
 
   cudaStream_t stream() const { return stream_; }
+  RoundChannel *channel() { return &channel_; }
 
   PostGkrScratch &post_gkr_scratch(size_t entries) {
     if (pg_.capacity < entries) {
@@ -102,6 +103,8 @@ class Context {
   uint64_t *host_ = nullptr;
   GkrScratch gk_;
   DeviceBuffer<f128> gk_layers_, gk_eq_, gk_eq_scratch_, gk_pair_;
+  RoundChannel channel_;
+  DeviceBuffer<unsigned int> counter_;
 };
 
 }  // namespace bz

@@ -45,7 +45,45 @@ inline int grid_for(size_t work, int per_block = kThreads, int max_blocks = kSMs
   return (int)b;
 }
 
+// A round's result delivered without a copy or a stream sync: the last block
+// of the kernel moves the accumulated words into host-mapped pinned memory
+// and then publishes a sequence number the host polls.
+struct Mailbox {
+  volatile unsigned long long seq;
+  unsigned long long pad[7];
+  unsigned long long payload[8];
+};
+
+// Where a round kernel publishes: counter counts finished blocks (reset by
+// the last one); a null counter disables publishing.
+struct Publish {
+  unsigned int *counter;
+  Mailbox *mailbox;  // device view of the mapped mailbox
+  unsigned long long seq;
+};
+
 #if defined(__CUDACC__)
+// Called by every thread after the block's atomics (issued by thread 0):
+// the last block to finish reads and clears the N accumulator words, writes
+// them to the mailbox, then the sequence number.
+template <int N>
+__device__ __forceinline__ void publish(unsigned long long *acc, const Publish &p) {
+  if (!p.counter) return;
+  if (threadIdx.x == 0) {
+    __threadfence();
+    unsigned int prev = atomicAdd(p.counter, 1u);
+    if (prev == gridDim.x - 1) {
+      __threadfence();
+#pragma unroll
+      for (int k = 0; k < N; k++) p.mailbox->payload[k] = atomicExch(acc + k, 0ull);
+      *p.counter = 0;
+      __threadfence_system();
+      p.mailbox->seq = p.seq;
+      __threadfence_system();
+    }
+  }
+}
+
 // XOR-reduce `n` 64-bit words across the block and fold the block's result
 // into `acc` with atomicXor. XOR is associative and commutative, so the total
 // is the same whatever the order the blocks land in.
@@ -73,6 +111,14 @@ __device__ __forceinline__ void block_xor_atomic(uint64_t (&v)[N], unsigned long
       if (lane == 0 && x) atomicXor(acc + k, (unsigned long long)x);
     }
   }
+}
+
+// block_xor_atomic, then publish the totals when this is the last block.
+template <int N>
+__device__ __forceinline__ void block_xor_publish(uint64_t (&v)[N], unsigned long long *acc,
+                                                  const Publish &p) {
+  block_xor_atomic<N>(v, acc);
+  publish<N>(acc, p);
 }
 
 // Sum `N` prime-field values across the block (mod q) and write the block's
@@ -114,6 +160,22 @@ __device__ __forceinline__ void block_fp_sum(fp (&v)[N], const FpCtx &c, fp *out
   }
 }
 
+#endif
+
+// Host side of a mailbox: one mapped pinned page, a device counter, and the
+// next sequence number. wait() polls with a time limit and surfaces any
+// stream error instead of spinning on a failed kernel.
+struct RoundChannel {
+  Mailbox *host = nullptr;  // host view
+  Mailbox *dev = nullptr;   // device view
+  unsigned int *counter = nullptr;
+  unsigned long long next = 0;
+  Publish arm() { return Publish{counter, dev, ++next}; }
+  // Waits for the publication armed last; copies n payload words.
+  void wait(cudaStream_t s, uint64_t *out, int n);
+};
+
+#if defined(__CUDACC__)
 __device__ __forceinline__ f128 ld(const f128 *p) {
   ulonglong2 v = *reinterpret_cast<const ulonglong2 *>(p);
   return mk(v.x, v.y);

@@ -40,7 +40,8 @@ __global__ void gkr_parent(const f128 *__restrict__ child, size_t half, f128 *__
 
 // Round i's sums (round_sums, lib.rs:164-216) before any bind: the top round.
 __global__ void gkr_top_sums(const f128 *__restrict__ c, size_t n_half, size_t h,
-                             const f128 *__restrict__ eq, int at_one, unsigned long long *acc) {
+                             const f128 *__restrict__ eq, int at_one, unsigned long long *acc,
+                             Publish pub) {
   const f128 *L = c, *R = c + n_half;
   wide sb = wzero(), si = wzero();
   for (size_t x = blockIdx.x * (size_t)blockDim.x + threadIdx.x; x < h;
@@ -53,13 +54,14 @@ __global__ void gkr_top_sums(const f128 *__restrict__ c, size_t n_half, size_t h
   }
   f128 a = greduce(sb), b = greduce(si);
   uint64_t v[4] = {a.lo, a.hi, b.lo, b.hi};
-  block_xor_atomic<4>(v, acc);
+  block_xor_publish<4>(v, acc, pub);
 }
 
 // Bind round i+1 at r (halves of 2^(i+1)), derive eq_i in place, and sum
 // round i (halves of 2^i). Thread x < 2^i owns entries x and x + 2^i.
 __global__ void gkr_bind_sums(f128 *__restrict__ c, size_t n_half, size_t h, f128 r,
-                              f128 *__restrict__ eq, int at_one, unsigned long long *acc) {
+                              f128 *__restrict__ eq, int at_one, unsigned long long *acc,
+                              Publish pub) {
   f128 *L = c, *R = c + n_half;
   const size_t h2 = 2 * h;
   wide sb = wzero(), si = wzero();
@@ -83,16 +85,44 @@ __global__ void gkr_bind_sums(f128 *__restrict__ c, size_t n_half, size_t h, f12
   }
   f128 a = greduce(sb), b = greduce(si);
   uint64_t v[4] = {a.lo, a.hi, b.lo, b.hi};
-  block_xor_atomic<4>(v, acc);
+  block_xor_publish<4>(v, acc, pub);
 }
 
-// The bind after round 0: one pair left in each half.
-__global__ void gkr_final_bind(const f128 *__restrict__ c, size_t n_half, f128 r, f128 *out) {
+// The bind after round 0: one pair left in each half. Delivered through the
+// mailbox when publishing, else to out[0..2).
+__global__ void gkr_final_bind(const f128 *__restrict__ c, size_t n_half, f128 r, f128 *out,
+                               Publish pub) {
   if (threadIdx.x == 0 && blockIdx.x == 0) {
     f128 l0 = ld(c), l1 = ld(c + 1), r0 = ld(c + n_half), r1 = ld(c + n_half + 1);
-    st(out, gadd(l0, gmul(r, gadd(l1, l0))));
-    st(out + 1, gadd(r0, gmul(r, gadd(r1, r0))));
+    f128 lr = gadd(l0, gmul(r, gadd(l1, l0)));
+    f128 rr = gadd(r0, gmul(r, gadd(r1, r0)));
+    if (pub.counter) {
+      pub.mailbox->payload[0] = lr.lo;
+      pub.mailbox->payload[1] = lr.hi;
+      pub.mailbox->payload[2] = rr.lo;
+      pub.mailbox->payload[3] = rr.hi;
+      __threadfence_system();
+      pub.mailbox->seq = pub.seq;
+      __threadfence_system();
+    } else {
+      st(out, lr);
+      st(out + 1, rr);
+    }
   }
+}
+
+static Publish arm(GkrScratch &sc) {
+  return sc.channel ? sc.channel->arm() : Publish{nullptr, nullptr, 0};
+}
+
+// The round's four words, from the mailbox or by a copy of `src`.
+static void round_read(GkrScratch &sc, const void *src, cudaStream_t s) {
+  if (sc.channel) {
+    sc.channel->wait(s, sc.host, 4);
+    return;
+  }
+  BZ_CUDA(cudaMemcpyAsync(sc.host, src, 32, cudaMemcpyDeviceToHost, s));
+  BZ_CUDA(cudaStreamSynchronize(s));
 }
 
 void gkr_build(const f128 *cols, int s, const f128 *images, GkrScratch &sc, cudaStream_t st_) {
@@ -125,13 +155,12 @@ f128 gkr_prove(int s, const f128 *zeta, uint32_t grind_bits, Transcript &ts, Gkr
     eq_table_device(point, n - 1, sc.eq, sc.eq_scratch, st_);
     size_t h = n_half / 2;
     gkr_top_sums<<<grid_for(h), kThreads, 0, st_>>>(c, n_half, h, sc.eq,
-                                                    gis_zero(point[n - 1]), sc.acc);
+                                                    gis_zero(point[n - 1]), sc.acc, arm(sc));
     BZ_LAUNCH_CHECK();
     f128 eq_bound = mk(1, 0);
     for (int i = n - 1; i >= 0; i--) {
       unsigned long long *acc = sc.acc + 4 * (n - 1 - i);
-      BZ_CUDA(cudaMemcpyAsync(sc.host, acc, 32, cudaMemcpyDeviceToHost, st_));
-      BZ_CUDA(cudaStreamSynchronize(st_));
+      round_read(sc, acc, st_);
       f128 sb = mk(sc.host[0], sc.host[1]), si = mk(sc.host[2], sc.host[3]);
       f128 msg[2] = {gmul(eq_bound, sb), gmul(eq_bound, si)};
       ts.prover_message(msg, 32);
@@ -142,16 +171,16 @@ f128 gkr_prove(int s, const f128 *zeta, uint32_t grind_bits, Transcript &ts, Gkr
       if (i > 0) {
         size_t hh = (size_t)1 << (i - 1);
         gkr_bind_sums<<<grid_for(hh), kThreads, 0, st_>>>(c, n_half, hh, r, sc.eq,
-                                                          gis_zero(point[i - 1]), acc + 4);
+                                                          gis_zero(point[i - 1]), acc + 4, arm(sc));
         BZ_LAUNCH_CHECK();
       } else {
-        gkr_final_bind<<<1, 32, 0, st_>>>(c, n_half, r, sc.pair);
+        gkr_final_bind<<<1, 32, 0, st_>>>(c, n_half, r, sc.pair, arm(sc));
         BZ_LAUNCH_CHECK();
       }
     }
     f128 lr[2];
-    BZ_CUDA(cudaMemcpyAsync(lr, sc.pair, 32, cudaMemcpyDeviceToHost, st_));
-    BZ_CUDA(cudaStreamSynchronize(st_));
+    round_read(sc, sc.pair, st_);
+    memcpy(lr, sc.host, 32);
     ts.prover_message(lr, 32);
     f128 t = ts.challenge_f128();
     next[n] = t;

@@ -2,6 +2,7 @@
 #pragma once
 #include <cuda_runtime.h>
 
+#include "device.cuh"
 #include "status.hpp"
 #include "transcript.hpp"
 
@@ -15,6 +16,7 @@ struct GkrScratch {
   f128 *pair = nullptr;               // 2 entries
   unsigned long long *acc = nullptr;  // 4 words per round
   uint64_t *host = nullptr;           // pinned, 4 words
+  RoundChannel *channel = nullptr;    // mailbox for round results; null: copy + sync
 };
 
 // Builds every layer from the packed columns (2^s F128, bit b of column c is

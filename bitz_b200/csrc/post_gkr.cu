@@ -20,7 +20,7 @@ namespace bz {
 // weights as one contiguous 2 KiB run.
 __global__ void pg_first_message(const f128 *__restrict__ rows, int log_rows,
                                  const f128 *__restrict__ cols, const f128 *__restrict__ packed,
-                                 size_t npacked, unsigned long long *acc) {
+                                 size_t npacked, unsigned long long *acc, Publish pub) {
   const int lane = threadIdx.x & 31;
   const size_t warp = (blockIdx.x * (size_t)blockDim.x + threadIdx.x) >> 5;
   const size_t nwarps = (gridDim.x * (size_t)blockDim.x) >> 5;
@@ -65,7 +65,7 @@ __global__ void pg_first_message(const f128 *__restrict__ rows, int log_rows,
   }
   f128 r0 = greduce(a0), r2 = greduce(a2), rw = greduce(ws);
   uint64_t v[6] = {r0.lo, r0.hi, r2.lo, r2.hi, rw.lo, rw.hi};
-  block_xor_atomic<6>(v, acc);
+  block_xor_publish<6>(v, acc, pub);
 }
 
 // Round 1's fold: W'[c * R/2 + k] = cols[c] * fold(rows)[k] and V' the bound
@@ -74,7 +74,7 @@ __global__ void pg_first_message(const f128 *__restrict__ rows, int log_rows,
 __global__ void pg_first_fold(const f128 *__restrict__ rows, int log_rows,
                               const f128 *__restrict__ cols, const f128 *__restrict__ packed,
                               f128 r, f128 *__restrict__ w_out, f128 *__restrict__ v_out,
-                              size_t npairs_out, unsigned long long *acc) {
+                              size_t npairs_out, unsigned long long *acc, Publish pub) {
   const size_t half_rows = (size_t)1 << (log_rows - 1);
   const f128 vals[4] = {mk(0, 0), mk(r.lo ^ 1, r.hi), r, mk(1, 0)};
   wide a0 = wzero(), a2 = wzero();
@@ -101,7 +101,7 @@ __global__ void pg_first_fold(const f128 *__restrict__ rows, int log_rows,
   }
   f128 r0 = greduce(a0), r2 = greduce(a2);
   uint64_t v[4] = {r0.lo, r0.hi, r2.lo, r2.hi};
-  block_xor_atomic<4>(v, acc);
+  block_xor_publish<4>(v, acc, pub);
 }
 
 // A quadratic round (sumcheck.rs:63-95,198-215): fold W and V at r (entry =
@@ -109,7 +109,7 @@ __global__ void pg_first_fold(const f128 *__restrict__ rows, int log_rows,
 // pairs. With emit == 0 only the fold runs (the last round).
 __global__ void pg_round(const f128 *__restrict__ w_in, const f128 *__restrict__ v_in, f128 r,
                          f128 *__restrict__ w_out, f128 *__restrict__ v_out, size_t nout,
-                         int emit, unsigned long long *acc) {
+                         int emit, unsigned long long *acc, Publish pub) {
   wide a0 = wzero(), a2 = wzero();
   const size_t npairs = (nout + 1) / 2;
   for (size_t j = blockIdx.x * (size_t)blockDim.x + threadIdx.x; j < npairs;
@@ -137,13 +137,13 @@ __global__ void pg_round(const f128 *__restrict__ w_in, const f128 *__restrict__
   if (emit) {
     f128 r0 = greduce(a0), r2 = greduce(a2);
     uint64_t v[4] = {r0.lo, r0.hi, r2.lo, r2.hi};
-    block_xor_atomic<4>(v, acc);
+    block_xor_publish<4>(v, acc, pub);
   }
 }
 
 // (a0, a2) over the pairs of W and V as they are (no fold).
 __global__ void pg_sums(const f128 *__restrict__ w, const f128 *__restrict__ v, size_t n,
-                        unsigned long long *acc) {
+                        unsigned long long *acc, Publish pub) {
   wide a0 = wzero(), a2 = wzero();
   for (size_t j = blockIdx.x * (size_t)blockDim.x + threadIdx.x; j < n / 2;
        j += (size_t)gridDim.x * blockDim.x) {
@@ -153,19 +153,20 @@ __global__ void pg_sums(const f128 *__restrict__ w, const f128 *__restrict__ v, 
   }
   f128 r0 = greduce(a0), r2 = greduce(a2);
   uint64_t o[4] = {r0.lo, r0.hi, r2.lo, r2.hi};
-  block_xor_atomic<4>(o, acc);
+  block_xor_publish<4>(o, acc, pub);
 }
 
-void quad_sums(const f128 *w, const f128 *v, size_t n, unsigned long long *acc, cudaStream_t s) {
-  pg_sums<<<grid_for(n / 2), kThreads, 0, s>>>(w, v, n, acc);
+void quad_sums(const f128 *w, const f128 *v, size_t n, unsigned long long *acc, Publish pub,
+               cudaStream_t s) {
+  pg_sums<<<grid_for(n / 2), kThreads, 0, s>>>(w, v, n, acc, pub);
   BZ_LAUNCH_CHECK();
 }
 
 void quad_fold(const f128 *w, const f128 *v, f128 r, f128 *w2, f128 *v2, size_t n, int emit,
-               unsigned long long *acc, cudaStream_t s) {
+               unsigned long long *acc, Publish pub, cudaStream_t s) {
   size_t nout = n / 2;
   pg_round<<<grid_for((nout + 1) / 2), kThreads, 0, s>>>(w, v, r, w2, v2, nout, emit && nout >= 2,
-                                                         acc);
+                                                         acc, pub);
   BZ_LAUNCH_CHECK();
 }
 
@@ -174,9 +175,19 @@ static f128 advance(f128 claim, f128 a0, f128 a2, f128 r) {
   return gadd(a0, gmul(r, gadd(gadd(claim, a2), gmul(r, a2))));
 }
 
-static void read_acc(const unsigned long long *d_acc, uint64_t *h_pinned, int words,
-                     cudaStream_t s) {
-  BZ_CUDA(cudaMemcpyAsync(h_pinned, d_acc, words * 8, cudaMemcpyDeviceToHost, s));
+// A round's result words: through the mailbox when the scratch has a
+// channel, else by a copy and a stream sync.
+static Publish arm(PostGkrScratch &sc) {
+  return sc.channel ? sc.channel->arm() : Publish{nullptr, nullptr, 0};
+}
+
+static void round_read(PostGkrScratch &sc, const unsigned long long *d_acc, int words,
+                       cudaStream_t s) {
+  if (sc.channel) {
+    sc.channel->wait(s, sc.host, words);
+    return;
+  }
+  BZ_CUDA(cudaMemcpyAsync(sc.host, d_acc, words * 8, cudaMemcpyDeviceToHost, s));
   BZ_CUDA(cudaStreamSynchronize(s));
 }
 
@@ -191,9 +202,9 @@ int post_gkr_prove(const PostGkrArgs &a, Transcript &ts, PostGkrScratch &sc, cud
   BZ_CUDA(cudaMemsetAsync(acc, 0, sizeof(unsigned long long) * 8 * (m + 2), s));
 
   pg_first_message<<<grid_for(npacked * 32), kThreads, 0, s>>>(a.rows, log_rows, a.cols,
-                                                                 a.packed, npacked, acc);
+                                                                 a.packed, npacked, acc, arm(sc));
   BZ_LAUNCH_CHECK();
-  read_acc(acc, sc.host, 6, s);
+  round_read(sc, acc, 6, s);
   f128 a0 = mk(sc.host[0], sc.host[1]), a2 = mk(sc.host[2], sc.host[3]);
   f128 wsum = mk(sc.host[4], sc.host[5]);
   if (!geq(wsum, a.target)) {
@@ -216,14 +227,14 @@ int post_gkr_prove(const PostGkrArgs &a, Transcript &ts, PostGkrScratch &sc, cud
     size_t npairs = n1 / 2;
     if (rounds >= 1) {
       pg_first_fold<<<grid_for(npairs), kThreads, 0, s>>>(a.rows, log_rows, a.cols, a.packed, r,
-                                                          w, v, npairs, acc1);
+                                                          w, v, npairs, acc1, arm(sc));
       BZ_LAUNCH_CHECK();
     }
   }
   size_t len = n1;
   for (int k = 0; k < rounds; k++) {
     unsigned long long *ak = acc + 8 * (k + 1);
-    read_acc(ak, sc.host, 4, s);
+    round_read(sc, ak, 4, s);
     f128 m0 = mk(sc.host[0], sc.host[1]), m2 = mk(sc.host[2], sc.host[3]);
     uint64_t mm[4] = {m0.lo, m0.hi, m2.lo, m2.hi};
     ts.prover_message(mm, 32);
@@ -234,7 +245,8 @@ int post_gkr_prove(const PostGkrArgs &a, Transcript &ts, PostGkrScratch &sc, cud
     size_t nout = len / 2;
     int emit = nout >= 2;
     pg_round<<<grid_for((nout + 1) / 2), kThreads, 0, s>>>(w, v, rr, w2, v2, nout, emit,
-                                                           acc + 8 * (k + 2));
+                                                           acc + 8 * (k + 2),
+                                                           emit ? arm(sc) : Publish{nullptr, nullptr, 0});
     BZ_LAUNCH_CHECK();
     f128 *t = w;
     w = w2;

@@ -4,6 +4,7 @@
 
 #include <string>
 
+#include "device.cuh"
 #include "status.hpp"
 #include "transcript.hpp"
 
@@ -27,14 +28,16 @@ struct PostGkrScratch {
   unsigned long long *acc = nullptr;  // 8 words per round, 64 rounds
   uint64_t *host = nullptr;           // pinned, 8 words
   f128 claim_seen{0, 0};              // the weighted sum found when a claim fails
+  RoundChannel *channel = nullptr;    // mailbox for round results; null: copy + sync
 };
 
 // The quadratic sumcheck round of <W, V> (shared with the Ligerito folds):
 // quad_sums accumulates (a0, a2) over the pairs as they are; quad_fold folds
 // both tables at r and, with emit, accumulates the next round's sums.
-void quad_sums(const f128 *w, const f128 *v, size_t n, unsigned long long *acc, cudaStream_t s);
+void quad_sums(const f128 *w, const f128 *v, size_t n, unsigned long long *acc, Publish pub,
+               cudaStream_t s);
 void quad_fold(const f128 *w, const f128 *v, f128 r, f128 *w2, f128 *v2, size_t n, int emit,
-               unsigned long long *acc, cudaStream_t s);
+               unsigned long long *acc, Publish pub, cudaStream_t s);
 
 // Runs the whole reduction: writes t+s challenges to point_out and the
 // closing evaluation to value_out, appending every message to `ts`.

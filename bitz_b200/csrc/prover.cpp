@@ -430,9 +430,9 @@ int ProofSystem::commit(cudaStream_t s) {
     eq_table_device(ood_point_.data(), log_n, W.eq_ood.get(), W.eqs.get(), s);
     W.acc.resize(512);
     BZ_CUDA(cudaMemsetAsync(W.acc.get(), 0, 16, s));
-    dot(W.eq_ood.get(), fpk, n, W.acc.get(), s);
-    BZ_CUDA(cudaMemcpyAsync(W.host_acc, W.acc.get(), 16, cudaMemcpyDeviceToHost, s));
-    BZ_CUDA(cudaStreamSynchronize(s));
+    RoundChannel *ch = Context::get().channel();
+    dot(W.eq_ood.get(), fpk, n, W.acc.get(), ch->arm(), s);
+    ch->wait(s, W.host_acc, 2);
     ood_value_ = mk(W.host_acc[0], W.host_acc[1]);
     t.prover_f128(ood_value_);
   }
@@ -490,14 +490,14 @@ std::vector<uint8_t> ProofSystem::ligerito(cudaStream_t s, f128 target) {
   DeviceBuffer<uint32_t> next_nodes[2];
   int flip = 0;
   unsigned long long *acc = W.acc.get();
+  RoundChannel *ch = Context::get().channel();
   for (int i = 0; i < cfg.nlevels; i++) {
     const PcsLevel &L = cfg.levels[i];
     std::vector<f128> rs;
     BZ_CUDA(cudaMemsetAsync(acc, 0, 8 * sizeof(unsigned long long) * (L.k + 1), s));
-    quad_sums(b, f, n, acc, s);
+    quad_sums(b, f, n, acc, ch->arm(), s);
     for (int r = 0; r < L.k; r++) {
-      BZ_CUDA(cudaMemcpyAsync(W.host_acc, acc + 8 * r, 32, cudaMemcpyDeviceToHost, s));
-      BZ_CUDA(cudaStreamSynchronize(s));
+      ch->wait(s, W.host_acc, 4);
       f128 a0 = mk(W.host_acc[0], W.host_acc[1]), a2 = mk(W.host_acc[2], W.host_acc[3]);
       t.prover_f128(a0);
       t.prover_f128(a2);
@@ -505,7 +505,9 @@ std::vector<uint8_t> ProofSystem::ligerito(cudaStream_t s, f128 target) {
       f128 c = t.challenge_f128();
       rs.push_back(c);
       claim = gadd(a0, gmul(c, gadd(gadd(claim, a2), gmul(c, a2))));
-      quad_fold(b, f, c, b2, f2, n, r + 1 < L.k, acc + 8 * (r + 1), s);
+      bool more = r + 1 < L.k;
+      quad_fold(b, f, c, b2, f2, n, more, acc + 8 * (r + 1),
+                more ? ch->arm() : Publish{nullptr, nullptr, 0}, s);
       std::swap(f, f2);
       std::swap(b, b2);
       n /= 2;
@@ -533,9 +535,8 @@ std::vector<uint8_t> ProofSystem::ligerito(cudaStream_t s, f128 target) {
         W.eqs.resize(eq_scratch_entries(l));
         eq_table_device(pt.data(), l, W.eq.get(), W.eqs.get(), s);
         BZ_CUDA(cudaMemsetAsync(acc, 0, 16, s));
-        dot(W.eq.get(), f, n, acc, s);
-        BZ_CUDA(cudaMemcpyAsync(W.host_acc, acc, 16, cudaMemcpyDeviceToHost, s));
-        BZ_CUDA(cudaStreamSynchronize(s));
+        dot(W.eq.get(), f, n, acc, ch->arm(), s);
+        ch->wait(s, W.host_acc, 2);
         f128 v = mk(W.host_acc[0], W.host_acc[1]);
         t.prover_f128(v);
         f128 mu = t.challenge_f128();
@@ -671,6 +672,7 @@ int ProofSystem::prove_after_commit(cudaStream_t s, std::vector<uint8_t> &proof)
   sc.sums = W.sp_sums.get();
   sc.tab = W.sp_tab.get();
   sc.host = W.host_fp;
+  sc.channel = ctx.channel();
   SpartanArgs sa;
   sa.ctx = fc;
   sa.q = q;

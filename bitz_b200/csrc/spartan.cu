@@ -176,13 +176,24 @@ __global__ void k_inner_round(const fp *D, const fp *W, const uint32_t *hbits, i
   if (emit) block_fp_sum<2>(acc, c, partial);
 }
 
+// One block adds the per-block partials; the totals go to out and, when
+// publishing, to the mailbox (written by the thread that wrote out).
 template <int N>
-__global__ void k_fp_finalize(const fp *partial, int nblocks, FpCtx c, fp *out) {
+__global__ void k_fp_finalize(const fp *partial, int nblocks, FpCtx c, fp *out, Publish pub) {
   fp acc[N];
   for (int k = 0; k < N; k++) acc[k] = fp_zero();
   for (int b = threadIdx.x; b < nblocks; b += blockDim.x)
     for (int k = 0; k < N; k++) acc[k] = fp_add(acc[k], partial[b * N + k], c);
   block_fp_sum<N>(acc, c, out);
+  if (pub.counter && threadIdx.x == 0) {
+    for (int k = 0; k < N; k++) {
+      pub.mailbox->payload[2 * k] = out[k].lo;
+      pub.mailbox->payload[2 * k + 1] = out[k].hi;
+    }
+    __threadfence_system();
+    pub.mailbox->seq = pub.seq;
+    __threadfence_system();
+  }
 }
 
 // The coefficient table of the bind: scale_k * coefficient for every distinct
@@ -247,14 +258,19 @@ __global__ void k_bind_bits(const uint32_t *__restrict__ rows, int n, const fp *
 // ------------------------------------------------------------------- host
 
 static fp host_partial_sum(const fp *d_partial, int nblocks, int N, fp *d_out, fp *h_out,
-                           const FpCtx &c, cudaStream_t s) {
+                           const FpCtx &c, cudaStream_t s, RoundChannel *ch) {
+  Publish pub = ch ? ch->arm() : Publish{nullptr, nullptr, 0};
   if (N == 3)
-    k_fp_finalize<3><<<1, kThreads, 0, s>>>(d_partial, nblocks, c, d_out);
+    k_fp_finalize<3><<<1, kThreads, 0, s>>>(d_partial, nblocks, c, d_out, pub);
   else
-    k_fp_finalize<2><<<1, kThreads, 0, s>>>(d_partial, nblocks, c, d_out);
+    k_fp_finalize<2><<<1, kThreads, 0, s>>>(d_partial, nblocks, c, d_out, pub);
   BZ_LAUNCH_CHECK();
-  BZ_CUDA(cudaMemcpyAsync(h_out, d_out, N * sizeof(fp), cudaMemcpyDeviceToHost, s));
-  BZ_CUDA(cudaStreamSynchronize(s));
+  if (ch) {
+    ch->wait(s, reinterpret_cast<uint64_t *>(h_out), 2 * N);
+  } else {
+    BZ_CUDA(cudaMemcpyAsync(h_out, d_out, N * sizeof(fp), cudaMemcpyDeviceToHost, s));
+    BZ_CUDA(cudaStreamSynchronize(s));
+  }
   return h_out[0];
 }
 
@@ -313,7 +329,7 @@ void spartan_prove(const SpartanArgs &a, Transcript &ts, SpartanScratch &sc, cud
     int g = grid_for(npairs);
     k_outer_round<<<g, kThreads, 0, s>>>(E, A, B, C, E2, A2, B2, C2, len, fold, 1, r, c, sc.partial);
     BZ_LAUNCH_CHECK();
-    host_partial_sum(sc.partial, g, 3, sc.sums, sc.host, c, s);
+    host_partial_sum(sc.partial, g, 3, sc.sums, sc.host, c, s, sc.channel);
     if (fold) {
       std::swap(E, E2);
       std::swap(A, A2);
@@ -377,7 +393,7 @@ void spartan_prove(const SpartanArgs &a, Transcript &ts, SpartanScratch &sc, cud
     k_inner_round<<<g, kThreads, 0, s>>>(D, W, a.hbits, w_bits, D2, W2, len, fold, 1, r, c,
                                          sc.partial);
     BZ_LAUNCH_CHECK();
-    host_partial_sum(sc.partial, g, 2, sc.sums, sc.host, c, s);
+    host_partial_sum(sc.partial, g, 2, sc.sums, sc.host, c, s, sc.channel);
     if (fold) {
       std::swap(D, D2);
       std::swap(W, W2);

@@ -4,6 +4,7 @@
 
 #include <vector>
 
+#include "device.cuh"
 #include "transcript.hpp"
 
 namespace bz {
@@ -40,6 +41,7 @@ struct SpartanScratch {
   fp *sums;        // device, 3 entries
   fp *tab;         // coefficient table, ntab entries
   fp *host;        // pinned, 4 entries
+  RoundChannel *channel = nullptr;  // mailbox for round results; null: copy + sync
 };
 
 struct SpartanOut {
