@@ -8,6 +8,9 @@ holding (lo, hi) in the reference's GF(2^128) basis.
   crates/transcript/src/prover.rs:10-84.
 - ``post_gkr_prove``: crates/post_gkr/src/lib.rs:85 (post_gkr::prove).
 - ``gkr_prove``: crates/gkr/src/lib.rs:24,785 (grand_product + gpgkr_prove).
+- ``CircuitProofSystem``: tooling/cli/src/end_to_end.rs:150-336.
+- ``batch_prove`` / ``ProveServer``: many proofs at once on prover lanes (no
+  reference counterpart; the reference proves one statement per call).
 """
 import ctypes
 
@@ -16,13 +19,15 @@ import numpy as np
 from . import _lib
 
 __all__ = ["BitzError", "ProverState", "build_prover", "post_gkr_prove", "gkr_prove",
-           "gkr_outputs", "device_count"]
+           "gkr_outputs", "device_count", "CircuitProofSystem", "batch_prove", "ProveServer",
+           "probe_kernel", "probe_read", "l2_flush"]
 
 _ERRORS = {
     1: "ArgumentError", 2: "ClaimDoesNotHold", 3: "Unsatisfied", 4: "Configuration",
     5: "CudaError", 6: "Internal", 7: "Scratch", 8: "VerifyError", 9: "MalformedProof",
-    10: "NoDevice",
+    10: "NoDevice", 11: "Pending",
 }
+PENDING = 11
 
 
 class BitzError(RuntimeError):
@@ -213,3 +218,97 @@ def gkr_outputs(row_images, columns):
     _check(_lib.load().bitz_gkr_outputs(ip, cp, log_cols,
                                         out.ctypes.data_as(ctypes.POINTER(ctypes.c_uint64))))
     return out
+
+
+def batch_prove(systems, lanes: int = 8):
+    """Proves every CircuitProofSystem in ``systems`` on ``lanes`` concurrent
+    prover lanes; returns (proofs, each proof's duration in ms)."""
+    lib = _lib.load()
+    n = len(systems)
+    hs = (ctypes.c_void_p * max(n, 1))(*[s._h.value for s in systems])
+    ptrs = (ctypes.c_void_p * max(n, 1))()
+    lens = (ctypes.c_size_t * max(n, 1))()
+    lat = (ctypes.c_double * max(n, 1))()
+    status = lib.bitz_batch_prove(hs, n, lanes, ptrs, lens, lat)
+    proofs = []
+    for i in range(n):
+        if ptrs[i]:
+            proofs.append(ctypes.string_at(ptrs[i], lens[i]))
+            lib.bitz_free(ptrs[i])
+        else:
+            proofs.append(None)
+    _check(status)
+    return proofs, list(lat[:n])
+
+
+class ProveServer:
+    """Continuous-batching prove server over ``lanes`` prover lanes, admitting
+    requests by padded-witness device footprint within ``hbm_budget`` bytes."""
+
+    def __init__(self, lanes: int = 8, hbm_budget: int = 64 << 30, security_bits: int = 100):
+        self._lib = _lib.load()
+        h = ctypes.c_void_p()
+        _check(self._lib.bitz_server_start(lanes, hbm_budget, security_bits, ctypes.byref(h)))
+        self._h = h
+
+    def submit(self, circuit: str, inputs, outputs) -> int:
+        inp = np.ascontiguousarray(inputs, dtype=np.uint8)
+        out = np.ascontiguousarray(outputs, dtype=np.uint8)
+        t = ctypes.c_uint64(0)
+        _check(self._lib.bitz_server_submit(self._h, CIRCUITS[circuit], inp.ctypes.data, inp.size,
+                                            out.ctypes.data, ctypes.byref(t)))
+        return t.value
+
+    def poll(self, ticket: int, wait_ms: int = 0):
+        """(proof bytes, latency ms) once done, else None; raises on failure."""
+        p = ctypes.POINTER(ctypes.c_uint8)()
+        n = ctypes.c_size_t(0)
+        lat = ctypes.c_double(0)
+        st = self._lib.bitz_server_poll(self._h, ticket, wait_ms, ctypes.byref(p), ctypes.byref(n),
+                                        ctypes.byref(lat))
+        if st == PENDING:
+            return None
+        _check(st)
+        data = ctypes.string_at(p, n.value)
+        self._lib.bitz_free(p)
+        return data, lat.value
+
+    def stats(self):
+        out = np.zeros(6, dtype=np.uint64)
+        _check(self._lib.bitz_server_stats(self._h, out.ctypes.data_as(ctypes.POINTER(ctypes.c_uint64))))
+        keys = ["submitted", "finished", "in_flight", "queued", "in_flight_bytes", "peak_in_flight"]
+        return dict(zip(keys, (int(x) for x in out)))
+
+    def stop(self):
+        if getattr(self, "_h", None):
+            _check(self._lib.bitz_server_stop(self._h))
+            self._h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.stop()
+
+    def __del__(self):
+        try:
+            self.stop()
+        except Exception:
+            pass
+
+
+def probe_kernel(name):
+    """Times every launch of kernel ``name`` with CUDA events (None: off)."""
+    _check(_lib.load().bitz_probe_kernel(name.encode() if name else None))
+
+
+def probe_read():
+    """(total ms, total algorithmic bytes, launches) of the probed kernel."""
+    ms, b, n = ctypes.c_double(0), ctypes.c_double(0), ctypes.c_ulonglong(0)
+    _check(_lib.load().bitz_probe_read(ctypes.byref(ms), ctypes.byref(b), ctypes.byref(n)))
+    return ms.value, b.value, n.value
+
+
+def l2_flush():
+    """Evicts the L2 cache by overwriting a 256 MiB device buffer."""
+    _check(_lib.load().bitz_l2_flush())

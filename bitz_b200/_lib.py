@@ -54,6 +54,22 @@ SIGNATURES = [
      [_vp, _vp, ctypes.c_size_t, _vp, ctypes.c_size_t, _vp, ctypes.c_size_t]),
     ("bitz_circuit_layout", ctypes.c_int,
      [ctypes.c_int, ctypes.c_size_t, _u64p, _u8p, _vp, _vp, _vp, _vp, _vp]),
+    ("bitz_batch_prove", ctypes.c_int,
+     [_vp, ctypes.c_size_t, ctypes.c_int, _vp, _vp, _vp]),
+    ("bitz_server_start", ctypes.c_int,
+     [ctypes.c_int, ctypes.c_uint64, ctypes.c_uint32, ctypes.POINTER(_vp)]),
+    ("bitz_server_submit", ctypes.c_int,
+     [_vp, ctypes.c_int, _vp, ctypes.c_size_t, _vp, ctypes.POINTER(ctypes.c_uint64)]),
+    ("bitz_server_poll", ctypes.c_int,
+     [_vp, ctypes.c_uint64, ctypes.c_int, ctypes.POINTER(_u8p), ctypes.POINTER(ctypes.c_size_t),
+      ctypes.POINTER(ctypes.c_double)]),
+    ("bitz_server_stats", ctypes.c_int, [_vp, _u64p]),
+    ("bitz_server_stop", ctypes.c_int, [_vp]),
+    ("bitz_probe_kernel", ctypes.c_int, [ctypes.c_char_p]),
+    ("bitz_probe_read", ctypes.c_int,
+     [ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double),
+      ctypes.POINTER(ctypes.c_ulonglong)]),
+    ("bitz_l2_flush", ctypes.c_int, []),
 ]
 
 _lib = None

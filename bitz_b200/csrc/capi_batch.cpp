@@ -1,0 +1,367 @@
+// Batched and served proving across prover lanes, and the measurement aids.
+//
+// A lane (Context) is one CUDA stream with its own round mailbox and scratch;
+// each lane is driven by one host thread, which runs the proof's transcript.
+// Proofs on different lanes overlap on the device: while one proof's host
+// thread absorbs a round message, the kernels of the others run. Lanes are
+// pooled per process, so their scratch stays resident in HBM across calls.
+#include <cuda_runtime.h>
+#include <stdlib.h>
+#include <string.h>
+
+#include <algorithm>
+#include <atomic>
+#include <chrono>
+#include <condition_variable>
+#include <deque>
+#include <memory>
+#include <mutex>
+#include <thread>
+#include <unordered_map>
+#include <vector>
+
+#include "../../include/bitz_b200.h"
+#include "prover.hpp"
+#include "status.hpp"
+
+struct bitz_system {
+  bz::ProofSystem *ps;
+};
+
+namespace bz {
+int capi_fail(int code, const std::string &msg);
+int check_statement(int circuit_kind, const uint8_t *input_bits, size_t n_inputs,
+                    const uint8_t *output_bits, uint32_t security_bits);
+
+namespace {
+
+constexpr int kMaxLanes = 64;
+
+// Process-wide pool of idle lanes (per device), grown on demand.
+class LanePool {
+ public:
+  static LanePool &get() {
+    static LanePool *p = new LanePool();
+    return *p;
+  }
+  std::vector<std::unique_ptr<Context>> take(int device, int n) {
+    std::vector<std::unique_ptr<Context>> out;
+    {
+      std::lock_guard<std::mutex> lk(mu_);
+      auto &idle = idle_[device];
+      while ((int)out.size() < n && !idle.empty()) {
+        out.push_back(std::move(idle.back()));
+        idle.pop_back();
+      }
+    }
+    while ((int)out.size() < n) out.push_back(std::make_unique<Context>());
+    return out;
+  }
+  void give(int device, std::vector<std::unique_ptr<Context>> &lanes) {
+    std::lock_guard<std::mutex> lk(mu_);
+    for (auto &l : lanes) idle_[device].push_back(std::move(l));
+    lanes.clear();
+  }
+
+ private:
+  std::mutex mu_;
+  std::unordered_map<int, std::vector<std::unique_ptr<Context>>> idle_;
+};
+
+double ms_between(std::chrono::steady_clock::time_point a, std::chrono::steady_clock::time_point b) {
+  return std::chrono::duration<double, std::milli>(b - a).count();
+}
+
+// Runs one proof on a lane; the status, message and bytes come back.
+int prove_on(ProofSystem &ps, Context &lane, std::vector<uint8_t> &proof, std::string &err) {
+  try {
+    int rc = ps.prove(proof, nullptr, true, &lane);
+    if (rc) err = ps.error;
+    return rc;
+  } catch (const CudaError &e) {
+    err = e.what();
+    return BZ_ERR_CUDA;
+  } catch (const std::exception &e) {
+    err = e.what();
+    return BZ_ERR_INTERNAL;
+  }
+}
+
+uint8_t *copy_out(const std::vector<uint8_t> &p) {
+  uint8_t *b = (uint8_t *)malloc(std::max<size_t>(p.size(), 1));
+  if (b) memcpy(b, p.data(), p.size());
+  return b;
+}
+
+}  // namespace
+}  // namespace bz
+
+using namespace bz;
+
+// ------------------------------------------------------------------ server
+
+struct ServeRequest {
+  uint64_t ticket = 0;
+  int kind = 0;
+  std::vector<uint8_t> inputs, outputs;
+  uint64_t footprint = 0;
+  std::chrono::steady_clock::time_point submitted;
+  bool done = false;
+  int status = BZ_OK;
+  std::string error;
+  std::vector<uint8_t> proof;
+  double latency_ms = 0;
+};
+
+struct bitz_server {
+  int device = 0;
+  uint32_t security = 100;
+  uint64_t budget = 0;
+  std::vector<std::unique_ptr<Context>> lanes;
+  std::vector<std::thread> workers;
+  std::mutex mu;
+  std::condition_variable work_cv, done_cv;
+  std::deque<std::shared_ptr<ServeRequest>> queue;
+  std::unordered_map<uint64_t, std::shared_ptr<ServeRequest>> tickets;
+  uint64_t next_ticket = 1, submitted = 0, finished = 0, in_flight = 0, in_flight_bytes = 0,
+           peak_in_flight = 0;
+  bool stopping = false;
+
+  // Admission: FIFO, a free lane, and the head's footprint fits the budget
+  // beside the requests in flight (always when none is in flight).
+  bool admissible() const {
+    if (queue.empty()) return false;
+    uint64_t need = queue.front()->footprint;
+    return in_flight == 0 || in_flight_bytes + need <= budget;
+  }
+
+  void run(Context *lane) {
+    cudaSetDevice(device);
+    for (;;) {
+      std::shared_ptr<ServeRequest> rq;
+      {
+        std::unique_lock<std::mutex> lk(mu);
+        work_cv.wait(lk, [&] { return stopping || admissible(); });
+        if (stopping) return;
+        rq = queue.front();
+        queue.pop_front();
+        in_flight++;
+        in_flight_bytes += rq->footprint;
+        peak_in_flight = std::max(peak_in_flight, in_flight);
+      }
+      std::vector<uint8_t> proof;
+      std::string err;
+      int rc;
+      try {
+        ProofSystem ps(rq->kind, rq->inputs.data(), rq->inputs.size(), rq->outputs.data(),
+                       (int)security, lane);
+        rc = prove_on(ps, *lane, proof, err);
+      } catch (const CudaError &e) {
+        rc = BZ_ERR_CUDA;
+        err = e.what();
+      } catch (const std::exception &e) {
+        rc = BZ_ERR_CONFIG;
+        err = e.what();
+      }
+      auto t = std::chrono::steady_clock::now();
+      {
+        std::lock_guard<std::mutex> lk(mu);
+        rq->status = rc;
+        rq->error = err;
+        rq->proof = std::move(proof);
+        rq->latency_ms = ms_between(rq->submitted, t);
+        rq->done = true;
+        in_flight--;
+        in_flight_bytes -= rq->footprint;
+        finished++;
+      }
+      done_cv.notify_all();
+      work_cv.notify_all();
+    }
+  }
+};
+
+extern "C" {
+
+int bitz_batch_prove(bitz_system *const *systems, size_t n, int lanes, uint8_t **proofs,
+                     size_t *proof_lens, double *latency_ms) {
+  if ((!systems || !proofs || !proof_lens) && n) return capi_fail(BZ_ERR_ARGUMENT, "null argument");
+  if (lanes < 1 || lanes > kMaxLanes) return capi_fail(BZ_ERR_ARGUMENT, "lanes must be 1..64");
+  for (size_t i = 0; i < n; i++) {
+    if (!systems[i]) return capi_fail(BZ_ERR_ARGUMENT, "null system");
+    proofs[i] = nullptr;
+    proof_lens[i] = 0;
+  }
+  if (n == 0) return BZ_OK;
+  int device = 0;
+  if (cudaGetDevice(&device) != cudaSuccess) return capi_fail(BZ_ERR_NO_DEVICE, "no CUDA device");
+  int nl = (int)std::min<size_t>((size_t)lanes, n);
+  std::vector<std::unique_ptr<Context>> pool;
+  try {
+    pool = LanePool::get().take(device, nl);
+  } catch (const std::exception &e) {
+    return capi_fail(BZ_ERR_CUDA, e.what());
+  }
+  std::atomic<size_t> next{0};
+  std::vector<int> status(n, BZ_OK);
+  std::vector<std::string> errors(n);
+  auto worker = [&](Context *lane) {
+    cudaSetDevice(device);
+    for (size_t i; (i = next.fetch_add(1)) < n;) {
+      std::vector<uint8_t> proof;
+      auto ts = std::chrono::steady_clock::now();
+      status[i] = prove_on(*systems[i]->ps, *lane, proof, errors[i]);
+      if (latency_ms) latency_ms[i] = ms_between(ts, std::chrono::steady_clock::now());
+      if (status[i] == BZ_OK) {
+        proofs[i] = copy_out(proof);
+        proof_lens[i] = proof.size();
+        if (!proofs[i]) {
+          status[i] = BZ_ERR_INTERNAL;
+          errors[i] = "out of host memory";
+        }
+      }
+    }
+  };
+  std::vector<std::thread> threads;
+  for (int k = 1; k < nl; k++) threads.emplace_back(worker, pool[k].get());
+  worker(pool[0].get());
+  for (auto &t : threads) t.join();
+  LanePool::get().give(device, pool);
+  for (size_t i = 0; i < n; i++)
+    if (status[i]) return capi_fail(status[i], "proof " + std::to_string(i) + ": " + errors[i]);
+  return BZ_OK;
+}
+
+int bitz_server_start(int lanes, uint64_t hbm_budget_bytes, uint32_t security_bits,
+                      bitz_server **out) {
+  if (!out) return capi_fail(BZ_ERR_ARGUMENT, "null argument");
+  *out = nullptr;
+  if (lanes < 1 || lanes > kMaxLanes) return capi_fail(BZ_ERR_ARGUMENT, "lanes must be 1..64");
+  if (security_bits != 100 && security_bits != 128)
+    return capi_fail(BZ_ERR_ARGUMENT, "security_bits must be 100 or 128");
+  auto *srv = new bitz_server();
+  if (cudaGetDevice(&srv->device) != cudaSuccess) {
+    delete srv;
+    return capi_fail(BZ_ERR_NO_DEVICE, "no CUDA device");
+  }
+  srv->security = security_bits;
+  srv->budget = hbm_budget_bytes;
+  try {
+    srv->lanes = LanePool::get().take(srv->device, lanes);
+  } catch (const std::exception &e) {
+    delete srv;
+    return capi_fail(BZ_ERR_CUDA, e.what());
+  }
+  for (auto &l : srv->lanes) srv->workers.emplace_back(&bitz_server::run, srv, l.get());
+  *out = srv;
+  return BZ_OK;
+}
+
+int bitz_server_submit(bitz_server *srv, int circuit_kind, const uint8_t *input_bits,
+                       size_t n_inputs, const uint8_t *output_bits, uint64_t *ticket) {
+  if (!srv || !ticket) return capi_fail(BZ_ERR_ARGUMENT, "null argument");
+  int rc = check_statement(circuit_kind, input_bits, n_inputs, output_bits, srv->security);
+  if (rc) return rc;
+  auto rq = std::make_shared<ServeRequest>();
+  rq->kind = circuit_kind;
+  rq->inputs.assign(input_bits, input_bits + n_inputs);
+  rq->outputs.assign(output_bits, output_bits + 256);
+  rq->footprint = ProofSystem::footprint_bytes(circuit_kind, n_inputs);
+  rq->submitted = std::chrono::steady_clock::now();
+  {
+    std::lock_guard<std::mutex> lk(srv->mu);
+    if (srv->stopping) return capi_fail(BZ_ERR_ARGUMENT, "server is stopping");
+    rq->ticket = srv->next_ticket++;
+    srv->tickets[rq->ticket] = rq;
+    srv->queue.push_back(rq);
+    srv->submitted++;
+    *ticket = rq->ticket;
+  }
+  srv->work_cv.notify_one();
+  return BZ_OK;
+}
+
+int bitz_server_poll(bitz_server *srv, uint64_t ticket, int wait_ms, uint8_t **proof,
+                     size_t *proof_len, double *latency_ms) {
+  if (!srv || !proof || !proof_len) return capi_fail(BZ_ERR_ARGUMENT, "null argument");
+  *proof = nullptr;
+  *proof_len = 0;
+  std::unique_lock<std::mutex> lk(srv->mu);
+  auto it = srv->tickets.find(ticket);
+  if (it == srv->tickets.end()) return capi_fail(BZ_ERR_ARGUMENT, "unknown ticket");
+  std::shared_ptr<ServeRequest> rq = it->second;
+  if (!rq->done && wait_ms > 0)
+    srv->done_cv.wait_for(lk, std::chrono::milliseconds(wait_ms), [&] { return rq->done; });
+  if (!rq->done) return BZ_PENDING;
+  srv->tickets.erase(it);
+  if (latency_ms) *latency_ms = rq->latency_ms;
+  if (rq->status) return capi_fail(rq->status, rq->error);
+  *proof = copy_out(rq->proof);
+  if (!*proof) return capi_fail(BZ_ERR_INTERNAL, "out of host memory");
+  *proof_len = rq->proof.size();
+  return BZ_OK;
+}
+
+int bitz_server_stats(bitz_server *srv, uint64_t out[6]) {
+  if (!srv || !out) return capi_fail(BZ_ERR_ARGUMENT, "null argument");
+  std::lock_guard<std::mutex> lk(srv->mu);
+  out[0] = srv->submitted;
+  out[1] = srv->finished;
+  out[2] = srv->in_flight;
+  out[3] = srv->queue.size();
+  out[4] = srv->in_flight_bytes;
+  out[5] = srv->peak_in_flight;
+  return BZ_OK;
+}
+
+int bitz_server_stop(bitz_server *srv) {
+  if (!srv) return capi_fail(BZ_ERR_ARGUMENT, "null argument");
+  {
+    std::lock_guard<std::mutex> lk(srv->mu);
+    srv->stopping = true;
+    srv->queue.clear();
+  }
+  srv->work_cv.notify_all();
+  for (auto &t : srv->workers) t.join();
+  LanePool::get().give(srv->device, srv->lanes);
+  delete srv;
+  return BZ_OK;
+}
+
+int bitz_probe_kernel(const char *name) {
+  try {
+    KernelProbe::get().enable(name);
+    return BZ_OK;
+  } catch (const std::exception &e) {
+    return capi_fail(BZ_ERR_CUDA, e.what());
+  }
+}
+
+int bitz_probe_read(double *ms_total, double *bytes_total, unsigned long long *launches) {
+  try {
+    KernelProbe::get().collect();
+    KernelProbe::get().read(ms_total, bytes_total, launches);
+    return BZ_OK;
+  } catch (const std::exception &e) {
+    return capi_fail(BZ_ERR_CUDA, e.what());
+  }
+}
+
+int bitz_l2_flush(void) {
+  static std::mutex mu;
+  static void *buf = nullptr;
+  const size_t bytes = (size_t)256 << 20;
+  std::lock_guard<std::mutex> lk(mu);
+  try {
+    cudaStream_t s = Context::get().stream();
+    if (!buf) BZ_CUDA(cudaMalloc(&buf, bytes));
+    static unsigned char v = 0;
+    BZ_CUDA(cudaMemsetAsync(buf, ++v, bytes, s));
+    BZ_CUDA(cudaStreamSynchronize(s));
+    return BZ_OK;
+  } catch (const std::exception &e) {
+    return capi_fail(BZ_ERR_CUDA, e.what());
+  }
+}
+
+}  // extern "C"

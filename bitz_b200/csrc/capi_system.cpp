@@ -17,17 +17,14 @@ struct bitz_system {
 
 namespace bz {
 int capi_fail(int code, const std::string &msg);
-}
 
-extern "C" {
-
-int bitz_system_new(int circuit_kind, const uint8_t *input_bits, size_t n_inputs,
-                    const uint8_t *output_bits, uint32_t security_bits, bitz_system **out) {
-  if (!input_bits || !output_bits || !out) return capi_fail(BZ_ERR_ARGUMENT, "null argument");
-  *out = nullptr;
+// Input checks of CircuitProofSystem::new (circuits.rs:58-210 dimensions).
+int check_statement(int circuit_kind, const uint8_t *input_bits, size_t n_inputs,
+                    const uint8_t *output_bits, uint32_t security_bits) {
   if (circuit_kind < 0 || circuit_kind > 3) return capi_fail(BZ_ERR_ARGUMENT, "unknown circuit");
   if (security_bits != 100 && security_bits != 128)
     return capi_fail(BZ_ERR_ARGUMENT, "security_bits must be 100 or 128");
+  if ((!input_bits && n_inputs) || !output_bits) return capi_fail(BZ_ERR_ARGUMENT, "null argument");
   bool ok = false;
   switch (circuit_kind) {
     case kCompression: ok = n_inputs == 768; break;
@@ -40,6 +37,18 @@ int bitz_system_new(int circuit_kind, const uint8_t *input_bits, size_t n_inputs
     if (input_bits[i] > 1) return capi_fail(BZ_ERR_ARGUMENT, "input bits must be 0 or 1");
   for (int i = 0; i < 256; i++)
     if (output_bits[i] > 1) return capi_fail(BZ_ERR_ARGUMENT, "output bits must be 0 or 1");
+  return BZ_OK;
+}
+}  // namespace bz
+
+extern "C" {
+
+int bitz_system_new(int circuit_kind, const uint8_t *input_bits, size_t n_inputs,
+                    const uint8_t *output_bits, uint32_t security_bits, bitz_system **out) {
+  if (!input_bits || !output_bits || !out) return capi_fail(BZ_ERR_ARGUMENT, "null argument");
+  *out = nullptr;
+  int rc = check_statement(circuit_kind, input_bits, n_inputs, output_bits, security_bits);
+  if (rc) return rc;
   int n = 0;
   if (cudaGetDeviceCount(&n) != cudaSuccess || n == 0)
     return capi_fail(BZ_ERR_NO_DEVICE, "no CUDA device");

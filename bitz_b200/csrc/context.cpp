@@ -4,6 +4,7 @@
 
 #include <atomic>
 #include <chrono>
+#include <thread>
 
 namespace bz {
 
@@ -21,7 +22,11 @@ void RoundChannel::wait(cudaStream_t s, uint64_t *out, int n) {
       if (std::chrono::steady_clock::now() - t0 > std::chrono::seconds(30))
         throw CudaError("timed out waiting for a round result");
     }
-    _mm_pause();
+    // spin briefly, then give the core to other lanes' host threads
+    if (spins < 4096)
+      _mm_pause();
+    else
+      std::this_thread::yield();
   }
   std::atomic_thread_fence(std::memory_order_acquire);
   const volatile unsigned long long *p = host->payload;
@@ -53,15 +58,82 @@ Context::Context() {
   gk_.channel = &channel_;
 }
 
-unsigned long long &launch_counter() {
-  static unsigned long long n = 0;
+Context::~Context() {
+  if (stream_) cudaStreamSynchronize(stream_);
+  workspace.reset();
+  if (channel_.host) cudaFreeHost(channel_.host);
+  if (host_) cudaFreeHost(host_);
+  if (stream_) cudaStreamDestroy(stream_);
+}
+
+std::atomic<unsigned long long> &launch_counter() {
+  static std::atomic<unsigned long long> n{0};
   return n;
 }
 
 Context &Context::get() {
-  // One context per process, created on first use on the current device.
+  // One default lane per process, created on first use on the current device.
   static Context *ctx = new Context();
   return *ctx;
+}
+
+// ------------------------------------------------------------ KernelProbe
+
+KernelProbe &KernelProbe::get() {
+  static KernelProbe *p = new KernelProbe();
+  return *p;
+}
+
+void KernelProbe::enable(const char *name) {
+  std::lock_guard<std::mutex> lk(mu_);
+  target_ = name ? name : "";
+  active_ = !target_.empty();
+  ms_ = bytes_ = 0;
+  launches_ = 0;
+  used_ = 0;
+  pending_bytes_.clear();
+  if (active_ && ev_.empty()) {
+    ev_.resize(2 * 4096);
+    for (auto &e : ev_) BZ_CUDA(cudaEventCreate(&e));
+  }
+}
+
+void KernelProbe::before(cudaStream_t s) {
+  std::lock_guard<std::mutex> lk(mu_);
+  if (2 * used_ + 1 >= ev_.size()) collect_locked_full();
+  BZ_CUDA(cudaEventRecord(ev_[2 * used_], s));
+}
+
+void KernelProbe::after(cudaStream_t s, double bytes) {
+  std::lock_guard<std::mutex> lk(mu_);
+  BZ_CUDA(cudaEventRecord(ev_[2 * used_ + 1], s));
+  pending_bytes_.push_back(bytes);
+  used_++;
+}
+
+void KernelProbe::collect() {
+  std::lock_guard<std::mutex> lk(mu_);
+  collect_locked_full();
+}
+
+void KernelProbe::collect_locked_full() {
+  for (size_t i = 0; i < used_; i++) {
+    BZ_CUDA(cudaEventSynchronize(ev_[2 * i + 1]));
+    float ms = 0;
+    BZ_CUDA(cudaEventElapsedTime(&ms, ev_[2 * i], ev_[2 * i + 1]));
+    ms_ += ms;
+    bytes_ += pending_bytes_[i];
+    launches_++;
+  }
+  used_ = 0;
+  pending_bytes_.clear();
+}
+
+void KernelProbe::read(double *ms, double *bytes, unsigned long long *launches) {
+  std::lock_guard<std::mutex> lk(mu_);
+  if (ms) *ms = ms_;
+  if (bytes) *bytes = bytes_;
+  if (launches) *launches = launches_;
 }
 
 }  // namespace bz

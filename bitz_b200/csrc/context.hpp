@@ -3,6 +3,9 @@
 #pragma once
 #include <cuda_runtime.h>
 
+#include <memory>
+#include <mutex>
+#include <string>
 #include <vector>
 
 #include "device.cuh"
@@ -52,12 +55,25 @@ class DeviceBuffer {
   size_t n_ = 0;
 };
 
+struct Workspace;  // the end-to-end prover's reusable buffers (prover.cpp)
+
+// A prover lane: one stream, one round mailbox and the scratch buffers that a
+// proof running on the stream reuses. Independent lanes prove concurrently;
+// one lane runs one proof at a time.
 class Context {
  public:
+  Context();
+  ~Context();
+  Context(const Context &) = delete;
+  Context &operator=(const Context &) = delete;
+
+  // The process-wide default lane, created on first use on the current device.
   static Context &get();
 
   cudaStream_t stream() const { return stream_; }
   RoundChannel *channel() { return &channel_; }
+  // Prover workspace slot, owned by the lane (created by the prover).
+  std::shared_ptr<Workspace> workspace;
 
   PostGkrScratch &post_gkr_scratch(size_t entries) {
     if (pg_.capacity < entries) {
@@ -95,7 +111,6 @@ class Context {
   }
 
  private:
-  Context();
   cudaStream_t stream_ = nullptr;
   PostGkrScratch pg_;
   DeviceBuffer<f128> pg_w0_, pg_v0_, pg_w1_, pg_v1_;
@@ -105,6 +120,32 @@ class Context {
   DeviceBuffer<f128> gk_layers_, gk_eq_, gk_eq_scratch_, gk_pair_;
   RoundChannel channel_;
   DeviceBuffer<unsigned int> counter_;
+};
+
+// Optional CUDA-event timing of every launch of one named kernel, with the
+// algorithmic bytes each launch moves (a measurement aid; off by default).
+// Events are recorded on the launching stream; totals are collected once the
+// stream has synchronised.
+class KernelProbe {
+ public:
+  static KernelProbe &get();
+  void enable(const char *name);  // null or "" turns the probe off
+  bool on(const char *name) const { return active_ && target_ == name; }
+  void before(cudaStream_t s);
+  void after(cudaStream_t s, double bytes);
+  void collect();  // adds the finished launches' times to the totals
+  void read(double *ms, double *bytes, unsigned long long *launches);
+
+ private:
+  void collect_locked_full();
+  std::mutex mu_;
+  bool active_ = false;
+  std::string target_;
+  std::vector<cudaEvent_t> ev_;
+  std::vector<double> pending_bytes_;
+  size_t used_ = 0;
+  double ms_ = 0, bytes_ = 0;
+  unsigned long long launches_ = 0;
 };
 
 }  // namespace bz

@@ -5,6 +5,7 @@
 #include <stdint.h>
 #include <stdio.h>
 
+#include <atomic>
 #include <stdexcept>
 #include <string>
 
@@ -26,7 +27,7 @@ struct CudaError : std::runtime_error {
 
 // Every launch site ends in BZ_LAUNCH_CHECK(), which also counts the launch
 // (read through bitz_launch_count()).
-unsigned long long &launch_counter();
+std::atomic<unsigned long long> &launch_counter();
 #define BZ_LAUNCH_CHECK()           \
   do {                              \
     ++::bz::launch_counter();       \

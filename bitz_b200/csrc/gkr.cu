@@ -14,6 +14,7 @@
 // down to round i's (eq_i[x] = eq_{i+1}[x] + eq_{i+1}[x + 2^i], summing out
 // coordinate i), and accumulates round i's two sums from the freshly bound
 // values; 32 bytes leave the device per round.
+#include "context.hpp"
 #include "eq.cuh"
 #include "gkr.hpp"
 
@@ -146,6 +147,7 @@ f128 gkr_prove(int s, const f128 *zeta, uint32_t grind_bits, Transcript &ts, Gkr
   for (int i = 0; i < s; i++) point[i] = zeta[i];
   int n = s;
   f128 claim = mk(0, 0);
+  KernelProbe &probe = KernelProbe::get();
   for (int j = 6; j >= 0; j--) {
     f128 *c = sc.layer[j];
     size_t n_half = (size_t)1 << n;
@@ -170,9 +172,13 @@ f128 gkr_prove(int s, const f128 *zeta, uint32_t grind_bits, Transcript &ts, Gkr
       eq_bound = gmul(eq_bound, eq_factor(r, point[i]));
       if (i > 0) {
         size_t hh = (size_t)1 << (i - 1);
+        const bool probed = probe.on("gkr_bind_sums");
+        if (probed) probe.before(st_);
         gkr_bind_sums<<<grid_for(hh), kThreads, 0, st_>>>(c, n_half, hh, r, sc.eq,
                                                           gis_zero(point[i - 1]), acc + 4, arm(sc));
         BZ_LAUNCH_CHECK();
+        // reads 8 child and 2 eq entries per thread, writes 4 and 1
+        if (probed) probe.after(st_, 240.0 * (double)hh);
       } else {
         gkr_final_bind<<<1, 32, 0, st_>>>(c, n_half, r, sc.pair, arm(sc));
         BZ_LAUNCH_CHECK();

@@ -217,7 +217,9 @@ Tables &tables(cudaStream_t s) {
   return *t;
 }
 
-// Per-proof device workspace, grown on demand.
+}  // namespace
+
+// Per-lane device workspace, grown on demand.
 struct Workspace {
   DeviceBuffer<uint32_t> states, msgs_u32;
   DeviceBuffer<uint64_t> offsets;
@@ -235,14 +237,17 @@ struct Workspace {
     BZ_CUDA(cudaMallocHost(&host_fp, 8 * sizeof(fp)));
     BZ_CUDA(cudaMallocHost(&host_acc, 512 * sizeof(uint64_t)));
   }
+  ~Workspace() {
+    if (host_fp) cudaFreeHost(host_fp);
+    if (host_acc) cudaFreeHost(host_acc);
+  }
 };
 
-Workspace &workspace() {
-  static Workspace *w = new Workspace();
-  return *w;
+// The lane's workspace, created on its first proof.
+static Workspace &workspace(Context &lane) {
+  if (!lane.workspace) lane.workspace = std::make_shared<Workspace>();
+  return *lane.workspace;
 }
-
-}  // namespace
 
 // ----------------------------------------------------------- ProofSystem
 
@@ -252,10 +257,10 @@ static void prepare_statement(int kind, const CircuitSetup &S, const std::vector
                               std::vector<uint8_t> &bitc);
 
 ProofSystem::ProofSystem(int kind, const uint8_t *inputs, size_t n_inputs, const uint8_t *outputs,
-                         int security_bits)
+                         int security_bits, Context *lane)
     : kind_(kind), security_(security_bits), inputs_(inputs, inputs + n_inputs),
       outputs_(outputs, outputs + 256) {
-  Context &ctx = Context::get();
+  Context &ctx = lane ? *lane : Context::get();
   cudaStream_t s = ctx.stream();
   dev_ = device_setup(kind, n_inputs, s);
   const CircuitSetup &S = *dev_->host;
@@ -287,6 +292,16 @@ ProofSystem::ProofSystem(int kind, const uint8_t *inputs, size_t n_inputs, const
   BZ_CUDA(cudaStreamSynchronize(s));
 }
 
+uint64_t ProofSystem::footprint_bytes(int kind, size_t n_inputs) {
+  // compressions and the layout's per-compression sizes (sha256.rs:45,54-60)
+  uint64_t c = kind == kCompression ? 1 : kind == kChain ? n_inputs / 512 : n_inputs / 512 + 1;
+  uint64_t h = 20456 * c + 2 * (uint64_t)n_inputs + 513, f = 6376 * c + n_inputs;
+  int mh = std::max(20, ceil_log2(h)), mf = std::max(20, ceil_log2(f));
+  // Spartan column tables and GKR layers (2^mh entries of 16 bytes, six of
+  // them with the eq tables), post-GKR tables, and a fixed remainder
+  return 96ull * (1ull << mh) + 64ull * (1ull << mf) + (16ull << 20);
+}
+
 ProofSystem::~ProofSystem() {
   if (ev_start_) cudaEventDestroy(ev_start_);
   if (ev_stop_) cudaEventDestroy(ev_stop_);
@@ -302,7 +317,7 @@ void ProofSystem::stage_statement(cudaStream_t s) {
 
 int ProofSystem::witness(cudaStream_t s) {
   const CircuitSetup &S = *dev_->host;
-  Workspace &W = workspace();
+  Workspace &W = workspace(*lane_);
   W.acc.resize(512);
   size_t n_in = inputs_.size();
   size_t fwords = ((size_t)1 << S.committed_m) / 32;
@@ -399,7 +414,7 @@ static void prepare_statement(int kind, const CircuitSetup &S, const std::vector
 
 int ProofSystem::commit(cudaStream_t s) {
   const CircuitSetup &S = *dev_->host;
-  Workspace &W = workspace();
+  Workspace &W = workspace(*lane_);
   Tables &T = tables(s);
   const PcsLevel &L0 = pcs_.levels[0];
   int log_n = pcs_.log_n;
@@ -430,7 +445,7 @@ int ProofSystem::commit(cudaStream_t s) {
     eq_table_device(ood_point_.data(), log_n, W.eq_ood.get(), W.eqs.get(), s);
     W.acc.resize(512);
     BZ_CUDA(cudaMemsetAsync(W.acc.get(), 0, 16, s));
-    RoundChannel *ch = Context::get().channel();
+    RoundChannel *ch = lane_->channel();
     dot(W.eq_ood.get(), fpk, n, W.acc.get(), ch->arm(), s);
     ch->wait(s, W.host_acc, 2);
     ood_value_ = mk(W.host_acc[0], W.host_acc[1]);
@@ -443,7 +458,7 @@ int ProofSystem::commit(cudaStream_t s) {
 // The Ligerito opening (the PCS restatement; see oracle/pcs.c for the
 // construction): returns the hint bytes, empty on an internal failure.
 std::vector<uint8_t> ProofSystem::ligerito(cudaStream_t s, f128 target) {
-  Workspace &W = workspace();
+  Workspace &W = workspace(*lane_);
   Tables &T = tables(s);
   Transcript &t = *ts_;
   const PcsConfig &cfg = pcs_;
@@ -490,7 +505,7 @@ std::vector<uint8_t> ProofSystem::ligerito(cudaStream_t s, f128 target) {
   DeviceBuffer<uint32_t> next_nodes[2];
   int flip = 0;
   unsigned long long *acc = W.acc.get();
-  RoundChannel *ch = Context::get().channel();
+  RoundChannel *ch = lane_->channel();
   for (int i = 0; i < cfg.nlevels; i++) {
     const PcsLevel &L = cfg.levels[i];
     std::vector<f128> rs;
@@ -622,9 +637,9 @@ std::vector<uint8_t> ProofSystem::ligerito(cudaStream_t s, f128 target) {
 
 int ProofSystem::prove_after_commit(cudaStream_t s, std::vector<uint8_t> &proof) {
   const CircuitSetup &S = *dev_->host;
-  Workspace &W = workspace();
+  Workspace &W = workspace(*lane_);
   Tables &T = tables(s);
-  Context &ctx = Context::get();
+  Context &ctx = *lane_;
   Transcript &t = *ts_;
   Phases ph(s);
   // bind (end_to_end.rs:442-455)
@@ -932,8 +947,10 @@ int ProofSystem::prove_after_commit(cudaStream_t s, std::vector<uint8_t> &proof)
   return BZ_OK;
 }
 
-int ProofSystem::prove(std::vector<uint8_t> &proof, StageTimes *times, bool restage) {
-  cudaStream_t s = Context::get().stream();
+int ProofSystem::prove(std::vector<uint8_t> &proof, StageTimes *times, bool restage,
+                       Context *lane) {
+  lane_ = lane ? lane : &Context::get();
+  cudaStream_t s = lane_->stream();
   auto t0 = std::chrono::steady_clock::now();
   BZ_CUDA(cudaEventRecord(ev_start_, s));
   if (restage) stage_statement(s);
@@ -948,6 +965,7 @@ int ProofSystem::prove(std::vector<uint8_t> &proof, StageTimes *times, bool rest
   rc = prove_after_commit(s, proof);
   BZ_CUDA(cudaEventRecord(ev_stop_, s));
   BZ_CUDA(cudaEventSynchronize(ev_stop_));
+  KernelProbe::get().collect();
   if (times) {
     times->witness_ms = tw;
     times->commit_ms = tc;
@@ -961,7 +979,7 @@ int ProofSystem::prove(std::vector<uint8_t> &proof, StageTimes *times, bool rest
 
 void ProofSystem::download_witness(std::vector<uint32_t> &f, std::vector<uint32_t> &h,
                                    std::vector<int64_t> &prod) {
-  cudaStream_t s = Context::get().stream();
+  cudaStream_t s = (lane_ ? lane_ : &Context::get())->stream();
   f.resize(f_.size());
   h.resize(h_.size());
   prod.resize(prod_.size());

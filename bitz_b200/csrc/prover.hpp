@@ -51,8 +51,12 @@ class ProofSystem {
  public:
   // CircuitProofSystem::new (end_to_end.rs:161-197): one statement (its input
   // and expected output bits, one byte each) at a PCS security level.
+  // Staging runs on `lane` (the default lane when null).
   ProofSystem(int kind, const uint8_t *inputs, size_t n_inputs, const uint8_t *outputs,
-              int security_bits);
+              int security_bits, Context *lane = nullptr);
+  // Device bytes a proof of this statement keeps in its lane's scratch at
+  // most (the padded tables of the largest stages), for admission control.
+  static uint64_t footprint_bytes(int kind, size_t n_inputs);
   ~ProofSystem();
   ProofSystem(const ProofSystem &) = delete;
   ProofSystem &operator=(const ProofSystem &) = delete;
@@ -61,7 +65,11 @@ class ProofSystem {
   // root || Spartan section || bitzPCS wire container. With restage set the
   // statement (input bits, chaining values, message words) is copied from
   // host memory first; otherwise the copy made at construction is reused.
-  int prove(std::vector<uint8_t> &proof, StageTimes *times, bool restage = true);
+  // The proof runs on `lane` (the process default lane when null); a system
+  // proves on one lane at a time, distinct systems on distinct lanes run
+  // concurrently.
+  int prove(std::vector<uint8_t> &proof, StageTimes *times, bool restage = true,
+            Context *lane = nullptr);
 
   const CircuitSetup &setup() const { return *dev_->host; }
   int security() const { return security_; }
@@ -78,6 +86,7 @@ class ProofSystem {
   int prove_after_commit(cudaStream_t s, std::vector<uint8_t> &proof);
   std::vector<uint8_t> ligerito(cudaStream_t s, f128 target);
 
+  Context *lane_ = nullptr;  // the lane of the proof in progress
   int kind_, security_;
   std::vector<uint8_t> inputs_, outputs_;
   std::shared_ptr<DeviceSetup> dev_;

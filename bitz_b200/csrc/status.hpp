@@ -15,3 +15,4 @@
 #define BZ_ERR_VERIFY 8          /* verification rejected the proof */
 #define BZ_ERR_MALFORMED 9       /* proof bytes do not decode */
 #define BZ_ERR_NO_DEVICE 10      /* no CUDA device is available */
+#define BZ_PENDING 11            /* a served request has not finished yet */

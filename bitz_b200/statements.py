@@ -82,3 +82,64 @@ def instance(kind: str, blocks: int, seed: int, initial_state=None):
 def random_state(seed: int):
     raw = splitmix64_bytes(seed ^ 0x5EED, 32)
     return [int.from_bytes(raw[4 * i:4 * i + 4], "little") for i in range(8)]
+
+
+def message_instance(kind: str, data: bytes):
+    """(input bits, output bits) of a padded-message circuit (block-aligned or
+    2kb) for the message ``data`` (tooling/cli/src/circuits.rs:103-139)."""
+    return (np.array(stream_bits(data), dtype=np.uint8),
+            np.array(stream_bits(hashlib.sha256(data).digest()), dtype=np.uint8))
+
+
+def blocks_proven(kind: str, n_inputs: int) -> int:
+    """Compression blocks a proof covers: message blocks, plus the padding
+    block of the padded-message circuits."""
+    if kind in ("sha256-block-aligned", "sha256-2kb"):
+        return n_inputs // 512 + 1
+    return max(n_inputs // 512, 1)
+
+
+def _u64s(seed: int, n: int):
+    raw = splitmix64_bytes(seed, 8 * n)
+    return [int.from_bytes(raw[8 * i:8 * i + 8], "little") for i in range(n)]
+
+
+def batch_mix(seed: int = 3, count: int = 256, max_blocks: int = 32):
+    """Independent sha256-block-aligned statements with message lengths
+    uniform over 0..max_blocks blocks (empty messages allowed) and uniform
+    random bytes: lengths from the SplitMix64 stream of ``seed``, message
+    bytes from the stream of ``seed + 1000003``. Returns a list of
+    (kind, input bits, output bits)."""
+    lengths = [v % (max_blocks + 1) for v in _u64s(seed, count)]
+    data = splitmix64_bytes(seed + 1000003, 64 * sum(lengths))
+    out, pos = [], 0
+    for k in lengths:
+        msg = data[pos:pos + 64 * k]
+        pos += 64 * k
+        out.append(("sha256-block-aligned",) + message_instance("sha256-block-aligned", msg))
+    return out
+
+
+def serve_mix(seed: int = 4, count: int = 64, max_blocks: int = 512):
+    """Serving requests: half sha256-2kb (2 KiB random message), half
+    sha256-block-aligned with k = floor(2^U(0, log2 max_blocks)) blocks,
+    clipped to 1..max_blocks. Kind and length come from the SplitMix64 stream
+    of ``seed``, message bytes from the stream of ``seed + 1000003``."""
+    import math
+    draws = _u64s(seed, 2 * count)
+    kinds, lengths = [], []
+    for i in range(count):
+        if draws[2 * i] & 1:
+            kinds.append("sha256-2kb")
+            lengths.append(32)
+        else:
+            u = (draws[2 * i + 1] >> 11) / float(1 << 53) * math.log2(max_blocks)
+            kinds.append("sha256-block-aligned")
+            lengths.append(min(max(int(2.0 ** u), 1), max_blocks))
+    data = splitmix64_bytes(seed + 1000003, 64 * sum(lengths))
+    out, pos = [], 0
+    for kind, k in zip(kinds, lengths):
+        msg = data[pos:pos + 64 * k]
+        pos += 64 * k
+        out.append((kind,) + message_instance(kind, msg))
+    return out

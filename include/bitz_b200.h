@@ -150,6 +150,59 @@ int bitz_circuit_layout(int circuit_kind, size_t n_inputs, uint64_t sizes[8],
                         uint8_t map_digest[32], uint32_t *m_off, uint32_t *m_pos,
                         uint32_t *c_off, uint32_t *c_col, int64_t *c_coef);
 
+/* ------------------------------------------------------ batch and serving
+ * No reference counterpart: the reference proves one statement per call
+ * (CircuitProofSystem::prove, end_to_end.rs:260-336, on a Rayon pool the
+ * caller installs, cmd/circuit_e2e.rs:50-56). These run many independent
+ * proofs at once on prover lanes: a lane is one CUDA stream, one host
+ * thread and its own round mailbox and scratch, so the rounds of different
+ * proofs overlap on the device while each proof's Fiat-Shamir transcript
+ * advances on its own thread. Every proof's bytes are the same as the
+ * single-proof call's for the same statement. */
+
+/* Proves systems[0..n) on `lanes` lanes (1..64). proofs[i] (freed with
+ * bitz_free) and proof_lens[i] receive each proof; latency_ms[i] (may be
+ * NULL) that proof's own duration, from its start on a lane to its bytes. Returns
+ * the first failure's status after every proof has finished; failed entries
+ * get a NULL proof. The systems must be distinct. */
+int bitz_batch_prove(bitz_system *const *systems, size_t n, int lanes, uint8_t **proofs,
+                     size_t *proof_lens, double *latency_ms);
+
+/* A prove server: `lanes` lanes take requests from a FIFO queue as they
+ * free up (continuous batching). A request is admitted when a lane is free
+ * and its padded-witness device footprint fits in hbm_budget_bytes beside
+ * the requests in flight (one request is always admitted when none is in
+ * flight). Each request builds its statement (CircuitProofSystem::new) and
+ * proves it on the lane. */
+typedef struct bitz_server bitz_server;
+int bitz_server_start(int lanes, uint64_t hbm_budget_bytes, uint32_t security_bits,
+                      bitz_server **out);
+/* Queues one statement (arguments as bitz_system_new); returns a ticket. */
+int bitz_server_submit(bitz_server *srv, int circuit_kind, const uint8_t *input_bits,
+                       size_t n_inputs, const uint8_t *output_bits, uint64_t *ticket);
+/* Waits up to wait_ms for the ticket's proof. BZ_OK: proof (freed with
+ * bitz_free), its length and the submit-to-proof latency are returned and the
+ * ticket is retired. BZ_PENDING: not finished yet. Any other status: that
+ * request failed (the ticket is retired). */
+int bitz_server_poll(bitz_server *srv, uint64_t ticket, int wait_ms, uint8_t **proof,
+                     size_t *proof_len, double *latency_ms);
+/* Counters: [0] submitted, [1] finished, [2] in flight, [3] queued,
+ * [4] bytes admitted in flight, [5] peak requests in flight. */
+int bitz_server_stats(bitz_server *srv, uint64_t out[6]);
+/* Finishes the requests already admitted, drops the queued ones, joins the
+ * lanes and frees the server. */
+int bitz_server_stop(bitz_server *srv);
+
+/* --------------------------------------------------------- measurement aids
+ * No reference counterpart. */
+/* Times every launch of the named kernel with CUDA events on its stream and
+ * counts the algorithmic bytes each launch moves; NULL or "" turns it off
+ * (and enabling resets the totals). Currently probed: "gkr_bind_sums". */
+int bitz_probe_kernel(const char *name);
+int bitz_probe_read(double *ms_total, double *bytes_total, unsigned long long *launches);
+/* Overwrites a 256 MiB device buffer and waits, evicting the L2 cache. */
+int bitz_l2_flush(void);
+
 #ifdef __cplusplus
 }
 #endif

@@ -715,4 +715,16 @@ void o_prover_free(o_prover *P) {
   delete P;
 }
 
+/* The PCS profile encoding for a committed size of 2^m bits
+ * (crates/pcs/src/commitment.rs:214-221). Returns its length. */
+size_t o_pcs_encoding(int m, int security, uint8_t *out, size_t cap) {
+  Setup s;
+  s.committed_m = m;
+  s.security = security;
+  std::vector<uint8_t> enc;
+  pcs_encoding(s, enc);
+  if (out && cap >= enc.size()) memcpy(out, enc.data(), enc.size());
+  return enc.size();
+}
+
 }  // extern "C"
