@@ -8,17 +8,31 @@
 
 namespace bz {
 
+// True once the first 2n slots all carry the tag of publication `want`.
+static bool mailbox_ready(const Mailbox *mb, unsigned long long want, int n) {
+  const volatile unsigned long long *s = mb->slot;
+  const unsigned long long tag = (want << 32) >> 32;
+  for (int k = 0; k < 2 * n; k++)
+    if ((s[k] >> 32) != tag) return false;
+  return true;
+}
+
 void RoundChannel::wait(cudaStream_t s, uint64_t *out, int n) {
+  if (n > kMailboxWords) throw CudaError("mailbox read too long");
   const unsigned long long want = next;
   auto t0 = std::chrono::steady_clock::now();
   uint64_t spins = 0;
-  while (host->seq != want) {
+  while (!mailbox_ready(host, want, n)) {
     if ((++spins & 0x3ff) == 0) {
       cudaError_t e = cudaStreamQuery(s);
       if (e != cudaSuccess && e != cudaErrorNotReady)
         throw CudaError(std::string("round kernel failed: ") + cudaGetErrorString(e));
-      if (e == cudaSuccess && host->seq != want)
-        throw CudaError("round kernel finished without publishing its result");
+      if (e == cudaSuccess && !mailbox_ready(host, want, n)) {
+        // the stream is idle: its writes land within microseconds
+        std::this_thread::sleep_for(std::chrono::milliseconds(2));
+        if (!mailbox_ready(host, want, n))
+          throw CudaError("round kernel finished without publishing its result");
+      }
       if (std::chrono::steady_clock::now() - t0 > std::chrono::seconds(30))
         throw CudaError("timed out waiting for a round result");
     }
@@ -29,8 +43,8 @@ void RoundChannel::wait(cudaStream_t s, uint64_t *out, int n) {
       std::this_thread::yield();
   }
   std::atomic_thread_fence(std::memory_order_acquire);
-  const volatile unsigned long long *p = host->payload;
-  for (int k = 0; k < n; k++) out[k] = p[k];
+  const volatile unsigned long long *p = host->slot;
+  for (int k = 0; k < n; k++) out[k] = (p[2 * k] & 0xffffffffull) | (p[2 * k + 1] << 32);
 }
 
 Context::Context() {

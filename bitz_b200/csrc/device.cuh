@@ -47,13 +47,25 @@ inline int grid_for(size_t work, int per_block = kThreads, int max_blocks = kSMs
 }
 
 // A round's result delivered without a copy or a stream sync: the last block
-// of the kernel moves the accumulated words into host-mapped pinned memory
-// and then publishes a sequence number the host polls.
+// of the kernel writes the accumulated words into host-mapped pinned memory.
+// Every 64-bit slot carries 32 data bits under a 32-bit tag (the round's
+// sequence number); naturally aligned 8-byte writes are single-copy atomic,
+// so the host accepts the result once every slot shows the current tag, and
+// the device needs no system-scope fence to order data before a flag.
+constexpr int kMailboxWords = 8;  // 64-bit data words per publication
 struct Mailbox {
-  volatile unsigned long long seq;
-  unsigned long long pad[7];
-  unsigned long long payload[8];
+  unsigned long long slot[2 * kMailboxWords];
 };
+
+#if defined(__CUDACC__)
+__device__ __forceinline__ void mailbox_post(Mailbox *mb, unsigned long long seq, int k,
+                                             unsigned long long v) {
+  const unsigned long long tag = seq << 32;
+  volatile unsigned long long *s = mb->slot;
+  s[2 * k] = tag | (v & 0xffffffffull);
+  s[2 * k + 1] = tag | (v >> 32);
+}
+#endif
 
 // Where a round kernel publishes: counter counts finished blocks (reset by
 // the last one); a null counter disables publishing.
@@ -65,10 +77,11 @@ struct Publish {
 
 #if defined(__CUDACC__)
 // Called by every thread after the block's atomics (issued by thread 0):
-// the last block to finish reads and clears the N accumulator words, writes
-// them to the mailbox, then the sequence number.
+// the last block to finish reads and clears the N accumulator words and
+// posts them, tagged, to the mailbox.
 template <int N>
 __device__ __forceinline__ void publish(unsigned long long *acc, const Publish &p) {
+  static_assert(N <= kMailboxWords, "mailbox too small");
   if (!p.counter) return;
   if (threadIdx.x == 0) {
     __threadfence();
@@ -76,11 +89,8 @@ __device__ __forceinline__ void publish(unsigned long long *acc, const Publish &
     if (prev == gridDim.x - 1) {
       __threadfence();
 #pragma unroll
-      for (int k = 0; k < N; k++) p.mailbox->payload[k] = atomicExch(acc + k, 0ull);
+      for (int k = 0; k < N; k++) mailbox_post(p.mailbox, p.seq, k, atomicExch(acc + k, 0ull));
       *p.counter = 0;
-      __threadfence_system();
-      p.mailbox->seq = p.seq;
-      __threadfence_system();
     }
   }
 }

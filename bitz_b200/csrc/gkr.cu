@@ -98,13 +98,10 @@ __global__ void gkr_final_bind(const f128 *__restrict__ c, size_t n_half, f128 r
     f128 lr = gadd(l0, gmul(r, gadd(l1, l0)));
     f128 rr = gadd(r0, gmul(r, gadd(r1, r0)));
     if (pub.counter) {
-      pub.mailbox->payload[0] = lr.lo;
-      pub.mailbox->payload[1] = lr.hi;
-      pub.mailbox->payload[2] = rr.lo;
-      pub.mailbox->payload[3] = rr.hi;
-      __threadfence_system();
-      pub.mailbox->seq = pub.seq;
-      __threadfence_system();
+      mailbox_post(pub.mailbox, pub.seq, 0, lr.lo);
+      mailbox_post(pub.mailbox, pub.seq, 1, lr.hi);
+      mailbox_post(pub.mailbox, pub.seq, 2, rr.lo);
+      mailbox_post(pub.mailbox, pub.seq, 3, rr.hi);
     } else {
       st(out, lr);
       st(out + 1, rr);

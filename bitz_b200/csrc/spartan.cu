@@ -185,14 +185,12 @@ __global__ void k_fp_finalize(const fp *partial, int nblocks, FpCtx c, fp *out, 
   for (int b = threadIdx.x; b < nblocks; b += blockDim.x)
     for (int k = 0; k < N; k++) acc[k] = fp_add(acc[k], partial[b * N + k], c);
   block_fp_sum<N>(acc, c, out);
+  static_assert(2 * N <= kMailboxWords, "mailbox too small");
   if (pub.counter && threadIdx.x == 0) {
     for (int k = 0; k < N; k++) {
-      pub.mailbox->payload[2 * k] = out[k].lo;
-      pub.mailbox->payload[2 * k + 1] = out[k].hi;
+      mailbox_post(pub.mailbox, pub.seq, 2 * k, out[k].lo);
+      mailbox_post(pub.mailbox, pub.seq, 2 * k + 1, out[k].hi);
     }
-    __threadfence_system();
-    pub.mailbox->seq = pub.seq;
-    __threadfence_system();
   }
 }
 
