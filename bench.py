@@ -241,8 +241,11 @@ def batched(args, bz):
     mix = statements.batch_mix(3, 256, 32)
     systems = [bz.CircuitProofSystem(kind, inp, out, args.security) for kind, inp, out in mix]
     blocks = sum(statements.blocks_proven(kind, inp.size) for kind, inp, _ in mix)
-    bz.batch_prove(systems[:2 * args.lanes], args.lanes)  # warm the lanes' scratch
-    bz.batch_prove(systems[:4], 1)
+    # warm-up: every lane's scratch grows to the largest shape of the mix
+    largest = sorted(range(len(mix)), key=lambda i: -mix[i][1].size)[:args.lanes]
+    bz.batch_prove([systems[i] for i in largest], args.lanes)
+    bz.batch_prove([systems[largest[0]]], 1)
+    bz.batch_prove(systems, args.lanes)
     res = {}
     for name, lanes in (("sequential", 1), ("batched", args.lanes)):
         bz.l2_flush()

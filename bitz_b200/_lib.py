@@ -70,6 +70,8 @@ SIGNATURES = [
      [ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double),
       ctypes.POINTER(ctypes.c_ulonglong)]),
     ("bitz_l2_flush", ctypes.c_int, []),
+    ("bitz_diag_round_trip", ctypes.c_int,
+     [ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_double)]),
 ]
 
 _lib = None

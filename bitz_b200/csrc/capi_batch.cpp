@@ -32,6 +32,7 @@ namespace bz {
 int capi_fail(int code, const std::string &msg);
 int check_statement(int circuit_kind, const uint8_t *input_bits, size_t n_inputs,
                     const uint8_t *output_bits, uint32_t security_bits);
+double diag_round_trip(int mode, int rounds);
 
 namespace {
 
@@ -341,6 +342,17 @@ int bitz_probe_read(double *ms_total, double *bytes_total, unsigned long long *l
   try {
     KernelProbe::get().collect();
     KernelProbe::get().read(ms_total, bytes_total, launches);
+    return BZ_OK;
+  } catch (const std::exception &e) {
+    return capi_fail(BZ_ERR_CUDA, e.what());
+  }
+}
+
+int bitz_diag_round_trip(int mode, int rounds, double *us_per_round) {
+  if (!us_per_round || rounds < 1 || (mode != 0 && mode != 1))
+    return capi_fail(BZ_ERR_ARGUMENT, "bad argument");
+  try {
+    *us_per_round = diag_round_trip(mode, rounds);
     return BZ_OK;
   } catch (const std::exception &e) {
     return capi_fail(BZ_ERR_CUDA, e.what());

@@ -45,6 +45,32 @@ void RoundChannel::wait(cudaStream_t s, uint64_t *out, int n) {
   std::atomic_thread_fence(std::memory_order_acquire);
   const volatile unsigned long long *p = host->slot;
   for (int k = 0; k < n; k++) out[k] = (p[2 * k] & 0xffffffffull) | (p[2 * k + 1] << 32);
+  wait_ns += (unsigned long long)std::chrono::duration_cast<std::chrono::nanoseconds>(
+                 std::chrono::steady_clock::now() - t0)
+                 .count();
+  waits++;
+}
+
+void RoundChannel::send(const uint64_t *words, int n) {
+  if (n > kMailboxWords) throw CudaError("downbox write too long");
+  const unsigned long long tag = (++down_next & 0xffffffffull) << 32;
+  volatile unsigned long long *s = down_host->slot;
+  for (int k = 0; k < n; k++) {
+    s[2 * k] = tag | (words[k] & 0xffffffffull);
+    s[2 * k + 1] = tag | (words[k] >> 32);
+  }
+  std::atomic_thread_fence(std::memory_order_release);
+}
+
+void RoundChannel::abort() {
+  volatile unsigned long long *s = down_host->slot;
+  for (int k = 0; k < 2 * kMailboxWords; k++) s[k] = 0xffffffffull << 32;
+  std::atomic_thread_fence(std::memory_order_release);
+}
+
+void RoundChannel::clear_down() {
+  volatile unsigned long long *s = down_host->slot;
+  for (int k = 0; k < 2 * kMailboxWords; k++) s[k] = 0;
 }
 
 Context::Context() {
@@ -65,6 +91,8 @@ Context::Context() {
   void *mbd = nullptr;
   BZ_CUDA(cudaHostGetDevicePointer(&mbd, mb, 0));
   channel_.dev = (Mailbox *)mbd;
+  channel_.down_host = (Mailbox *)((char *)mb + 512);
+  channel_.down_dev = (Mailbox *)((char *)mbd + 512);
   counter_.resize(1);
   BZ_CUDA(cudaMemset(counter_.get(), 0, sizeof(unsigned int)));
   channel_.counter = counter_.get();

@@ -55,6 +55,32 @@ class DeviceBuffer {
   size_t n_ = 0;
 };
 
+// Page-locked host memory, grown on demand (for asynchronous copies).
+template <class T>
+class PinnedBuffer {
+ public:
+  PinnedBuffer() = default;
+  ~PinnedBuffer() {
+    if (p_) cudaFreeHost(p_);
+  }
+  PinnedBuffer(const PinnedBuffer &) = delete;
+  PinnedBuffer &operator=(const PinnedBuffer &) = delete;
+  T *get(size_t n) {
+    if (n > n_) {
+      if (p_) cudaFreeHost(p_);
+      p_ = nullptr;
+      n_ = 0;
+      BZ_CUDA(cudaMallocHost(&p_, (n ? n : 1) * sizeof(T)));
+      n_ = n;
+    }
+    return p_;
+  }
+
+ private:
+  T *p_ = nullptr;
+  size_t n_ = 0;
+};
+
 struct Workspace;  // the end-to-end prover's reusable buffers (prover.cpp)
 
 // A prover lane: one stream, one round mailbox and the scratch buffers that a

@@ -124,6 +124,35 @@ __device__ __forceinline__ void block_xor_atomic(uint64_t (&v)[N], unsigned long
   }
 }
 
+// XOR-reduce `n` 64-bit words across the block; thread 0 ends with the
+// totals in v. Every thread must call it (it synchronises the block twice).
+template <int N>
+__device__ __forceinline__ void block_xor_reduce(uint64_t (&v)[N]) {
+  __shared__ uint64_t sm[N][kThreads / 32];
+#pragma unroll
+  for (int k = 0; k < N; k++) {
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) v[k] ^= __shfl_xor_sync(0xffffffffu, v[k], off);
+  }
+  int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  if (lane == 0) {
+#pragma unroll
+    for (int k = 0; k < N; k++) sm[k][warp] = v[k];
+  }
+  __syncthreads();
+  if (warp == 0) {
+    int nw = blockDim.x >> 5;
+#pragma unroll
+    for (int k = 0; k < N; k++) {
+      uint64_t x = lane < nw ? sm[k][lane] : 0;
+#pragma unroll
+      for (int off = 16; off > 0; off >>= 1) x ^= __shfl_xor_sync(0xffffffffu, x, off);
+      v[k] = x;
+    }
+  }
+  __syncthreads();
+}
+
 // block_xor_atomic, then publish the totals when this is the last block.
 template <int N>
 __device__ __forceinline__ void block_xor_publish(uint64_t (&v)[N], unsigned long long *acc,
@@ -181,10 +210,60 @@ struct RoundChannel {
   Mailbox *dev = nullptr;   // device view
   unsigned int *counter = nullptr;
   unsigned long long next = 0;
+  // The reverse direction, for kernels that run several rounds and wait for
+  // the host's challenge between them: same tagged format, host to device.
+  Mailbox *down_host = nullptr, *down_dev = nullptr;
+  unsigned long long down_next = 0;
+  // host time spent inside wait() and the number of waits (phase timer)
+  unsigned long long wait_ns = 0, waits = 0;
   Publish arm() { return Publish{counter, dev, ++next}; }
   // Waits for the publication armed last; copies n payload words.
   void wait(cudaStream_t s, uint64_t *out, int n);
+  // Posts n words to the device as publication down_next + 1.
+  void send(const uint64_t *words, int n);
+  // Posts an abort marker that a waiting kernel reads as "stop"; clear_down
+  // empties the downbox again once no kernel can be waiting.
+  void abort();
+  void clear_down();
 };
+
+#if defined(__CUDACC__)
+// The host's abort marker: every slot tagged 0xffffffff.
+constexpr unsigned long long kDownAbortTag = 0xffffffffull;
+
+__device__ __forceinline__ unsigned long long globaltimer_ns() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
+// Thread-level wait for host publication `seq` (n words) in a device-view
+// mailbox. Bounded by time: returns false after `limit_ns` or on the host's
+// abort marker, so a kernel never spins forever on a host that went away.
+__device__ __forceinline__ bool mailbox_wait_device(const Mailbox *mb, unsigned long long seq,
+                                                    int n, unsigned long long *out,
+                                                    unsigned long long limit_ns) {
+  const volatile unsigned long long *s = mb->slot;
+  const unsigned long long tag = seq & 0xffffffffull;
+  const unsigned long long t0 = globaltimer_ns();
+  for (;;) {
+    bool ready = true;
+    for (int k = 0; k < 2 * n; k++) {
+      unsigned long long t = s[k] >> 32;
+      if (t == kDownAbortTag) return false;
+      if (t != tag) {
+        ready = false;
+        break;
+      }
+    }
+    if (ready) break;
+    if (globaltimer_ns() - t0 > limit_ns) return false;
+    __nanosleep(64);
+  }
+  for (int k = 0; k < n; k++) out[k] = (s[2 * k] & 0xffffffffull) | (s[2 * k + 1] << 32);
+  return true;
+}
+#endif
 
 #if defined(__CUDACC__)
 __device__ __forceinline__ f128 ld(const f128 *p) {

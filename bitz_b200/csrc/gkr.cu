@@ -109,6 +109,74 @@ __global__ void gkr_final_bind(const f128 *__restrict__ c, size_t n_half, f128 r
   }
 }
 
+// The last rounds of a layer in one resident block. From iteration i0 (where
+// the live halves hold 4h0 = 2^(i0+1) entries, h0 <= kTailH) down to 0 the
+// block keeps both halves and the eq table in shared memory; each iteration
+// waits for the host's challenge r_i in the lane's downbox (bounded), binds
+// and sums exactly as gkr_bind_sums / gkr_final_bind, and posts the round's
+// four words to the mailbox (publication seq0 + i0 - i). A missing challenge
+// ends the kernel without a post, which the host reads as a failed round.
+constexpr int kTailH = 256;
+constexpr unsigned long long kTailWaitNs = 2000000000ull;  // 2 s per challenge
+
+__global__ void __launch_bounds__(kThreads) gkr_tail(const f128 *__restrict__ c, size_t n_half,
+                                                     int i0, const f128 *__restrict__ eq,
+                                                     uint32_t at_one_mask, Mailbox *mb,
+                                                     unsigned long long seq0, const Mailbox *down,
+                                                     unsigned long long dseq0) {
+  __shared__ f128 L[4 * kTailH], R[4 * kTailH], E[2 * kTailH];
+  __shared__ unsigned long long chal[2];
+  __shared__ int ok;
+  const int h0 = i0 > 0 ? 1 << (i0 - 1) : 1;
+  const int live = i0 > 0 ? 4 * h0 : 2;
+  for (int k = threadIdx.x; k < live; k += blockDim.x) {
+    L[k] = ld(c + k);
+    R[k] = ld(c + n_half + k);
+  }
+  for (int k = threadIdx.x; k < 2 * h0 && i0 > 0; k += blockDim.x) E[k] = ld(eq + k);
+  for (int i = i0; i >= 0; i--) {
+    if (threadIdx.x == 0) ok = mailbox_wait_device(down, dseq0 + (i0 - i), 2, chal, kTailWaitNs);
+    __syncthreads();
+    if (!ok) return;
+    const f128 r = mk(chal[0], chal[1]);
+    const unsigned long long seq = seq0 + (i0 - i);
+    if (i == 0) {
+      if (threadIdx.x == 0) {
+        f128 lr = gadd(L[0], gmul(r, gadd(L[1], L[0])));
+        f128 rr = gadd(R[0], gmul(r, gadd(R[1], R[0])));
+        mailbox_post(mb, seq, 0, lr.lo);
+        mailbox_post(mb, seq, 1, lr.hi);
+        mailbox_post(mb, seq, 2, rr.lo);
+        mailbox_post(mb, seq, 3, rr.hi);
+      }
+      return;
+    }
+    const int h = 1 << (i - 1), h2 = 2 * h;
+    const int at_one = (at_one_mask >> (i - 1)) & 1;
+    wide sb = wzero(), si = wzero();
+    for (int x = threadIdx.x; x < h; x += blockDim.x) {
+      f128 l0 = gadd(L[x], gmul(r, gadd(L[x + h2], L[x])));
+      f128 l1 = gadd(L[x + h], gmul(r, gadd(L[x + h + h2], L[x + h])));
+      f128 r0 = gadd(R[x], gmul(r, gadd(R[x + h2], R[x])));
+      f128 r1 = gadd(R[x + h], gmul(r, gadd(R[x + h + h2], R[x + h])));
+      L[x] = l0;
+      L[x + h] = l1;
+      R[x] = r0;
+      R[x + h] = r1;
+      f128 e = gadd(E[x], E[x + h]);
+      E[x] = e;
+      f128 lb = at_one ? l1 : l0, rb = at_one ? r1 : r0;
+      wacc(sb, gmul_wide(gmul(e, lb), rb));
+      wacc(si, gmul_wide(gmul(e, gadd(l1, l0)), gadd(r1, r0)));
+    }
+    f128 a = greduce(sb), b = greduce(si);
+    uint64_t v[4] = {a.lo, a.hi, b.lo, b.hi};
+    block_xor_reduce<4>(v);  // also orders this round's table writes before the next
+    if (threadIdx.x == 0)
+      for (int k = 0; k < 4; k++) mailbox_post(mb, seq, k, v[k]);
+  }
+}
+
 static Publish arm(GkrScratch &sc) {
   return sc.channel ? sc.channel->arm() : Publish{nullptr, nullptr, 0};
 }
@@ -145,6 +213,9 @@ f128 gkr_prove(int s, const f128 *zeta, uint32_t grind_bits, Transcript &ts, Gkr
   int n = s;
   f128 claim = mk(0, 0);
   KernelProbe &probe = KernelProbe::get();
+  RoundChannel *ch = sc.channel;
+  bool tail = false;  // a tail kernel of this layer is resident and waiting
+  try {
   for (int j = 6; j >= 0; j--) {
     f128 *c = sc.layer[j];
     size_t n_half = (size_t)1 << n;
@@ -167,7 +238,19 @@ f128 gkr_prove(int s, const f128 *zeta, uint32_t grind_bits, Transcript &ts, Gkr
       f128 r = ts.challenge_f128();
       next[i] = r;
       eq_bound = gmul(eq_bound, eq_factor(r, point[i]));
-      if (i > 0) {
+      const uint64_t rw[2] = {r.lo, r.hi};
+      if (!tail && ch && (i == 0 || ((size_t)1 << (i - 1)) <= (size_t)kTailH)) {
+        uint32_t mask = 0;
+        for (int k = 1; k <= i; k++) mask |= (uint32_t)gis_zero(point[k - 1]) << (k - 1);
+        gkr_tail<<<1, kThreads, 0, st_>>>(c, n_half, i, sc.eq, mask, ch->dev, ch->next + 1,
+                                          ch->down_dev, ch->down_next + 1);
+        BZ_LAUNCH_CHECK();
+        tail = true;
+      }
+      if (tail) {
+        ch->send(rw, 2);
+        ch->arm();
+      } else if (i > 0) {
         size_t hh = (size_t)1 << (i - 1);
         const bool probed = probe.on("gkr_bind_sums");
         if (probed) probe.before(st_);
@@ -183,6 +266,7 @@ f128 gkr_prove(int s, const f128 *zeta, uint32_t grind_bits, Transcript &ts, Gkr
     }
     f128 lr[2];
     round_read(sc, sc.pair, st_);
+    tail = false;  // the tail kernel ends after posting the pair
     memcpy(lr, sc.host, 32);
     ts.prover_message(lr, 32);
     f128 t = ts.challenge_f128();
@@ -190,6 +274,14 @@ f128 gkr_prove(int s, const f128 *zeta, uint32_t grind_bits, Transcript &ts, Gkr
     claim = gadd(lr[0], gmul(t, gadd(lr[1], lr[0])));
     n++;
     for (int i = 0; i < n; i++) point[i] = next[i];
+  }
+  } catch (...) {
+    if (tail) {  // release the waiting kernel before the lane is reused
+      ch->abort();
+      cudaStreamSynchronize(st_);
+      ch->clear_down();
+    }
+    throw;
   }
   for (int i = 0; i < n; i++) point_out[i] = point[i];
   return claim;

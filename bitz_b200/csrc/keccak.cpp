@@ -14,7 +14,7 @@ static const uint64_t KRC[24] = {
     0x8000000000008002ull, 0x8000000000000080ull, 0x000000000000800aull, 0x800000008000000aull,
     0x8000000080008081ull, 0x8000000000008080ull, 0x0000000080000001ull, 0x8000000080008008ull};
 
-static inline uint64_t rol(uint64_t x, int n) { return (x << n) | (x >> ((64 - n) & 63)); }
+#define rol(x, n) (((x) << (n)) | ((x) >> ((64 - (n)) & 63)))
 
 #define KECCAK_ROUND(RC) \
   { \
@@ -82,17 +82,32 @@ static inline uint64_t rol(uint64_t x, int n) { return (x << n) | (x >> ((64 - n
   }
 
 
-void keccak_f1600(uint64_t st[25]) {
-  uint64_t a0 = st[0], a1 = st[1], a2 = st[2], a3 = st[3], a4 = st[4], a5 = st[5], a6 = st[6],
-           a7 = st[7], a8 = st[8], a9 = st[9], a10 = st[10], a11 = st[11], a12 = st[12],
-           a13 = st[13], a14 = st[14], a15 = st[15], a16 = st[16], a17 = st[17], a18 = st[18],
-           a19 = st[19], a20 = st[20], a21 = st[21], a22 = st[22], a23 = st[23], a24 = st[24];
-  for (int round = 0; round < 24; round++) KECCAK_ROUND(KRC[round]);
-  st[0] = a0, st[1] = a1, st[2] = a2, st[3] = a3, st[4] = a4, st[5] = a5, st[6] = a6;
-  st[7] = a7, st[8] = a8, st[9] = a9, st[10] = a10, st[11] = a11, st[12] = a12;
-  st[13] = a13, st[14] = a14, st[15] = a15, st[16] = a16, st[17] = a17, st[18] = a18;
+#define KECCAK_BODY \
+  uint64_t a0 = st[0], a1 = st[1], a2 = st[2], a3 = st[3], a4 = st[4], a5 = st[5], a6 = st[6], \
+           a7 = st[7], a8 = st[8], a9 = st[9], a10 = st[10], a11 = st[11], a12 = st[12], \
+           a13 = st[13], a14 = st[14], a15 = st[15], a16 = st[16], a17 = st[17], a18 = st[18], \
+           a19 = st[19], a20 = st[20], a21 = st[21], a22 = st[22], a23 = st[23], a24 = st[24]; \
+  for (int round = 0; round < 24; round++) KECCAK_ROUND(KRC[round]); \
+  st[0] = a0, st[1] = a1, st[2] = a2, st[3] = a3, st[4] = a4, st[5] = a5, st[6] = a6; \
+  st[7] = a7, st[8] = a8, st[9] = a9, st[10] = a10, st[11] = a11, st[12] = a12; \
+  st[13] = a13, st[14] = a14, st[15] = a15, st[16] = a16, st[17] = a17, st[18] = a18; \
   st[19] = a19, st[20] = a20, st[21] = a21, st[22] = a22, st[23] = a23, st[24] = a24;
+
+static void keccak_generic(uint64_t st[25]) { KECCAK_BODY }
+
+// The same permutation compiled for BMI1/BMI2 (ANDN for chi, RORX): about a
+// third faster where the CPU has them.
+__attribute__((target("bmi,bmi2"))) static void keccak_bmi(uint64_t st[25]) { KECCAK_BODY }
+
+void keccak_f1600(uint64_t st[25]) {
+  static const bool bmi = __builtin_cpu_supports("bmi") && __builtin_cpu_supports("bmi2");
+  if (bmi)
+    keccak_bmi(st);
+  else
+    keccak_generic(st);
 }
+#undef KECCAK_BODY
 #undef KECCAK_ROUND
+#undef rol
 
 }  // namespace bz

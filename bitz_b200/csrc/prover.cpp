@@ -112,15 +112,23 @@ double ms_since(std::chrono::steady_clock::time_point t) {
 struct Phases {
   cudaStream_t s;
   bool on;
+  RoundChannel *ch;
   std::chrono::steady_clock::time_point t;
-  explicit Phases(cudaStream_t st) : s(st), on(getenv("BITZ_PHASES") != nullptr) {
+  unsigned long long w0 = 0, n0 = 0;
+  Phases(cudaStream_t st, RoundChannel *c)
+      : s(st), on(getenv("BITZ_PHASES") != nullptr), ch(c) {
     t = std::chrono::steady_clock::now();
+    if (ch) w0 = ch->wait_ns, n0 = ch->waits;
   }
   void mark(const char *name) {
     if (!on) return;
     cudaStreamSynchronize(s);
-    fprintf(stderr, "[phase] %-22s %8.3f ms\n", name, ms_since(t));
+    double wait_ms = ch ? (ch->wait_ns - w0) * 1e-6 : 0.0;
+    unsigned long long waits = ch ? ch->waits - n0 : 0;
+    fprintf(stderr, "[phase] %-22s %8.3f ms  (%llu round waits, %.3f ms waiting)\n", name,
+            ms_since(t), waits, wait_ms);
     t = std::chrono::steady_clock::now();
+    if (ch) w0 = ch->wait_ns, n0 = ch->waits;
   }
 };
 
@@ -233,13 +241,22 @@ struct Workspace {
   DeviceBuffer<unsigned long long> acc;
   fp *host_fp = nullptr;
   uint64_t *host_acc = nullptr;
+  // the claim's canonical column weights and the column folds, copied back
+  // while the host absorbs earlier messages
+  DeviceBuffer<fp> cols_canon;
+  PinnedBuffer<u128> host_cols, host_folds;
+  cudaEvent_t ev_cols = nullptr, ev_folds = nullptr;
   Workspace() {
     BZ_CUDA(cudaMallocHost(&host_fp, 8 * sizeof(fp)));
     BZ_CUDA(cudaMallocHost(&host_acc, 512 * sizeof(uint64_t)));
+    BZ_CUDA(cudaEventCreateWithFlags(&ev_cols, cudaEventDisableTiming));
+    BZ_CUDA(cudaEventCreateWithFlags(&ev_folds, cudaEventDisableTiming));
   }
   ~Workspace() {
     if (host_fp) cudaFreeHost(host_fp);
     if (host_acc) cudaFreeHost(host_acc);
+    if (ev_cols) cudaEventDestroy(ev_cols);
+    if (ev_folds) cudaEventDestroy(ev_folds);
   }
 };
 
@@ -641,7 +658,7 @@ int ProofSystem::prove_after_commit(cudaStream_t s, std::vector<uint8_t> &proof)
   Tables &T = tables(s);
   Context &ctx = *lane_;
   Transcript &t = *ts_;
-  Phases ph(s);
+  Phases ph(s, lane_->channel());
   // bind (end_to_end.rs:442-455)
   t.public_u64(public_bytes_.size());
   t.public_message(public_bytes_.data(), public_bytes_.size());
@@ -734,11 +751,30 @@ int ProofSystem::prove_after_commit(cudaStream_t s, std::vector<uint8_t> &proof)
     }
     for (int b = 0; b < 128; b++) rows_w[b] = fp_canonical(fp_mul(e[b], so.d_at_ry, fc), fc);
   }
+  // Device work that needs no further challenge is queued first, so it runs
+  // while the host absorbs the claim: the column weights in canonical form,
+  // the column folds and row images, and the GKR product layers.
   W.cols_fp.resize(ncol + 2);
+  W.cols_canon.resize(ncol);
   fp_eq_table(pt.data() + 7, sc_cols, fc, W.cols_fp.get(), sc.eq_scratch, s);
-  std::vector<fp> cols_h(ncol);
-  BZ_CUDA(cudaMemcpyAsync(cols_h.data(), W.cols_fp.get(), ncol * sizeof(fp), cudaMemcpyDeviceToHost, s));
-  BZ_CUDA(cudaStreamSynchronize(s));
+  fp_canonical_device(W.cols_fp.get(), ncol, fc, W.cols_canon.get(), s);
+  u128 *cols_h = W.host_cols.get(ncol);
+  BZ_CUDA(cudaMemcpyAsync(cols_h, W.cols_canon.get(), ncol * 16, cudaMemcpyDeviceToHost, s));
+  BZ_CUDA(cudaEventRecord(W.ev_cols, s));
+  // send_fold (crates/prover/src/fold.rs:38-75) and the GKR build
+  W.exps.upload(rows_w.data(), 128, s);
+  W.folds.resize(ncol);
+  const f128 *hpk = reinterpret_cast<const f128 *>(h_.get());
+  fold_columns(hpk, ncol, W.exps.get(), W.folds.get(), s);
+  u128 *folds_h = W.host_folds.get(ncol + 128);  // the folds, then the 128 row images
+  BZ_CUDA(cudaMemcpyAsync(folds_h, W.folds.get(), ncol * 16, cudaMemcpyDeviceToHost, s));
+  W.images.resize(128);
+  comb_pow(T.comb.get(), W.exps.get(), 128, W.images.get(), s);
+  f128 *row_images_h = reinterpret_cast<f128 *>(folds_h + ncol);
+  BZ_CUDA(cudaMemcpyAsync(row_images_h, W.images.get(), 128 * 16, cudaMemcpyDeviceToHost, s));
+  BZ_CUDA(cudaEventRecord(W.ev_folds, s));
+  GkrScratch &gs = ctx.gkr_scratch(sc_cols);
+  gkr_build(hpk, sc_cols, W.images.get(), gs, s);
   u128 target_p = fp_canonical(so.final_claim, fc);
   // prove_virtual (crates/prover/src/prove.rs:96-152)
   t.public_message("bitz/virtual-statement/v1", 25);
@@ -751,37 +787,31 @@ int ProofSystem::prove_after_commit(cudaStream_t s, std::vector<uint8_t> &proof)
   }
   t.public_message(S.map_digest, 32);
   {
-    std::vector<uint8_t> ce;
-    ce.reserve(16 * (130 + ncol));
-    put_u64(ce, 128);
-    for (auto w : rows_w) put_u128(ce, w);
-    put_u64(ce, ncol);
-    for (size_t c = 0; c < ncol; c++) put_u128(ce, fp_canonical(cols_h[c], fc));
-    put_u128(ce, target_p);
-    t.public_message(ce.data(), ce.size());
+    // one public message: 128, the row weights, ncol, the column weights,
+    // the target (the sponge has no per-call framing, so it is absorbed in
+    // pieces as the column weights arrive)
+    std::vector<uint8_t> head;
+    head.reserve(16 * 129 + 8);
+    put_u64(head, 128);
+    for (auto w : rows_w) put_u128(head, w);
+    put_u64(head, ncol);
+    t.public_message(head.data(), head.size());
+    BZ_CUDA(cudaEventSynchronize(W.ev_cols));
+    t.public_message(cols_h, ncol * 16);
+    std::vector<uint8_t> tail;
+    put_u128(tail, target_p);
+    t.public_message(tail.data(), tail.size());
   }
   t.public_message(pcs_enc_.data(), pcs_enc_.size());
   ph.mark("claim");
-  // send_fold (crates/prover/src/fold.rs:38-75)
-  W.exps.upload(rows_w.data(), 128, s);
-  W.folds.resize(ncol);
-  const f128 *hpk = reinterpret_cast<const f128 *>(h_.get());
-  fold_columns(hpk, ncol, W.exps.get(), W.folds.get(), s);
-  std::vector<u128> folds(ncol);
-  BZ_CUDA(cudaMemcpyAsync(folds.data(), W.folds.get(), ncol * 16, cudaMemcpyDeviceToHost, s));
-  W.images.resize(128);
-  comb_pow(T.comb.get(), W.exps.get(), 128, W.images.get(), s);
-  std::vector<f128> row_images(128);
-  BZ_CUDA(cudaMemcpyAsync(row_images.data(), W.images.get(), 128 * 16, cudaMemcpyDeviceToHost, s));
-  BZ_CUDA(cudaStreamSynchronize(s));
-  for (auto fd : folds) t.prover_message(&fd, 16);
+  BZ_CUDA(cudaEventSynchronize(W.ev_folds));
+  t.prover_message(folds_h, ncol * 16);
+  std::vector<f128> row_images(row_images_h, row_images_h + 128);
   t.grind("bitz/columns/v1", grinding_bits((uint32_t)security_, (uint64_t)sc_cols));
   std::vector<f128> zeta(sc_cols);
   for (auto &z : zeta) z = t.challenge_f128();
   ph.mark("fold");
-  // gkr_reduce (crates/prover/src/reduce.rs:17-47)
-  GkrScratch &gs = ctx.gkr_scratch(sc_cols);
-  gkr_build(hpk, sc_cols, W.images.get(), gs, s);
+  // gkr_reduce (crates/prover/src/reduce.rs:17-47); the layers were built above
   std::vector<f128> gpt(sc_cols + 7);
   f128 gclaim = gkr_prove(sc_cols, zeta.data(), grinding_bits((uint32_t)security_, 3), t, gs, s,
                           gpt.data());

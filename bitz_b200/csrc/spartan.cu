@@ -438,6 +438,19 @@ u128 fp_canonical(fp mont, const FpCtx &c) {
   return (u128)v.lo | ((u128)v.hi << 64);
 }
 
+// Montgomery residues to canonical values (the 16-byte little-endian codec of
+// crates/field/src/codec.rs:69-73), one thread per element.
+__global__ void k_fp_canonical(const fp *__restrict__ in, size_t n, FpCtx c, fp *__restrict__ out) {
+  for (size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x; k < n;
+       k += (size_t)gridDim.x * blockDim.x)
+    out[k] = fp_mul(in[k], fp{1, 0}, c);
+}
+
+void fp_canonical_device(const fp *in, size_t n, const FpCtx &c, fp *out, cudaStream_t s) {
+  k_fp_canonical<<<grid_for(n), kThreads, 0, s>>>(in, n, c, out);
+  BZ_LAUNCH_CHECK();
+}
+
 fp fp_to_mont(u128 v, const FpCtx &c) { return fp_mul(fp{(uint64_t)v, (uint64_t)(v >> 64)}, c.r2, c); }
 
 }  // namespace bz

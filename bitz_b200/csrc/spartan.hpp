@@ -53,6 +53,8 @@ struct SpartanOut {
 
 FpCtx make_fp_ctx(u128 q);
 u128 fp_canonical(fp mont, const FpCtx &c);
+// out[k] = canonical value of in[k] (as two LE words), on the device.
+void fp_canonical_device(const fp *in, size_t n, const FpCtx &c, fp *out, cudaStream_t s);
 fp fp_to_mont(u128 v, const FpCtx &c);
 void fp_eq_table(const fp *point, int n, const FpCtx &c, fp *out, fp *scratch, cudaStream_t s);
 

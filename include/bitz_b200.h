@@ -202,6 +202,10 @@ int bitz_probe_kernel(const char *name);
 int bitz_probe_read(double *ms_total, double *bytes_total, unsigned long long *launches);
 /* Overwrites a 256 MiB device buffer and waits, evicting the L2 cache. */
 int bitz_l2_flush(void);
+/* Mean microseconds per host<->device round on the default lane: mode 0
+ * launches one kernel per round that posts to the mailbox; mode 1 runs one
+ * resident kernel that waits (bounded) for each host word and posts it back. */
+int bitz_diag_round_trip(int mode, int rounds, double *us_per_round);
 
 #ifdef __cplusplus
 }
