@@ -215,6 +215,13 @@ f128 gkr_prove(int s, const f128 *zeta, uint32_t grind_bits, Transcript &ts, Gkr
   KernelProbe &probe = KernelProbe::get();
   RoundChannel *ch = sc.channel;
   bool tail = false;  // a tail kernel of this layer is resident and waiting
+  // BITZ_RESIDENT_ROUNDS=0 runs every round as its own launch (same results):
+  // a kernel profiler that serialises launches and holds the host thread at
+  // each one cannot run a kernel that waits for the host.
+  static const bool resident = [] {
+    const char *e = getenv("BITZ_RESIDENT_ROUNDS");
+    return !(e && e[0] == '0');
+  }();
   try {
   for (int j = 6; j >= 0; j--) {
     f128 *c = sc.layer[j];
@@ -239,7 +246,7 @@ f128 gkr_prove(int s, const f128 *zeta, uint32_t grind_bits, Transcript &ts, Gkr
       next[i] = r;
       eq_bound = gmul(eq_bound, eq_factor(r, point[i]));
       const uint64_t rw[2] = {r.lo, r.hi};
-      if (!tail && ch && (i == 0 || ((size_t)1 << (i - 1)) <= (size_t)kTailH)) {
+      if (!tail && ch && resident && (i == 0 || ((size_t)1 << (i - 1)) <= (size_t)kTailH)) {
         uint32_t mask = 0;
         for (int k = 1; k <= i; k++) mask |= (uint32_t)gis_zero(point[k - 1]) << (k - 1);
         gkr_tail<<<1, kThreads, 0, st_>>>(c, n_half, i, sc.eq, mask, ch->dev, ch->next + 1,

@@ -70,3 +70,25 @@ def test_false_statement_is_unsatisfied():
     assert e.value.code == "Unsatisfied"
     rc, _, _ = of.prove(1, inp, bad, 100)
     assert rc == 3
+
+
+def test_per_round_launches_give_the_same_proof():
+    """BITZ_RESIDENT_ROUNDS=0 runs the GKR tail rounds as separate launches
+    instead of one resident kernel; the proof bytes must not change."""
+    import os
+    import subprocess
+    import sys
+    code = ("import sys; sys.path.insert(0, %r)\n"
+            "import bitz_b200 as bz\n"
+            "from bitz_b200 import statements as ci\n"
+            "inp, out, _ = ci.instance('sha256-chain', 2, 13)\n"
+            "p, _ = bz.CircuitProofSystem('sha256-chain', inp, out, 100).prove()\n"
+            "sys.stdout.write(p.hex())\n") % os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    runs = []
+    for flag in ("0", "1"):
+        env = dict(os.environ, BITZ_RESIDENT_ROUNDS=flag)
+        r = subprocess.run([sys.executable, "-c", code], env=env, capture_output=True, text=True,
+                           timeout=300)
+        assert r.returncode == 0, r.stderr[-2000:]
+        runs.append(r.stdout)
+    assert runs[0] == runs[1] and len(runs[0]) > 1000
