@@ -214,3 +214,16 @@ def prove(kind: int, inputs, expected, security: int):
     L.o_prover_times(h, times.ctypes.data)
     L.o_prover_free(h)
     return st.value, buf.raw[:n], times
+
+
+def verify(kind: int, inputs, expected, security: int, proof: bytes) -> int:
+    """Runs the oracle's restated verifier; 0 when it accepts, else the code of
+    the first failed check."""
+    L = lib()
+    L.o_verify.restype = ctypes.c_int
+    L.o_verify.argtypes = [ctypes.c_int, _vp, ctypes.c_size_t, _vp, ctypes.c_int, ctypes.c_char_p,
+                           ctypes.c_size_t]
+    inputs = np.ascontiguousarray(inputs, dtype=np.uint8)
+    expected = np.ascontiguousarray(expected, dtype=np.uint8)
+    return L.o_verify(kind, inputs.ctypes.data, inputs.size, expected.ctypes.data, security,
+                      proof, len(proof))

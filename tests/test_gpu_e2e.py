@@ -92,3 +92,26 @@ def test_per_round_launches_give_the_same_proof():
         assert r.returncode == 0, r.stderr[-2000:]
         runs.append(r.stdout)
     assert runs[0] == runs[1] and len(runs[0]) > 1000
+
+
+@pytest.mark.parametrize("kind,blocks,seed,security", [
+    ("sha256-chain", 64, 1, 100),        # the benchmark statement
+    ("sha256-block-aligned", 32, 3, 100),
+    ("sha256-2kb", 32, 4, 128),
+])
+def test_full_size_proofs_are_accepted_by_the_restated_verifier(kind, blocks, seed, security):
+    inp, out, _ = ci.instance(kind, blocks, seed)
+    proof, _ = bz.CircuitProofSystem(kind, inp, out, security).prove()
+    assert of.verify(ci.KINDS[kind], inp, out, security, proof) == 0
+    bad = bytearray(proof)
+    bad[len(bad) // 2] ^= 0x10
+    assert of.verify(ci.KINDS[kind], inp, out, security, bytes(bad)) != 0
+
+
+def test_large_proof_is_accepted_by_the_restated_verifier():
+    """sha256-chain n=1024 at 128 bits (unique decoding, no OOD): a
+    multi-million-entry witness, checked by the verifier instead of a second
+    proof on the CPU."""
+    inp, out, _ = ci.instance("sha256-chain", 1024, 2)
+    proof, _ = bz.CircuitProofSystem("sha256-chain", inp, out, 128).prove()
+    assert of.verify(ci.KINDS["sha256-chain"], inp, out, 128, proof) == 0
