@@ -160,11 +160,12 @@ def peaks():
         return {"hbm_gbs": FALLBACK_HBM_GBS}, "fallback"
 
 
-def traffic_per_launch():
-    """DRAM bytes per launch of the probed kernel from its ncu summary, or None."""
+def profile_figure(key):
+    """A figure of the probed kernel's ncu summary (e.g. DRAM bytes per
+    launch), or None."""
     try:
         for line in open(TRAFFIC_SUMMARY):
-            if line.startswith("traffic_bytes_per_launch:"):
+            if line.startswith(key + ":"):
                 return float(line.split(":", 1)[1])
     except OSError:
         pass
@@ -376,7 +377,7 @@ def ours(args):
     if rank == 0:
         pk, pk_kind = peaks()
         achieved = probe_bytes / (probe_ms / 1000.0) / 1e9 if probe_ms > 0 else None
-        per_launch = traffic_per_launch()
+        per_launch = profile_figure("traffic_bytes_per_launch")
         line = {
             "metric": "SHA-256 blocks proven/sec", "value": value, "unit": "blocks/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": statistics.mean(spans),
@@ -398,7 +399,10 @@ def ours(args):
                          "algorithmic_bytes_per_launch": probe_bytes / probe_launches if probe_launches else None,
                          "launches": probe_launches,
                          "avg_launch_us": 1000 * probe_ms / probe_launches if probe_launches else None,
-                         "share_of_device_time": probe_ms / sum(spans) if spans else None},
+                         "share_of_device_time": probe_ms / sum(spans) if spans else None,
+                         "integer_issue_active_ncu": profile_figure("issue_active_largest_launch"),
+                         "note": "integer-issue bound (GF(2^128) products), not HBM bound: "
+                                 "see profiles/gkr_bind_sums_sha256-chain-n64.md"},
             "clocks": clk.summary(),
             "proof_bytes": len(proof),
             "peaks": pk_kind,
