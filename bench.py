@@ -53,7 +53,7 @@ def parse():
     p.add_argument("--blocks", type=int, default=64)
     p.add_argument("--seed", type=int, default=1)
     p.add_argument("--security", type=int, default=100)
-    p.add_argument("--lanes", type=int, default=12)
+    p.add_argument("--lanes", type=int, default=16)
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-batch", action="store_true")
     p.add_argument("--serve", action="store_true")

@@ -375,4 +375,27 @@ void query_basis(const f128 *w, const f128 *scale, int nq, int l, f128 *basis, c
   BZ_LAUNCH_CHECK();
 }
 
+// The opened rows and their Merkle paths, in proof order: per query the row
+// (width entries of 16 bytes), then the sibling of every node from the leaf
+// (rows + idx) up to the root's children (32 bytes each). One block per query.
+__global__ void k_gather_openings(const f128 *__restrict__ cw, const uint32_t *__restrict__ nodes,
+                                  size_t rows, int width, int depth,
+                                  const uint64_t *__restrict__ idx, f128 *__restrict__ out) {
+  const size_t stride = (size_t)width + 2 * (size_t)depth;  // in 16-byte units
+  f128 *o = out + blockIdx.x * stride;
+  const uint64_t id = idx[blockIdx.x];
+  for (int c = threadIdx.x; c < width; c += blockDim.x) st(o + c, ld(cw + id * width + c));
+  for (int k = threadIdx.x; k < 2 * depth; k += blockDim.x) {
+    const int d = k >> 1, half = k & 1;
+    const size_t sib = ((rows + id) >> d) ^ 1;
+    st(o + width + k, ld(reinterpret_cast<const f128 *>(nodes + 8 * sib) + half));
+  }
+}
+
+void gather_openings(const f128 *cw, const uint32_t *nodes, size_t rows, int width, int depth,
+                     const uint64_t *idx, int nq, f128 *out, cudaStream_t s) {
+  k_gather_openings<<<nq, 64, 0, s>>>(cw, nodes, rows, width, depth, idx, out);
+  BZ_LAUNCH_CHECK();
+}
+
 }  // namespace bz

@@ -27,6 +27,10 @@ void rs_encode(const f128 *msg, int log_n, int k, int rate, const f128 *wh, f128
                cudaStream_t s);
 void merkle_build(const f128 *cw, size_t rows, int k, uint32_t *nodes, cudaStream_t s);
 void query_basis(const f128 *w, const f128 *scale, int nq, int l, f128 *basis, cudaStream_t s);
+// Per query (idx[q] < rows): the codeword row and its Merkle siblings, packed
+// as width + 2 * depth 16-byte units.
+void gather_openings(const f128 *cw, const uint32_t *nodes, size_t rows, int width, int depth,
+                     const uint64_t *idx, int nq, f128 *out, cudaStream_t s);
 
 // Host helpers (GF(2^128) on the CPU for the few scalar steps).
 f128 gf_inv_host(f128 a);

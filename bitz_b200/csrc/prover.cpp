@@ -227,6 +227,11 @@ Tables &tables(cudaStream_t s) {
 
 }  // namespace
 
+// Slots of Workspace::pin_small, the page-locked home of the small
+// device-to-host reads (16-byte units).
+constexpr size_t kPinFlag = 0, kPinRoot = 1, kPinLevelRoot = 3, kPinW0 = 5, kPinOne = 6,
+                 kPinClaims = 8, kPinSmall = 8 + 128;
+
 // Per-lane device workspace, grown on demand.
 struct Workspace {
   DeviceBuffer<uint32_t> states, msgs_u32;
@@ -245,6 +250,13 @@ struct Workspace {
   // while the host absorbs earlier messages
   DeviceBuffer<fp> cols_canon;
   PinnedBuffer<u128> host_cols, host_folds;
+  // Ligerito: the next levels' codewords and trees, the query indices and the
+  // gathered openings, with their host copies
+  DeviceBuffer<f128> lig_cw[2], openings;
+  DeviceBuffer<uint32_t> lig_nodes[2];
+  DeviceBuffer<uint64_t> qidx;
+  PinnedBuffer<uint64_t> pin_idx;
+  PinnedBuffer<f128> pin_open, pin_f, pin_b, pin_qw, pin_small;
   cudaEvent_t ev_cols = nullptr, ev_folds = nullptr;
   Workspace() {
     BZ_CUDA(cudaMallocHost(&host_fp, 8 * sizeof(fp)));
@@ -369,10 +381,10 @@ int ProofSystem::witness(cudaStream_t s) {
   a.prod = prod_.get();
   a.unsat = W.flag.get();
   witness_generate(a, s);
-  int unsat = 0;
-  BZ_CUDA(cudaMemcpyAsync(&unsat, W.flag.get(), sizeof(int), cudaMemcpyDeviceToHost, s));
+  int *unsat_h = reinterpret_cast<int *>(W.pin_small.get(kPinSmall) + kPinFlag);
+  BZ_CUDA(cudaMemcpyAsync(unsat_h, W.flag.get(), sizeof(int), cudaMemcpyDeviceToHost, s));
   BZ_CUDA(cudaStreamSynchronize(s));
-  if (unsat) {
+  if (*unsat_h) {
     error = "circuit witness does not satisfy the constraints";
     return BZ_ERR_UNSATISFIED;
   }
@@ -441,8 +453,10 @@ int ProofSystem::commit(cudaStream_t s) {
   const f128 *fpk = reinterpret_cast<const f128 *>(f_.get());
   rs_encode(fpk, log_n, L0.k, L0.log_inv_rate, T.wh.get(), codeword0_.get(), s);
   merkle_build(codeword0_.get(), rows, L0.k, nodes0_.get(), s);
-  BZ_CUDA(cudaMemcpyAsync(root_, nodes0_.get() + 8, 32, cudaMemcpyDeviceToHost, s));
+  f128 *root_h = W.pin_small.get(kPinSmall) + kPinRoot;
+  BZ_CUDA(cudaMemcpyAsync(root_h, nodes0_.get() + 8, 32, cudaMemcpyDeviceToHost, s));
   BZ_CUDA(cudaStreamSynchronize(s));
+  memcpy(root_, root_h, 32);
   const char *dom = circuit_name(kind_);
   ts_.reset(new Transcript((const uint8_t *)"bitz/circuit-e2e/v2", 19, (const uint8_t *)dom,
                            strlen(dom)));
@@ -518,8 +532,8 @@ std::vector<uint8_t> ProofSystem::ligerito(cudaStream_t s, f128 target) {
   const uint32_t *nodes = nodes0_.get();
   int cur_k = cfg.levels[0].k;
   size_t cur_rows = (size_t)1 << (cfg.log_n - cur_k + cfg.levels[0].log_inv_rate);
-  DeviceBuffer<f128> next_cw[2];
-  DeviceBuffer<uint32_t> next_nodes[2];
+  DeviceBuffer<f128> *next_cw = W.lig_cw;
+  DeviceBuffer<uint32_t> *next_nodes = W.lig_nodes;
   int flip = 0;
   unsigned long long *acc = W.acc.get();
   RoundChannel *ch = lane_->channel();
@@ -556,11 +570,13 @@ std::vector<uint8_t> ProofSystem::ligerito(cudaStream_t s, f128 target) {
       next_nodes[flip].resize(16 * nrows);
       rs_encode(f, l, N.k, N.log_inv_rate, T.wh.get(), next_cw[flip].get(), s);
       merkle_build(next_cw[flip].get(), nrows, N.k, next_nodes[flip].get(), s);
+      f128 *root_h = W.pin_small.get(kPinSmall) + kPinLevelRoot;
+      BZ_CUDA(cudaMemcpyAsync(root_h, next_nodes[flip].get() + 8, 32, cudaMemcpyDeviceToHost, s));
+      BZ_CUDA(cudaStreamSynchronize(s));
       uint8_t root[36];
       uint32_t len = 32;
       memcpy(root, &len, 4);
-      BZ_CUDA(cudaMemcpyAsync(root + 4, next_nodes[flip].get() + 8, 32, cudaMemcpyDeviceToHost, s));
-      BZ_CUDA(cudaStreamSynchronize(s));
+      memcpy(root + 4, root_h, 32);
       t.prover_message(root, 36);
       if (N.ood_samples) {
         std::vector<f128> pt = sample_vec((size_t)l);
@@ -576,39 +592,38 @@ std::vector<uint8_t> ProofSystem::ligerito(cudaStream_t s, f128 target) {
         claim = gadd(claim, gmul(mu, v));
       }
     } else {
-      std::vector<f128> hf(n);
-      BZ_CUDA(cudaMemcpyAsync(hf.data(), f, n * 16, cudaMemcpyDeviceToHost, s));
+      f128 *hf = W.pin_f.get(n);
+      BZ_CUDA(cudaMemcpyAsync(hf, f, n * 16, cudaMemcpyDeviceToHost, s));
       BZ_CUDA(cudaStreamSynchronize(s));
       uint32_t cnt = (uint32_t)n;
       t.prover_message(&cnt, 4);
-      for (auto &x : hf) t.prover_f128(x);
+      t.prover_message(hf, n * 16);  // one f128 message per entry, no framing between
     }
-    // queries into this level's codeword
+    // queries into this level's codeword: the rows and Merkle paths are
+    // gathered on the device and only they cross to the host
     grind();
     std::vector<f128> qs = sample_vec((size_t)L.queries);
     int width = 1 << cur_k;
     int depth = ceil_log2(cur_rows);
-    std::vector<f128> hcw(cur_rows << cur_k);
-    std::vector<uint32_t> hnodes(16 * cur_rows);
-    BZ_CUDA(cudaMemcpyAsync(hcw.data(), cw, hcw.size() * 16, cudaMemcpyDeviceToHost, s));
-    BZ_CUDA(cudaMemcpyAsync(hnodes.data(), nodes, hnodes.size() * 4, cudaMemcpyDeviceToHost, s));
+    const size_t stride = (size_t)width + 2 * (size_t)depth;  // 16-byte units per query
+    uint64_t *idx = W.pin_idx.get(L.queries);
+    for (int q = 0; q < L.queries; q++) idx[q] = qs[q].lo & (cur_rows - 1);
+    W.qidx.resize(L.queries);
+    BZ_CUDA(cudaMemcpyAsync(W.qidx.get(), idx, (size_t)L.queries * 8, cudaMemcpyHostToDevice, s));
+    W.openings.resize(stride * L.queries);
+    gather_openings(cw, nodes, cur_rows, width, depth, W.qidx.get(), L.queries, W.openings.get(), s);
+    f128 *opened = W.pin_open.get(stride * L.queries);
+    BZ_CUDA(cudaMemcpyAsync(opened, W.openings.get(), stride * L.queries * 16,
+                            cudaMemcpyDeviceToHost, s));
     BZ_CUDA(cudaStreamSynchronize(s));
     put_u64(proof, (uint64_t)L.queries);
+    const uint8_t *ob = reinterpret_cast<const uint8_t *>(opened);
+    proof.insert(proof.end(), ob, ob + stride * L.queries * 16);
     std::vector<f128> eqr((size_t)1 << L.k);
     eq_table_host(rs.data(), L.k, eqr.data());
     std::vector<f128> vals(L.queries);
-    std::vector<uint64_t> idx(L.queries);
     for (int q = 0; q < L.queries; q++) {
-      idx[q] = qs[q].lo & (cur_rows - 1);
-      const f128 *row = hcw.data() + idx[q] * width;
-      const uint8_t *rb = reinterpret_cast<const uint8_t *>(row);
-      proof.insert(proof.end(), rb, rb + 16 * width);
-      size_t node = cur_rows + idx[q];
-      for (int d = 0; d < depth; d++) {
-        const uint8_t *sib = reinterpret_cast<const uint8_t *>(hnodes.data() + 8 * (node ^ 1));
-        proof.insert(proof.end(), sib, sib + 32);
-        node >>= 1;
-      }
+      const f128 *row = opened + q * stride;
       wide v = wzero();
       for (int c = 0; c < width; c++) wacc(v, gmul_wide(row[c], eqr[c]));
       vals[q] = greduce(v);
@@ -619,19 +634,23 @@ std::vector<uint8_t> ProofSystem::ligerito(cudaStream_t s, f128 target) {
     std::vector<f128> beta((size_t)1 << av);
     eq_table_host(alpha.data(), av, beta.data());
     // glue: basis += sum_q s_q X(x_q) with X_j(x) = prod_{t in j} Wh_t(x)
-    std::vector<f128> wq((size_t)L.queries * kMaxRsDim), sq(L.queries);
+    const size_t nwq = (size_t)L.queries * kMaxRsDim;
+    f128 *wq = W.pin_qw.get(nwq + L.queries), *sq = wq + nwq;
     for (int q = 0; q < L.queries; q++) {
       sq[q] = gmul(mu, beta[q]);
       claim = gadd(claim, gmul(sq[q], vals[q]));
-      for (int tt = 0; tt < l; tt++) {
+      for (int tt = 0; tt < kMaxRsDim; tt++) {
         f128 w = mk(0, 0);
-        for (int sb = tt; sb < kMaxRsDim; sb++)
-          if ((idx[q] >> sb) & 1) w = gadd(w, T.wh_host[tt * kMaxRsDim + sb]);
+        if (tt < l)
+          for (int sb = tt; sb < kMaxRsDim; sb++)
+            if ((idx[q] >> sb) & 1) w = gadd(w, T.wh_host[tt * kMaxRsDim + sb]);
         wq[(size_t)q * kMaxRsDim + tt] = w;
       }
     }
-    W.qw.upload(wq.data(), wq.size(), s);
-    W.qs.upload(sq.data(), sq.size(), s);
+    W.qw.resize(nwq);
+    W.qs.resize(L.queries);
+    BZ_CUDA(cudaMemcpyAsync(W.qw.get(), wq, nwq * 16, cudaMemcpyHostToDevice, s));
+    BZ_CUDA(cudaMemcpyAsync(W.qs.get(), sq, (size_t)L.queries * 16, cudaMemcpyHostToDevice, s));
     query_basis(W.qw.get(), W.qs.get(), L.queries, l, b, s);
     if (!last) {
       cw = next_cw[flip].get();
@@ -642,9 +661,9 @@ std::vector<uint8_t> ProofSystem::ligerito(cudaStream_t s, f128 target) {
     }
   }
   // the final vector meets its basis
-  std::vector<f128> hf(n), hb(n);
-  BZ_CUDA(cudaMemcpyAsync(hf.data(), f, n * 16, cudaMemcpyDeviceToHost, s));
-  BZ_CUDA(cudaMemcpyAsync(hb.data(), b, n * 16, cudaMemcpyDeviceToHost, s));
+  f128 *hf = W.pin_f.get(n), *hb = W.pin_b.get(n);
+  BZ_CUDA(cudaMemcpyAsync(hf, f, n * 16, cudaMemcpyDeviceToHost, s));
+  BZ_CUDA(cudaMemcpyAsync(hb, b, n * 16, cudaMemcpyDeviceToHost, s));
   BZ_CUDA(cudaStreamSynchronize(s));
   f128 chk = mk(0, 0);
   for (size_t j = 0; j < n; j++) chk = gadd(chk, gmul(hb[j], hf[j]));
@@ -830,8 +849,8 @@ int ProofSystem::prove_after_commit(cudaStream_t s, std::vector<uint8_t> &proof)
   W.w0.resize(2);
   mt_transpose(dev_->csc_off.get(), dev_->csc_row.get(), S.f_bits + 1, W.u1.get(), W.u2.get(),
                W.weights.get(), nbits, W.w0.get(), s);
-  f128 w0;
-  BZ_CUDA(cudaMemcpyAsync(&w0, W.w0.get(), 16, cudaMemcpyDeviceToHost, s));
+  f128 *w0_h = W.pin_small.get(kPinSmall) + kPinW0;
+  BZ_CUDA(cudaMemcpyAsync(w0_h, W.w0.get(), 16, cudaMemcpyDeviceToHost, s));
   // the inner-product statement's weight digest (opening.rs:337-368)
   size_t nchunks = nbits * 16 / 1024;
   W.b3.resize(16 * nchunks);
@@ -853,7 +872,7 @@ int ProofSystem::prove_after_commit(cudaStream_t s, std::vector<uint8_t> &proof)
     b3_compress(dk.key, pm, 0, 64, B3_DERIVE_KEY_MATERIAL | B3_PARENT | B3_ROOT, out);
     b3_store_le(out, digest, 8);
   }
-  f128 target2 = gadd(ip_target, w0);
+  f128 target2 = gadd(ip_target, *w0_h);
   t.public_message("bitz/pcs/bit-inner-product/v3", 29);
   t.public_message(root_, 32);
   t.public_message(pcs_enc_.data(), pcs_enc_.size());
@@ -865,8 +884,9 @@ int ProofSystem::prove_after_commit(cudaStream_t s, std::vector<uint8_t> &proof)
   ph.mark("transpose+digest");
   // post-GKR sumcheck
   W.ones.resize(1);
-  f128 one = mk(1, 0);
-  BZ_CUDA(cudaMemcpyAsync(W.ones.get(), &one, 16, cudaMemcpyHostToDevice, s));
+  f128 *one_h = W.pin_small.get(kPinSmall) + kPinOne;
+  *one_h = mk(1, 0);
+  BZ_CUDA(cudaMemcpyAsync(W.ones.get(), one_h, 16, cudaMemcpyHostToDevice, s));
   PostGkrArgs pa;
   pa.rows = W.weights.get();
   pa.log_rows = S.committed_m;
@@ -899,9 +919,10 @@ int ProofSystem::prove_after_commit(cudaStream_t s, std::vector<uint8_t> &proof)
   eq_table_device(rho.data() + 7, log_n, W.suffix.get(), W.eqs.get(), s);
   BZ_CUDA(cudaMemsetAsync(W.acc.get(), 0, 256 * 8, s));
   ring_claims(pa.packed, W.suffix.get(), np, W.acc.get(), s);
-  std::vector<f128> claims(128);
-  BZ_CUDA(cudaMemcpyAsync(claims.data(), W.acc.get(), 128 * 16, cudaMemcpyDeviceToHost, s));
+  f128 *claims_h = W.pin_small.get(kPinSmall) + kPinClaims;
+  BZ_CUDA(cudaMemcpyAsync(claims_h, W.acc.get(), 128 * 16, cudaMemcpyDeviceToHost, s));
   BZ_CUDA(cudaStreamSynchronize(s));
+  std::vector<f128> claims(claims_h, claims_h + 128);
   {
     std::vector<f128> pre(128);
     eq_table_host(rho.data(), 7, pre.data());
