@@ -54,6 +54,7 @@ SIGNATURES = [
      [_vp, _vp, ctypes.c_size_t, _vp, ctypes.c_size_t, _vp, ctypes.c_size_t]),
     ("bitz_circuit_layout", ctypes.c_int,
      [ctypes.c_int, ctypes.c_size_t, _u64p, _u8p, _vp, _vp, _vp, _vp, _vp]),
+    ("bitz_statement_digest", ctypes.c_int, [ctypes.c_int, _vp, ctypes.c_size_t, _vp, _u8p]),
     ("bitz_batch_prove", ctypes.c_int,
      [_vp, ctypes.c_size_t, ctypes.c_int, _vp, _vp, _vp]),
     ("bitz_server_start", ctypes.c_int,

@@ -18,6 +18,9 @@ struct bitz_system {
 namespace bz {
 int capi_fail(int code, const std::string &msg);
 
+// integer_matrix_digest with the statement's bit constants (circuit.cpp)
+void matrix_digest(const CircuitSetup &S, const std::vector<int64_t> &expected_c, uint8_t out[32]);
+
 // Input checks of CircuitProofSystem::new (circuits.rs:58-210 dimensions).
 int check_statement(int circuit_kind, const uint8_t *input_bits, size_t n_inputs,
                     const uint8_t *output_bits, uint32_t security_bits) {
@@ -159,6 +162,24 @@ int bitz_circuit_layout(int circuit_kind, size_t n_inputs, uint64_t sizes[8],
     if (c_off) memcpy(c_off, S.abc[2].off.data(), S.abc[2].off.size() * 4);
     if (c_col) memcpy(c_col, S.abc[2].col.data(), S.abc[2].col.size() * 4);
     if (c_coef) memcpy(c_coef, S.abc[2].coef.data(), S.abc[2].coef.size() * 8);
+    return BZ_OK;
+  } catch (const std::exception &e) {
+    return capi_fail(BZ_ERR_INTERNAL, e.what());
+  }
+}
+
+int bitz_statement_digest(int circuit_kind, const uint8_t *input_bits, size_t n_inputs,
+                          const uint8_t *output_bits, uint8_t digest[32]) {
+  if (!digest) return capi_fail(BZ_ERR_ARGUMENT, "null argument");
+  int rc = check_statement(circuit_kind, input_bits, n_inputs, output_bits, 100);
+  if (rc) return rc;
+  try {
+    CircuitSetup S;
+    build_circuit_setup(circuit_kind, n_inputs, S);
+    std::vector<int64_t> ex(n_inputs + 256);
+    for (size_t i = 0; i < n_inputs; i++) ex[i] = input_bits[i];
+    for (int i = 0; i < 256; i++) ex[n_inputs + i] = output_bits[i];
+    matrix_digest(S, ex, digest);
     return BZ_OK;
   } catch (const std::exception &e) {
     return capi_fail(BZ_ERR_INTERNAL, e.what());

@@ -1,6 +1,7 @@
 // Symbolic replay of the SHA-256 circuits (setup only: no witness values).
 #include "circuit.hpp"
 
+#include <immintrin.h>
 #include <string.h>
 
 #include <algorithm>
@@ -450,6 +451,80 @@ void sha256_host(const uint8_t *in, size_t len, uint8_t out[32]) {
   }
 }
 
+// SHA-256 over many blocks: the SHA extensions where the CPU has them (the
+// published SHA-NI round and message-schedule instruction sequence), else the
+// portable compression. The dispatch checks the extension against the
+// portable code on one block before trusting it.
+__attribute__((target("sha,sse4.1"))) static void sha256_blocks_ni(uint32_t st[8],
+                                                                   const uint8_t *p,
+                                                                   size_t nblocks) {
+  const __m128i bswap = _mm_set_epi64x(0x0c0d0e0f08090a0bULL, 0x0405060700010203ULL);
+  __m128i tmp = _mm_loadu_si128((const __m128i *)&st[0]);  // D C B A
+  __m128i s1 = _mm_loadu_si128((const __m128i *)&st[4]);   // H G F E
+  tmp = _mm_shuffle_epi32(tmp, 0xB1);                       // C D A B
+  s1 = _mm_shuffle_epi32(s1, 0x1B);                         // E F G H
+  __m128i s0 = _mm_alignr_epi8(tmp, s1, 8);                 // A B E F
+  s1 = _mm_blend_epi16(s1, tmp, 0xF0);                      // C D G H
+  for (; nblocks; nblocks--, p += 64) {
+    const __m128i abef = s0, cdgh = s1;
+    __m128i w[4];
+    for (int g = 0; g < 16; g++) {
+      __m128i wg;
+      if (g < 4) {
+        wg = _mm_shuffle_epi8(_mm_loadu_si128((const __m128i *)(p + 16 * g)), bswap);
+      } else {
+        // W[4g..4g+3] from the four previous groups
+        __m128i a = w[g & 3], b = w[(g + 1) & 3], c = w[(g + 2) & 3], d = w[(g + 3) & 3];
+        wg = _mm_sha256msg2_epu32(
+            _mm_add_epi32(_mm_sha256msg1_epu32(a, b), _mm_alignr_epi8(d, c, 4)), d);
+      }
+      w[g & 3] = wg;
+      __m128i msg = _mm_add_epi32(wg, _mm_loadu_si128((const __m128i *)&SHA_K[4 * g]));
+      s1 = _mm_sha256rnds2_epu32(s1, s0, msg);
+      s0 = _mm_sha256rnds2_epu32(s0, s1, _mm_shuffle_epi32(msg, 0x0E));
+    }
+    s0 = _mm_add_epi32(s0, abef);
+    s1 = _mm_add_epi32(s1, cdgh);
+  }
+  tmp = _mm_shuffle_epi32(s0, 0x1B);   // F E B A
+  s1 = _mm_shuffle_epi32(s1, 0xB1);    // D C H G
+  s0 = _mm_blend_epi16(tmp, s1, 0xF0); // D C B A
+  s1 = _mm_alignr_epi8(s1, tmp, 8);    // H G F E
+  _mm_storeu_si128((__m128i *)&st[0], s0);
+  _mm_storeu_si128((__m128i *)&st[4], s1);
+}
+
+static void sha256_blocks_portable(uint32_t s[8], const uint8_t *p, size_t nblocks) {
+  uint32_t m[16];
+  for (; nblocks; nblocks--, p += 64) {
+    for (int i = 0; i < 16; i++)
+      m[i] = (uint32_t)p[4 * i] << 24 | (uint32_t)p[4 * i + 1] << 16 | (uint32_t)p[4 * i + 2] << 8 |
+             p[4 * i + 3];
+    sha256_compress_host(s, m);
+  }
+}
+
+static bool sha_ni_usable() {
+  if (!__builtin_cpu_supports("sha") || !__builtin_cpu_supports("sse4.1")) return false;
+  uint8_t blk[128];
+  for (int i = 0; i < 128; i++) blk[i] = (uint8_t)(i * 37 + 11);
+  uint32_t a[8] = {0x6a09e667, 0xbb67ae85, 0x3c6ef372, 0xa54ff53a,
+                   0x510e527f, 0x9b05688c, 0x1f83d9ab, 0x5be0cd19};
+  uint32_t b[8];
+  memcpy(b, a, sizeof a);
+  sha256_blocks_ni(a, blk, 2);
+  sha256_blocks_portable(b, blk, 2);
+  return memcmp(a, b, sizeof a) == 0;
+}
+
+static void sha256_blocks(uint32_t s[8], const uint8_t *p, size_t nblocks) {
+  static const bool ni = sha_ni_usable();
+  if (ni)
+    sha256_blocks_ni(s, p, nblocks);
+  else
+    sha256_blocks_portable(s, p, nblocks);
+}
+
 // SHA-256 over a byte stream fed in pieces (the digest input is large).
 struct Sha256Stream {
   uint32_t s[8] = {0x6a09e667, 0xbb67ae85, 0x3c6ef372, 0xa54ff53a,
@@ -457,26 +532,24 @@ struct Sha256Stream {
   uint8_t buf[64];
   size_t n = 0;
   uint64_t total = 0;
-  void block(const uint8_t *p) {
-    uint32_t m[16];
-    for (int i = 0; i < 16; i++)
-      m[i] = (uint32_t)p[4 * i] << 24 | (uint32_t)p[4 * i + 1] << 16 | (uint32_t)p[4 * i + 2] << 8 |
-             p[4 * i + 3];
-    sha256_compress_host(s, m);
-  }
   void update(const uint8_t *p, size_t len) {
     total += len;
-    while (len) {
+    if (n) {
       size_t take = 64 - n < len ? 64 - n : len;
       memcpy(buf + n, p, take);
       n += take;
       p += take;
       len -= take;
-      if (n == 64) {
-        block(buf);
-        n = 0;
-      }
+      if (n < 64) return;
+      sha256_blocks(s, buf, 1);
+      n = 0;
     }
+    size_t full = len / 64;
+    if (full) sha256_blocks(s, p, full);
+    p += 64 * full;
+    len -= 64 * full;
+    memcpy(buf, p, len);
+    n = len;
   }
   void u64(uint64_t v) {
     uint8_t b[8];
@@ -485,12 +558,11 @@ struct Sha256Stream {
   }
   void finish(uint8_t out[32]) {
     uint64_t bits = total * 8;
-    uint8_t pad = 0x80;
-    update(&pad, 1);
-    uint8_t z = 0;
-    while (n != 56) update(&z, 1);
+    uint8_t pad[72] = {0x80};
+    size_t padlen = n < 56 ? 56 - n : 120 - n;
     uint8_t l[8];
     for (int i = 0; i < 8; i++) l[i] = (uint8_t)(bits >> (56 - 8 * i));
+    update(pad, padlen);
     update(l, 8);
     for (int i = 0; i < 8; i++) {
       out[4 * i] = (uint8_t)(s[i] >> 24);
@@ -501,44 +573,95 @@ struct Sha256Stream {
   }
 };
 
-void matrix_digest(const CircuitSetup &S, const std::vector<int64_t> &expected_c,
-                   uint8_t out[32]) {
-  Sha256Stream h;
-  const char *dom = "bitz/spartan/integer-constraint-matrices/v1";
-  h.update((const uint8_t *)dom, strlen(dom));
-  h.update((const uint8_t *)"M", 1);
-  h.u64(S.h_len);
-  h.u64(S.f_bits + 1);
-  for (size_t r = 0; r < S.h_len; r++) {
-    h.u64(S.m_off[r + 1] - S.m_off[r]);
-    for (uint32_t e = S.m_off[r]; e < S.m_off[r + 1]; e++) h.u64(S.m_pos[e]);
+// Little-endian u64 words gathered into 16 KB before they reach the hash.
+struct WordSink {
+  Sha256Stream &h;
+  uint8_t buf[16384];
+  size_t n = 0;
+  explicit WordSink(Sha256Stream &hh) : h(hh) {}
+  ~WordSink() { flush(); }
+  void flush() {
+    if (n) h.update(buf, n);
+    n = 0;
   }
-  const char lab[3] = {'A', 'B', 'C'};
-  size_t n_bits = S.n_inputs;  // bit-constraint rows: inputs first, outputs last
-  for (int k = 0; k < 3; k++) {
-    h.update((const uint8_t *)&lab[k], 1);
-    h.u64(S.rows);
-    h.u64(S.h_len);
+  void bytes(const void *p, size_t len) {
+    flush();
+    h.update((const uint8_t *)p, len);
+  }
+  void u64(uint64_t v) {
+    if (n + 8 > sizeof buf) flush();
+    for (int i = 0; i < 8; i++) buf[n + i] = (uint8_t)(v >> (8 * i));
+    n += 8;
+  }
+};
+
+// The statement-independent prefix of the integer-matrix digest (the domain,
+// M, A and B): hashed once per circuit shape, resumed per statement.
+static void digest_prefix(const CircuitSetup &S, Sha256Stream &h) {
+  WordSink w(h);
+  const char *dom = "bitz/spartan/integer-constraint-matrices/v1";
+  w.bytes(dom, strlen(dom));
+  w.bytes("M", 1);
+  w.u64(S.h_len);
+  w.u64(S.f_bits + 1);
+  for (size_t r = 0; r < S.h_len; r++) {
+    w.u64(S.m_off[r + 1] - S.m_off[r]);
+    for (uint32_t e = S.m_off[r]; e < S.m_off[r + 1]; e++) w.u64(S.m_pos[e]);
+  }
+  const char lab[2] = {'A', 'B'};
+  for (int k = 0; k < 2; k++) {
+    w.bytes(&lab[k], 1);
+    w.u64(S.rows);
+    w.u64(S.h_len);
     const Matrix &M = S.abc[k];
     for (size_t r = 0; r < S.rows; r++) {
+      w.u64(M.off[r + 1] - M.off[r]);
+      for (uint32_t e = M.off[r]; e < M.off[r + 1]; e++) {
+        w.u64(M.col[e]);
+        w.u64(1);  // a nonzero i64 coefficient is one canonical word
+        w.u64((uint64_t)M.coef[e]);
+      }
+    }
+  }
+}
+
+void matrix_digest(const CircuitSetup &S, const std::vector<int64_t> &expected_c,
+                   uint8_t out[32]) {
+  // Only C holds statement-dependent entries (the bit constraints' expected
+  // values); the hash state after the domain, M, A and B is cached per shape.
+  static_assert(sizeof(Sha256Stream) <= sizeof(S.digest_prefix_state), "prefix slot too small");
+  std::call_once(*S.digest_prefix_once, [&] {
+    Sha256Stream h;
+    digest_prefix(S, h);
+    memcpy(S.digest_prefix_state, &h, sizeof h);
+  });
+  Sha256Stream h;
+  memcpy(&h, S.digest_prefix_state, sizeof h);
+  {
+    WordSink w(h);
+    size_t n_bits = S.n_inputs;  // bit-constraint rows: inputs first, outputs last
+    w.bytes("C", 1);
+    w.u64(S.rows);
+    w.u64(S.h_len);
+    const Matrix &M = S.abc[2];
+    for (size_t r = 0; r < S.rows; r++) {
       bool bitrow = r < n_bits || r >= S.rows - 256;
-      if (k == 2 && bitrow) {
+      if (bitrow) {
         size_t bi = r < n_bits ? r : n_bits + (r - (S.rows - 256));
         int64_t v = expected_c[bi];
-        h.u64(v ? 1 : 0);
+        w.u64(v ? 1 : 0);
         if (v) {
-          h.u64(0);
-          h.u64(1);
-          h.u64((uint64_t)v);
+          w.u64(0);
+          w.u64(1);
+          w.u64((uint64_t)v);
         }
         continue;
       }
-      h.u64(M.off[r + 1] - M.off[r]);
+      w.u64(M.off[r + 1] - M.off[r]);
       for (uint32_t e = M.off[r]; e < M.off[r + 1]; e++) {
-        h.u64(M.col[e]);
-        int64_t v = M.coef[e];
-        h.u64(1);  // a nonzero i64 coefficient is one canonical word
-        h.u64((uint64_t)v);
+        w.u64(M.col[e]);
+        w.u64(1);
+        w.u64((uint64_t)M.coef[e]);
       }
     }
   }

@@ -8,6 +8,8 @@
 #include <stdint.h>
 
 #include <string>
+#include <memory>
+#include <mutex>
 #include <vector>
 
 namespace bz {
@@ -42,6 +44,10 @@ struct CircuitSetup {
   uint8_t matrix_digest[32];
   int claim_log_cols = 0;  // s of the claim shape (7 row bits)
   int committed_m = 0;     // log2 of committed bits after padding
+  // the integer-matrix digest's hash state after its statement-independent
+  // prefix, computed on first use
+  std::shared_ptr<std::once_flag> digest_prefix_once = std::make_shared<std::once_flag>();
+  mutable uint8_t digest_prefix_state[160];
 };
 
 // Builds everything that does not depend on the witness. n_inputs is the

@@ -149,6 +149,12 @@ int bitz_system_witness(bitz_system *sys, uint32_t *f_words, size_t f_cap, uint3
 int bitz_circuit_layout(int circuit_kind, size_t n_inputs, uint64_t sizes[8],
                         uint8_t map_digest[32], uint32_t *m_off, uint32_t *m_pos,
                         uint32_t *c_off, uint32_t *c_col, int64_t *c_coef);
+/* Diagnostic (no reference counterpart): the statement's integer-matrix
+ * digest (crates/spartan/src/matrix.rs:562-661, SHA-256 over M, A, B and C
+ * with the bit constraints' expected values) as CircuitProofSystem::new
+ * absorbs it. Needs no GPU. */
+int bitz_statement_digest(int circuit_kind, const uint8_t *input_bits, size_t n_inputs,
+                          const uint8_t *output_bits, uint8_t digest[32]);
 
 /* ------------------------------------------------------ batch and serving
  * No reference counterpart: the reference proves one statement per call

@@ -1274,4 +1274,13 @@ int o_verify(int kind, const uint8_t *inputs, size_t n_inputs, const uint8_t *ex
   return verify_proof(kind, inputs, n_inputs, expected, security, proof, proof_len);
 }
 
+/* The statement's integer-matrix digest (crates/spartan/src/matrix.rs:562-661). */
+void o_matrix_digest(int kind, const uint8_t *inputs, size_t n_inputs, const uint8_t *expected,
+                     uint8_t out[32]) {
+  Setup s;
+  build_setup(s, kind, inputs, n_inputs, expected, 100);
+  memcpy(out, s.matrix_digest, 32);
+  o_circuit_free(s.circ);
+}
+
 }  // extern "C"

@@ -86,3 +86,32 @@ def test_per_compression_counts():
     # compression statement: 768 inputs + 6,376 hints; 1 + 768 + 20,456 + 256 lifts
     c = product_layout(0, 768)[0]
     assert c[0] == 7144 and c[1] == 21481 and c[2] == 1208
+
+
+@pytest.mark.parametrize("kind,blocks,seed", [("sha256-compression", 1, 3), ("sha256-chain", 2, 4),
+                                              ("sha256-block-aligned", 0, 5),
+                                              ("sha256-block-aligned", 3, 6), ("sha256-2kb", 32, 7)])
+def test_statement_digest_matches_oracle(kind, blocks, seed):
+    """The integer-matrix digest with the statement's bit constants
+    (crates/spartan/src/matrix.rs:562-661): the product hashes the
+    statement-independent prefix once per shape and resumes from it."""
+    st = ci.random_state(seed) if kind == "sha256-compression" else None
+    inp, out, _ = ci.instance(kind, blocks, seed, st)
+    L = _lib.load()
+    got = (ctypes.c_uint8 * 32)()
+    assert L.bitz_statement_digest(ci.KINDS[kind], inp.ctypes.data, inp.size, out.ctypes.data,
+                                   got) == 0
+    O = of.lib()
+    O.o_matrix_digest.restype = None
+    O.o_matrix_digest.argtypes = [ctypes.c_int, ctypes.c_void_p, ctypes.c_size_t, ctypes.c_void_p,
+                                  ctypes.c_void_p]
+    want = (ctypes.c_uint8 * 32)()
+    O.o_matrix_digest(ci.KINDS[kind], inp.ctypes.data, inp.size, out.ctypes.data, want)
+    assert bytes(got) == bytes(want)
+    # a different expected output changes the digest
+    out2 = out.copy()
+    out2[0] ^= 1
+    got2 = (ctypes.c_uint8 * 32)()
+    assert L.bitz_statement_digest(ci.KINDS[kind], inp.ctypes.data, inp.size, out2.ctypes.data,
+                                   got2) == 0
+    assert bytes(got2) != bytes(got)
