@@ -14,6 +14,7 @@
 #include <chrono>
 #include <condition_variable>
 #include <deque>
+#include <map>
 #include <memory>
 #include <mutex>
 #include <thread>
@@ -107,6 +108,7 @@ struct ServeRequest {
   std::vector<uint8_t> inputs, outputs;
   uint64_t footprint = 0;
   std::chrono::steady_clock::time_point submitted;
+  std::unique_ptr<ProofSystem> ps;  // the prepared statement
   bool done = false;
   int status = BZ_OK;
   std::string error;
@@ -114,26 +116,76 @@ struct ServeRequest {
   double latency_ms = 0;
 };
 
+// Two stages: preparer threads build each request's statement (the circuit
+// shape from the cache, the statement's matrix digest, the staged inputs: host
+// work), prover lanes prove prepared requests. A lane never idles on host-only
+// set-up while prepared work waits.
 struct bitz_server {
   int device = 0;
   uint32_t security = 100;
   uint64_t budget = 0;
-  std::vector<std::unique_ptr<Context>> lanes;
+  std::vector<std::unique_ptr<Context>> lanes, prep_lanes;
   std::vector<std::thread> workers;
   std::mutex mu;
-  std::condition_variable work_cv, done_cv;
-  std::deque<std::shared_ptr<ServeRequest>> queue;
+  std::condition_variable prep_cv, work_cv, done_cv;
+  std::deque<std::shared_ptr<ServeRequest>> queue;           // submitted, not prepared
+  std::map<uint64_t, std::shared_ptr<ServeRequest>> ready;   // prepared, by ticket
   std::unordered_map<uint64_t, std::shared_ptr<ServeRequest>> tickets;
   uint64_t next_ticket = 1, submitted = 0, finished = 0, in_flight = 0, in_flight_bytes = 0,
            peak_in_flight = 0;
   bool stopping = false;
 
-  // Admission: FIFO, a free lane, and the head's footprint fits the budget
-  // beside the requests in flight (always when none is in flight).
+  // Admission: oldest prepared request first, a free lane, and its footprint
+  // fits the budget beside the requests in flight (always when none is).
   bool admissible() const {
-    if (queue.empty()) return false;
-    uint64_t need = queue.front()->footprint;
+    if (ready.empty()) return false;
+    uint64_t need = ready.begin()->second->footprint;
     return in_flight == 0 || in_flight_bytes + need <= budget;
+  }
+
+  void finish(const std::shared_ptr<ServeRequest> &rq, int rc, std::string err,
+              std::vector<uint8_t> proof) {
+    auto t = std::chrono::steady_clock::now();
+    {
+      std::lock_guard<std::mutex> lk(mu);
+      rq->status = rc;
+      rq->error = std::move(err);
+      rq->proof = std::move(proof);
+      rq->latency_ms = ms_between(rq->submitted, t);
+      rq->ps.reset();
+      rq->done = true;
+      finished++;
+    }
+    done_cv.notify_all();
+  }
+
+  void prepare(Context *lane) {
+    cudaSetDevice(device);
+    for (;;) {
+      std::shared_ptr<ServeRequest> rq;
+      {
+        std::unique_lock<std::mutex> lk(mu);
+        prep_cv.wait(lk, [&] { return stopping || !queue.empty(); });
+        if (stopping) return;
+        rq = queue.front();
+        queue.pop_front();
+      }
+      try {
+        rq->ps.reset(new ProofSystem(rq->kind, rq->inputs.data(), rq->inputs.size(),
+                                     rq->outputs.data(), (int)security, lane));
+      } catch (const CudaError &e) {
+        finish(rq, BZ_ERR_CUDA, e.what(), {});
+        continue;
+      } catch (const std::exception &e) {
+        finish(rq, BZ_ERR_CONFIG, e.what(), {});
+        continue;
+      }
+      {
+        std::lock_guard<std::mutex> lk(mu);
+        ready[rq->ticket] = rq;
+      }
+      work_cv.notify_one();
+    }
   }
 
   void run(Context *lane) {
@@ -144,39 +196,32 @@ struct bitz_server {
         std::unique_lock<std::mutex> lk(mu);
         work_cv.wait(lk, [&] { return stopping || admissible(); });
         if (stopping) return;
-        rq = queue.front();
-        queue.pop_front();
+        rq = ready.begin()->second;
+        ready.erase(ready.begin());
         in_flight++;
         in_flight_bytes += rq->footprint;
         peak_in_flight = std::max(peak_in_flight, in_flight);
       }
       std::vector<uint8_t> proof;
       std::string err;
+      // the statement was staged on the device when it was prepared
       int rc;
       try {
-        ProofSystem ps(rq->kind, rq->inputs.data(), rq->inputs.size(), rq->outputs.data(),
-                       (int)security, lane);
-        rc = prove_on(ps, *lane, proof, err);
+        rc = rq->ps->prove(proof, nullptr, false, lane);
+        if (rc) err = rq->ps->error;
       } catch (const CudaError &e) {
         rc = BZ_ERR_CUDA;
         err = e.what();
       } catch (const std::exception &e) {
-        rc = BZ_ERR_CONFIG;
+        rc = BZ_ERR_INTERNAL;
         err = e.what();
       }
-      auto t = std::chrono::steady_clock::now();
       {
         std::lock_guard<std::mutex> lk(mu);
-        rq->status = rc;
-        rq->error = err;
-        rq->proof = std::move(proof);
-        rq->latency_ms = ms_between(rq->submitted, t);
-        rq->done = true;
         in_flight--;
         in_flight_bytes -= rq->footprint;
-        finished++;
       }
-      done_cv.notify_all();
+      finish(rq, rc, std::move(err), std::move(proof));
       work_cv.notify_all();
     }
   }
@@ -249,11 +294,14 @@ int bitz_server_start(int lanes, uint64_t hbm_budget_bytes, uint32_t security_bi
   srv->budget = hbm_budget_bytes;
   try {
     srv->lanes = LanePool::get().take(srv->device, lanes);
+    unsigned hw = std::thread::hardware_concurrency();
+    srv->prep_lanes = LanePool::get().take(srv->device, (int)std::max(2u, hw / 2));
   } catch (const std::exception &e) {
     delete srv;
     return capi_fail(BZ_ERR_CUDA, e.what());
   }
   for (auto &l : srv->lanes) srv->workers.emplace_back(&bitz_server::run, srv, l.get());
+  for (auto &l : srv->prep_lanes) srv->workers.emplace_back(&bitz_server::prepare, srv, l.get());
   *out = srv;
   return BZ_OK;
 }
@@ -278,7 +326,7 @@ int bitz_server_submit(bitz_server *srv, int circuit_kind, const uint8_t *input_
     srv->submitted++;
     *ticket = rq->ticket;
   }
-  srv->work_cv.notify_one();
+  srv->prep_cv.notify_one();
   return BZ_OK;
 }
 
@@ -309,7 +357,7 @@ int bitz_server_stats(bitz_server *srv, uint64_t out[6]) {
   out[0] = srv->submitted;
   out[1] = srv->finished;
   out[2] = srv->in_flight;
-  out[3] = srv->queue.size();
+  out[3] = srv->queue.size() + srv->ready.size();
   out[4] = srv->in_flight_bytes;
   out[5] = srv->peak_in_flight;
   return BZ_OK;
@@ -321,10 +369,13 @@ int bitz_server_stop(bitz_server *srv) {
     std::lock_guard<std::mutex> lk(srv->mu);
     srv->stopping = true;
     srv->queue.clear();
+    srv->ready.clear();
   }
   srv->work_cv.notify_all();
+  srv->prep_cv.notify_all();
   for (auto &t : srv->workers) t.join();
   LanePool::get().give(srv->device, srv->lanes);
+  LanePool::get().give(srv->device, srv->prep_lanes);
   delete srv;
   return BZ_OK;
 }

@@ -234,8 +234,6 @@ constexpr size_t kPinFlag = 0, kPinRoot = 1, kPinLevelRoot = 3, kPinW0 = 5, kPin
 
 // Per-lane device workspace, grown on demand.
 struct Workspace {
-  DeviceBuffer<uint32_t> states, msgs_u32;
-  DeviceBuffer<uint64_t> offsets;
   DeviceBuffer<int> flag;
   DeviceBuffer<fp> sp_t, sp_d, sp_eqs, sp_part, sp_sums, sp_tab;
   DeviceBuffer<fp> cols_fp;
@@ -257,6 +255,14 @@ struct Workspace {
   DeviceBuffer<uint64_t> qidx;
   PinnedBuffer<uint64_t> pin_idx;
   PinnedBuffer<f128> pin_open, pin_f, pin_b, pin_qw, pin_small;
+  // the proof's own state: the staged statement, the witness, the level-0
+  // codeword and tree
+  DeviceBuffer<uint32_t> states, msgs, fin, f, h, bit_rows, nodes0;
+  DeviceBuffer<uint64_t> offsets;
+  DeviceBuffer<int64_t> prod;
+  DeviceBuffer<uint8_t> bit_c;
+  DeviceBuffer<f128> codeword0;
+  uint64_t staged_serial = 0;  // the system whose statement these hold
   cudaEvent_t ev_cols = nullptr, ev_folds = nullptr;
   Workspace() {
     BZ_CUDA(cudaMallocHost(&host_fp, 8 * sizeof(fp)));
@@ -315,7 +321,8 @@ ProofSystem::ProofSystem(int kind, const uint8_t *inputs, size_t n_inputs, const
   put_u64(pcs_enc_, (uint64_t)1 << S.committed_m);
   for (int i = 0; i < 4; i++) pcs_enc_.push_back((uint8_t)((uint32_t)security_bits >> (8 * i)));
   prepare_statement(kind, S, inputs_, outputs_, states_h_, msgs_h_, fin_h_, bitc_h_);
-  stage_statement(s);
+  static std::atomic<uint64_t> serials{0};
+  serial_ = ++serials;
   BZ_CUDA(cudaEventCreate(&ev_start_));
   BZ_CUDA(cudaEventCreate(&ev_stop_));
   BZ_CUDA(cudaStreamSynchronize(s));
@@ -337,11 +344,11 @@ ProofSystem::~ProofSystem() {
 }
 
 void ProofSystem::stage_statement(cudaStream_t s) {
-  states_.upload(states_h_.data(), states_h_.size(), s);
-  msgs_.upload(msgs_h_.data(), msgs_h_.size(), s);
-  offsets_.upload(dev_->host->block_f_offset.data(), dev_->host->block_f_offset.size(), s);
-  if (!fin_h_.empty()) fin_.upload(fin_h_.data(), fin_h_.size(), s);  // empty message: no inputs
-  bit_c_.upload(bitc_h_.data(), bitc_h_.size(), s);
+  states_->upload(states_h_.data(), states_h_.size(), s);
+  msgs_->upload(msgs_h_.data(), msgs_h_.size(), s);
+  offsets_->upload(dev_->host->block_f_offset.data(), dev_->host->block_f_offset.size(), s);
+  if (!fin_h_.empty()) fin_->upload(fin_h_.data(), fin_h_.size(), s);  // empty message: no inputs
+  bit_c_->upload(bitc_h_.data(), bitc_h_.size(), s);
 }
 
 int ProofSystem::witness(cudaStream_t s) {
@@ -351,25 +358,25 @@ int ProofSystem::witness(cudaStream_t s) {
   size_t n_in = inputs_.size();
   size_t fwords = ((size_t)1 << S.committed_m) / 32;
   size_t hwords = ((size_t)1 << (S.claim_log_cols + 7)) / 32;
-  f_.resize(fwords);
-  h_.resize(hwords);
-  BZ_CUDA(cudaMemsetAsync(f_.get(), 0, fwords * 4, s));
-  BZ_CUDA(cudaMemsetAsync(h_.get(), 0, hwords * 4, s));
+  f_->resize(fwords);
+  h_->resize(hwords);
+  BZ_CUDA(cudaMemsetAsync(f_->get(), 0, fwords * 4, s));
+  BZ_CUDA(cudaMemsetAsync(h_->get(), 0, hwords * 4, s));
   if (n_in)
-    BZ_CUDA(cudaMemcpyAsync(f_.get(), fin_.get(), fin_h_.size() * 4, cudaMemcpyDeviceToDevice, s));
-  prod_.resize(3 * S.rows);
+    BZ_CUDA(cudaMemcpyAsync(f_->get(), fin_->get(), fin_h_.size() * 4, cudaMemcpyDeviceToDevice, s));
+  prod_->resize(3 * S.rows);
   W.flag.resize(1);
   BZ_CUDA(cudaMemsetAsync(W.flag.get(), 0, sizeof(int), s));
   WitnessArgs a;
-  a.states = states_.get();
-  a.msgs = msgs_.get();
-  a.offsets = offsets_.get();
+  a.states = states_->get();
+  a.msgs = msgs_->get();
+  a.offsets = offsets_->get();
   a.nblocks = (int)S.n_blocks;
-  a.f = f_.get();
+  a.f = f_->get();
   a.h_len = S.h_len;
   a.m_off = dev_->m_off.get();
   a.m_pos = dev_->m_pos.get();
-  a.h = h_.get();
+  a.h = h_->get();
   a.rows = S.rows;
   a.n_inputs = n_in;
   for (int k = 0; k < 3; k++) {
@@ -377,8 +384,8 @@ int ProofSystem::witness(cudaStream_t s) {
     a.abc_col[k] = dev_->abc_col[k].get();
     a.abc_coef[k] = dev_->abc_coef[k].get();
   }
-  a.bit_c = bit_c_.get();
-  a.prod = prod_.get();
+  a.bit_c = bit_c_->get();
+  a.prod = prod_->get();
   a.unsat = W.flag.get();
   witness_generate(a, s);
   int *unsat_h = reinterpret_cast<int *>(W.pin_small.get(kPinSmall) + kPinFlag);
@@ -448,13 +455,13 @@ int ProofSystem::commit(cudaStream_t s) {
   const PcsLevel &L0 = pcs_.levels[0];
   int log_n = pcs_.log_n;
   size_t rows = (size_t)1 << (log_n - L0.k + L0.log_inv_rate);
-  codeword0_.resize(rows << L0.k);
-  nodes0_.resize(16 * rows);
-  const f128 *fpk = reinterpret_cast<const f128 *>(f_.get());
-  rs_encode(fpk, log_n, L0.k, L0.log_inv_rate, T.wh.get(), codeword0_.get(), s);
-  merkle_build(codeword0_.get(), rows, L0.k, nodes0_.get(), s);
+  codeword0_->resize(rows << L0.k);
+  nodes0_->resize(16 * rows);
+  const f128 *fpk = reinterpret_cast<const f128 *>(f_->get());
+  rs_encode(fpk, log_n, L0.k, L0.log_inv_rate, T.wh.get(), codeword0_->get(), s);
+  merkle_build(codeword0_->get(), rows, L0.k, nodes0_->get(), s);
   f128 *root_h = W.pin_small.get(kPinSmall) + kPinRoot;
-  BZ_CUDA(cudaMemcpyAsync(root_h, nodes0_.get() + 8, 32, cudaMemcpyDeviceToHost, s));
+  BZ_CUDA(cudaMemcpyAsync(root_h, nodes0_->get() + 8, 32, cudaMemcpyDeviceToHost, s));
   BZ_CUDA(cudaStreamSynchronize(s));
   memcpy(root_, root_h, 32);
   const char *dom = circuit_name(kind_);
@@ -528,8 +535,8 @@ std::vector<uint8_t> ProofSystem::ligerito(cudaStream_t s, f128 target) {
   size_t n = (size_t)1 << cfg.log_n;
   f128 *f = W.lf.get(), *b = W.lb.get(), *f2 = W.lf2.get(), *b2 = W.lb2.get();
   // the current level's codeword and tree
-  const f128 *cw = codeword0_.get();
-  const uint32_t *nodes = nodes0_.get();
+  const f128 *cw = codeword0_->get();
+  const uint32_t *nodes = nodes0_->get();
   int cur_k = cfg.levels[0].k;
   size_t cur_rows = (size_t)1 << (cfg.log_n - cur_k + cfg.levels[0].log_inv_rate);
   DeviceBuffer<f128> *next_cw = W.lig_cw;
@@ -712,9 +719,9 @@ int ProofSystem::prove_after_commit(cudaStream_t s, std::vector<uint8_t> &proof)
   W.sp_sums.resize(4);
   W.sp_tab.resize(dev_->ntab + 1);
   if (bit_rows_.empty())
-    d_bit_rows_.resize(1);
+    d_bit_rows_->resize(1);
   else
-    d_bit_rows_.upload(bit_rows_.data(), bit_rows_.size(), s);
+    d_bit_rows_->upload(bit_rows_.data(), bit_rows_.size(), s);
   SpartanScratch sc;
   for (int i = 0; i < 8; i++) sc.t[i] = W.sp_t.get() + i * R;
   for (int i = 0; i < 4; i++) sc.d[i] = W.sp_d.get() + i * Cn;
@@ -731,8 +738,8 @@ int ProofSystem::prove_after_commit(cudaStream_t s, std::vector<uint8_t> &proof)
   sa.num_col_vars = nc;
   sa.rows = S.rows;
   sa.cols = S.h_len;
-  sa.prod = prod_.get();
-  sa.hbits = h_.get();
+  sa.prod = prod_->get();
+  sa.hbits = h_->get();
   sa.digest = matrix_digest_;
   sa.csc_off = dev_->sp_off.get();
   sa.csc_row = dev_->sp_row.get();
@@ -741,7 +748,7 @@ int ProofSystem::prove_after_commit(cudaStream_t s, std::vector<uint8_t> &proof)
   sa.tab_vals = dev_->tab_vals.get();
   sa.tab_which = dev_->tab_which.get();
   sa.ntab = dev_->ntab;
-  sa.bit_rows = d_bit_rows_.get();
+  sa.bit_rows = d_bit_rows_->get();
   sa.n_bit_rows = (int)bit_rows_.size();
   SpartanOut so;
   spartan_prove(sa, t, sc, s, so);
@@ -783,7 +790,7 @@ int ProofSystem::prove_after_commit(cudaStream_t s, std::vector<uint8_t> &proof)
   // send_fold (crates/prover/src/fold.rs:38-75) and the GKR build
   W.exps.upload(rows_w.data(), 128, s);
   W.folds.resize(ncol);
-  const f128 *hpk = reinterpret_cast<const f128 *>(h_.get());
+  const f128 *hpk = reinterpret_cast<const f128 *>(h_->get());
   fold_columns(hpk, ncol, W.exps.get(), W.folds.get(), s);
   u128 *folds_h = W.host_folds.get(ncol + 128);  // the folds, then the 128 row images
   BZ_CUDA(cudaMemcpyAsync(folds_h, W.folds.get(), ncol * 16, cudaMemcpyDeviceToHost, s));
@@ -892,7 +899,7 @@ int ProofSystem::prove_after_commit(cudaStream_t s, std::vector<uint8_t> &proof)
   pa.log_rows = S.committed_m;
   pa.cols = W.ones.get();
   pa.log_cols = 0;
-  pa.packed = reinterpret_cast<const f128 *>(f_.get());
+  pa.packed = reinterpret_cast<const f128 *>(f_->get());
   pa.target = target2;
   pa.grind_bits = grinding_bits((uint32_t)security_, 2);
   PostGkrScratch &ps = ctx.post_gkr_scratch(nbits / 2);
@@ -967,7 +974,7 @@ int ProofSystem::prove_after_commit(cudaStream_t s, std::vector<uint8_t> &proof)
   }
   packed_basis(W.suffix.get(), np, W.bw.get(), security_ == 100 ? W.eq_ood.get() : nullptr, coef,
                W.lb.get(), s);
-  BZ_CUDA(cudaMemcpyAsync(W.lf.get(), f_.get(), np * 16, cudaMemcpyDeviceToDevice, s));
+  BZ_CUDA(cudaMemcpyAsync(W.lf.get(), f_->get(), np * 16, cudaMemcpyDeviceToDevice, s));
   ph.mark("ring_switch");
   std::vector<uint8_t> lproof = ligerito(s, ptarget);
   ph.mark("ligerito");
@@ -1003,8 +1010,15 @@ int ProofSystem::prove(std::vector<uint8_t> &proof, StageTimes *times, bool rest
   lane_ = lane ? lane : &Context::get();
   cudaStream_t s = lane_->stream();
   auto t0 = std::chrono::steady_clock::now();
+  Workspace &W = workspace(*lane_);
+  states_ = &W.states, msgs_ = &W.msgs, fin_ = &W.fin, offsets_ = &W.offsets;
+  f_ = &W.f, h_ = &W.h, prod_ = &W.prod, bit_c_ = &W.bit_c, d_bit_rows_ = &W.bit_rows;
+  codeword0_ = &W.codeword0, nodes0_ = &W.nodes0;
   BZ_CUDA(cudaEventRecord(ev_start_, s));
-  if (restage) stage_statement(s);
+  if (restage || W.staged_serial != serial_) {
+    stage_statement(s);
+    W.staged_serial = serial_;
+  }
   int rc = witness(s);
   if (rc) return rc;
   double tw = ms_since(t0);
@@ -1030,13 +1044,16 @@ int ProofSystem::prove(std::vector<uint8_t> &proof, StageTimes *times, bool rest
 
 void ProofSystem::download_witness(std::vector<uint32_t> &f, std::vector<uint32_t> &h,
                                    std::vector<int64_t> &prod) {
-  cudaStream_t s = (lane_ ? lane_ : &Context::get())->stream();
-  f.resize(f_.size());
-  h.resize(h_.size());
-  prod.resize(prod_.size());
-  f_.download(f.data(), f.size(), s);
-  h_.download(h.data(), h.size(), s);
-  prod_.download(prod.data(), prod.size(), s);
+  if (!lane_ || !f_) throw std::runtime_error("no proof has run on this system");
+  cudaStream_t s = lane_->stream();
+  // this statement's sizes (the lane's buffers may be larger)
+  const CircuitSetup &S = *dev_->host;
+  f.resize(((size_t)1 << S.committed_m) / 32);
+  h.resize(((size_t)1 << (S.claim_log_cols + 7)) / 32);
+  prod.resize(3 * S.rows);
+  f_->download(f.data(), f.size(), s);
+  h_->download(h.data(), h.size(), s);
+  prod_->download(prod.data(), prod.size(), s);
   BZ_CUDA(cudaStreamSynchronize(s));
 }
 

@@ -96,21 +96,23 @@ class ProofSystem {
   std::vector<uint32_t> bit_rows_;  // bit constraints whose expected value is one
   f128 generator_;
 
-  // the statement on the device: chaining values, message words, hint
+  // the statement in host memory: chaining values, message words, hint
   // offsets, the packed input bits and every bit constraint's expected value
   std::vector<uint32_t> states_h_, msgs_h_, fin_h_;
   std::vector<uint8_t> bitc_h_;
-  DeviceBuffer<uint32_t> states_, msgs_, fin_;
-  DeviceBuffer<uint64_t> offsets_;
+  uint64_t serial_;  // identifies the statement staged in a lane's buffers
   cudaEvent_t ev_start_ = nullptr, ev_stop_ = nullptr;
 
-  // per-proof device state
-  DeviceBuffer<uint32_t> f_, h_;
-  DeviceBuffer<int64_t> prod_;
-  DeviceBuffer<uint8_t> bit_c_;
-  DeviceBuffer<uint32_t> d_bit_rows_;
-  DeviceBuffer<f128> codeword0_;
-  DeviceBuffer<uint32_t> nodes0_;
+  // the proof's device state, in the buffers of the lane running it (bound
+  // at the start of prove())
+  DeviceBuffer<uint32_t> *states_ = nullptr, *msgs_ = nullptr, *fin_ = nullptr;
+  DeviceBuffer<uint64_t> *offsets_ = nullptr;
+  DeviceBuffer<uint32_t> *f_ = nullptr, *h_ = nullptr;
+  DeviceBuffer<int64_t> *prod_ = nullptr;
+  DeviceBuffer<uint8_t> *bit_c_ = nullptr;
+  DeviceBuffer<uint32_t> *d_bit_rows_ = nullptr;
+  DeviceBuffer<f128> *codeword0_ = nullptr;
+  DeviceBuffer<uint32_t> *nodes0_ = nullptr;
   std::unique_ptr<Transcript> ts_;
   uint8_t root_[32];
   std::vector<f128> ood_point_;

@@ -178,8 +178,10 @@ int bitz_batch_prove(bitz_system *const *systems, size_t n, int lanes, uint8_t *
  * free up (continuous batching). A request is admitted when a lane is free
  * and its padded-witness device footprint fits in hbm_budget_bytes beside
  * the requests in flight (one request is always admitted when none is in
- * flight). Each request builds its statement (CircuitProofSystem::new) and
- * proves it on the lane. */
+ * flight). Host threads beside the lanes (half the host's hardware threads,
+ * at least two) prepare each request's statement (CircuitProofSystem::new:
+ * the cached circuit shape and the statement's matrix digest) in submission
+ * order; the lanes prove prepared requests, oldest first. */
 typedef struct bitz_server bitz_server;
 int bitz_server_start(int lanes, uint64_t hbm_budget_bytes, uint32_t security_bits,
                       bitz_server **out);
