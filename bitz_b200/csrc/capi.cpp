@@ -237,6 +237,7 @@ static int gkr_common(const f128 *images, const f128 *columns, int log_cols, con
                       uint64_t claim_out[2]) {
   Context &ctx = Context::get();
   GkrScratch &sc = ctx.gkr_scratch(log_cols);
+  sc.live_cols = 0;  // arbitrary columns: all live
   gkr_build(columns, log_cols, images, sc, ctx.stream());
   f128 z[kMaxPointGkr], pt[kMaxPointGkr];
   for (int i = 0; i < log_cols; i++) z[i] = mk(zeta[2 * i], zeta[2 * i + 1]);
@@ -297,6 +298,7 @@ int bitz_gkr_outputs(const uint64_t *row_images, const uint64_t *columns, int lo
     d_img.upload((const f128 *)row_images, 128, ctx.stream());
     d_cols.upload((const f128 *)columns, nc, ctx.stream());
     GkrScratch &sc = ctx.gkr_scratch(log_cols);
+    sc.live_cols = 0;
     gkr_build(d_cols.get(), log_cols, d_img.get(), sc, ctx.stream());
     BZ_CUDA(cudaMemcpyAsync(out, sc.layer[7], nc * 16, cudaMemcpyDeviceToHost, ctx.stream()));
     BZ_CUDA(cudaStreamSynchronize(ctx.stream()));

@@ -33,20 +33,36 @@ __global__ void gkr_leaves(const f128 *__restrict__ cols, int s, const f128 *__r
   }
 }
 
-__global__ void gkr_parent(const f128 *__restrict__ child, size_t half, f128 *__restrict__ out) {
+// Padding: the low s bits of every layer index are the column, and a column at
+// or beyond `live` has only one-valued nodes. Whenever entry x of a half is
+// such a column, so are x + h and x + 2h (same column, or a higher one below
+// 2^s), so a thread whose x is padded binds nothing (1 + r (1 + 1) = 1) and
+// adds e * 1 * 1 = e to the first sum and e * 0 * 0 = 0 to the second.
+__device__ __forceinline__ bool padded(size_t x, size_t colmask, size_t live) {
+  return (x & colmask) >= live;
+}
+
+__global__ void gkr_parent(const f128 *__restrict__ child, size_t half, f128 *__restrict__ out,
+                           size_t colmask, size_t live) {
   for (size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x; k < half;
        k += (size_t)gridDim.x * blockDim.x)
-    st(out + k, gmul(ld(child + k), ld(child + half + k)));
+    st(out + k, padded(k, colmask, live) ? mk(1, 0) : gmul(ld(child + k), ld(child + half + k)));
 }
 
 // Round i's sums (round_sums, lib.rs:164-216) before any bind: the top round.
 __global__ void gkr_top_sums(const f128 *__restrict__ c, size_t n_half, size_t h,
                              const f128 *__restrict__ eq, int at_one, unsigned long long *acc,
-                             Publish pub) {
+                             Publish pub, size_t colmask, size_t live) {
   const f128 *L = c, *R = c + n_half;
   wide sb = wzero(), si = wzero();
   for (size_t x = blockIdx.x * (size_t)blockDim.x + threadIdx.x; x < h;
        x += (size_t)gridDim.x * blockDim.x) {
+    if (padded(x, colmask, live)) {
+      f128 e = ld(eq + x);
+      sb.w0 ^= e.lo;
+      sb.w1 ^= e.hi;
+      continue;
+    }
     f128 l0 = ld(L + x), l1 = ld(L + h + x), r0 = ld(R + x), r1 = ld(R + h + x);
     f128 e = ld(eq + x);
     f128 lb = at_one ? l1 : l0, rb = at_one ? r1 : r0;
@@ -62,12 +78,19 @@ __global__ void gkr_top_sums(const f128 *__restrict__ c, size_t n_half, size_t h
 // round i (halves of 2^i). Thread x < 2^i owns entries x and x + 2^i.
 __global__ void gkr_bind_sums(f128 *__restrict__ c, size_t n_half, size_t h, f128 r,
                               f128 *__restrict__ eq, int at_one, unsigned long long *acc,
-                              Publish pub) {
+                              Publish pub, size_t colmask, size_t live) {
   f128 *L = c, *R = c + n_half;
   const size_t h2 = 2 * h;
   wide sb = wzero(), si = wzero();
   for (size_t x = blockIdx.x * (size_t)blockDim.x + threadIdx.x; x < h;
        x += (size_t)gridDim.x * blockDim.x) {
+    if (padded(x, colmask, live)) {
+      f128 e = gadd(ld(eq + x), ld(eq + x + h));
+      st(eq + x, e);
+      sb.w0 ^= e.lo;
+      sb.w1 ^= e.hi;
+      continue;
+    }
     f128 a0 = ld(L + x), a1 = ld(L + x + h2), b0 = ld(L + x + h), b1 = ld(L + x + h + h2);
     f128 l0 = gadd(a0, gmul(r, gadd(a1, a0)));
     f128 l1 = gadd(b0, gmul(r, gadd(b1, b0)));
@@ -123,7 +146,8 @@ __global__ void __launch_bounds__(kThreads) gkr_tail(const f128 *__restrict__ c,
                                                      int i0, const f128 *__restrict__ eq,
                                                      uint32_t at_one_mask, Mailbox *mb,
                                                      unsigned long long seq0, const Mailbox *down,
-                                                     unsigned long long dseq0) {
+                                                     unsigned long long dseq0, size_t colmask,
+                                                     size_t live_cols) {
   __shared__ f128 L[4 * kTailH], R[4 * kTailH], E[2 * kTailH];
   __shared__ unsigned long long chal[2];
   __shared__ int ok;
@@ -155,6 +179,13 @@ __global__ void __launch_bounds__(kThreads) gkr_tail(const f128 *__restrict__ c,
     const int at_one = (at_one_mask >> (i - 1)) & 1;
     wide sb = wzero(), si = wzero();
     for (int x = threadIdx.x; x < h; x += blockDim.x) {
+      if (padded((size_t)x, colmask, live_cols)) {
+        f128 e = gadd(E[x], E[x + h]);
+        E[x] = e;
+        sb.w0 ^= e.lo;
+        sb.w1 ^= e.hi;
+        continue;
+      }
       f128 l0 = gadd(L[x], gmul(r, gadd(L[x + h2], L[x])));
       f128 l1 = gadd(L[x + h], gmul(r, gadd(L[x + h + h2], L[x + h])));
       f128 r0 = gadd(R[x], gmul(r, gadd(R[x + h2], R[x])));
@@ -197,8 +228,11 @@ void gkr_build(const f128 *cols, int s, const f128 *images, GkrScratch &sc, cuda
   gkr_leaves<<<grid_for(total), kThreads, 0, st_>>>(cols, s, images, sc.layer[0]);
   BZ_LAUNCH_CHECK();
   size_t len = total;
+  const size_t colmask = ((size_t)1 << s) - 1;
+  const size_t live = sc.live_cols ? sc.live_cols : colmask + 1;
   for (int j = 0; j < 7; j++) {
-    gkr_parent<<<grid_for(len / 2), kThreads, 0, st_>>>(sc.layer[j], len / 2, sc.layer[j + 1]);
+    gkr_parent<<<grid_for(len / 2), kThreads, 0, st_>>>(sc.layer[j], len / 2, sc.layer[j + 1],
+                                                         colmask, live);
     BZ_LAUNCH_CHECK();
     len /= 2;
   }
@@ -211,6 +245,8 @@ f128 gkr_prove(int s, const f128 *zeta, uint32_t grind_bits, Transcript &ts, Gkr
   f128 point[kMaxPoint], next[kMaxPoint];
   for (int i = 0; i < s; i++) point[i] = zeta[i];
   int n = s;
+  const size_t colmask = ((size_t)1 << s) - 1;
+  const size_t live = sc.live_cols ? sc.live_cols : colmask + 1;
   f128 claim = mk(0, 0);
   KernelProbe &probe = KernelProbe::get();
   RoundChannel *ch = sc.channel;
@@ -232,7 +268,8 @@ f128 gkr_prove(int s, const f128 *zeta, uint32_t grind_bits, Transcript &ts, Gkr
     eq_table_device(point, n - 1, sc.eq, sc.eq_scratch, st_);
     size_t h = n_half / 2;
     gkr_top_sums<<<grid_for(h), kThreads, 0, st_>>>(c, n_half, h, sc.eq,
-                                                    gis_zero(point[n - 1]), sc.acc, arm(sc));
+                                                    gis_zero(point[n - 1]), sc.acc, arm(sc),
+                                                    colmask, live);
     BZ_LAUNCH_CHECK();
     f128 eq_bound = mk(1, 0);
     for (int i = n - 1; i >= 0; i--) {
@@ -250,7 +287,7 @@ f128 gkr_prove(int s, const f128 *zeta, uint32_t grind_bits, Transcript &ts, Gkr
         uint32_t mask = 0;
         for (int k = 1; k <= i; k++) mask |= (uint32_t)gis_zero(point[k - 1]) << (k - 1);
         gkr_tail<<<1, kThreads, 0, st_>>>(c, n_half, i, sc.eq, mask, ch->dev, ch->next + 1,
-                                          ch->down_dev, ch->down_next + 1);
+                                          ch->down_dev, ch->down_next + 1, colmask, live);
         BZ_LAUNCH_CHECK();
         tail = true;
       }
@@ -262,10 +299,16 @@ f128 gkr_prove(int s, const f128 *zeta, uint32_t grind_bits, Transcript &ts, Gkr
         const bool probed = probe.on("gkr_bind_sums");
         if (probed) probe.before(st_);
         gkr_bind_sums<<<grid_for(hh), kThreads, 0, st_>>>(c, n_half, hh, r, sc.eq,
-                                                          gis_zero(point[i - 1]), acc + 4, arm(sc));
+                                                          gis_zero(point[i - 1]), acc + 4, arm(sc),
+                                                          colmask, live);
         BZ_LAUNCH_CHECK();
         // reads 8 child and 2 eq entries per thread, writes 4 and 1
-        if (probed) probe.after(st_, 240.0 * (double)hh);
+        if (probed) {
+          // live threads move 15 entries, padded ones the eq table's 3
+          double nl = hh > colmask ? (double)(hh / (colmask + 1)) * (double)live
+                                   : (double)std::min(hh, live);
+          probe.after(st_, 240.0 * nl + 48.0 * ((double)hh - nl));
+        }
       } else {
         gkr_final_bind<<<1, 32, 0, st_>>>(c, n_half, r, sc.pair, arm(sc));
         BZ_LAUNCH_CHECK();

@@ -17,6 +17,10 @@ struct GkrScratch {
   unsigned long long *acc = nullptr;  // 4 words per round
   uint64_t *host = nullptr;           // pinned, 4 words
   RoundChannel *channel = nullptr;    // mailbox for round results; null: copy + sync
+  // Columns at or beyond live_cols hold no set bit (the padding of h), so
+  // every node of theirs is one in every layer; the kernels skip their
+  // products and add their known contribution. 0: every column is live.
+  size_t live_cols = 0;
 };
 
 // Builds every layer from the packed columns (2^s F128, bit b of column c is

@@ -800,6 +800,7 @@ int ProofSystem::prove_after_commit(cudaStream_t s, std::vector<uint8_t> &proof)
   BZ_CUDA(cudaMemcpyAsync(row_images_h, W.images.get(), 128 * 16, cudaMemcpyDeviceToHost, s));
   BZ_CUDA(cudaEventRecord(W.ev_folds, s));
   GkrScratch &gs = ctx.gkr_scratch(sc_cols);
+  gs.live_cols = (S.h_len + 127) / 128;  // packed columns past h's last bit are all zero
   gkr_build(hpk, sc_cols, W.images.get(), gs, s);
   u128 target_p = fp_canonical(so.final_claim, fc);
   // prove_virtual (crates/prover/src/prove.rs:96-152)
