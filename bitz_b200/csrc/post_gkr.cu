@@ -177,6 +177,71 @@ static f128 advance(f128 claim, f128 a0, f128 a2, f128 r) {
 
 // A round's result words: through the mailbox when the scratch has a
 // channel, else by a copy and a stream sync.
+// The last rounds in one resident block, fed through the lane's downbox like
+// the GKR tail: the tables (at most 2 * kPgTailN entries each) sit in shared
+// memory; each round waits (bounded) for the host's challenge, folds both
+// tables at it and posts the next round's (a0, a2), or, after the last fold,
+// the closing pair (w, v). A missing challenge ends the kernel without a post.
+constexpr int kPgTailN = 512;  // entries after the first fold
+constexpr unsigned long long kPgWaitNs = 2000000000ull;
+
+__global__ void __launch_bounds__(kThreads) pg_tail(const f128 *__restrict__ w_in,
+                                                    const f128 *__restrict__ v_in, int len0,
+                                                    Mailbox *mb, unsigned long long seq0,
+                                                    const Mailbox *down, unsigned long long dseq0) {
+  __shared__ f128 W[2 * kPgTailN], V[2 * kPgTailN];
+  __shared__ unsigned long long chal[2];
+  __shared__ int ok;
+  for (int k = threadIdx.x; k < len0; k += blockDim.x) {
+    W[k] = ld(w_in + k);
+    V[k] = ld(v_in + k);
+  }
+  int len = len0;
+  for (int round = 0; len > 1; round++) {
+    if (threadIdx.x == 0) ok = mailbox_wait_device(down, dseq0 + round, 2, chal, kPgWaitNs);
+    __syncthreads();
+    if (!ok) return;
+    const f128 r = mk(chal[0], chal[1]);
+    const unsigned long long seq = seq0 + round;
+    const int nout = len / 2;
+    // fold: read every pair first, then write (the halves overlap in place)
+    f128 fw[2], fv[2];
+    int cnt = 0;
+    for (int o = threadIdx.x; o < nout; o += blockDim.x, cnt++) {
+      fw[cnt] = gadd(W[2 * o], gmul(r, gadd(W[2 * o], W[2 * o + 1])));
+      fv[cnt] = gadd(V[2 * o], gmul(r, gadd(V[2 * o], V[2 * o + 1])));
+    }
+    __syncthreads();
+    cnt = 0;
+    for (int o = threadIdx.x; o < nout; o += blockDim.x, cnt++) {
+      W[o] = fw[cnt];
+      V[o] = fv[cnt];
+    }
+    __syncthreads();
+    len = nout;
+    if (len == 1) {
+      if (threadIdx.x == 0) {
+        mailbox_post(mb, seq, 0, W[0].lo);
+        mailbox_post(mb, seq, 1, W[0].hi);
+        mailbox_post(mb, seq, 2, V[0].lo);
+        mailbox_post(mb, seq, 3, V[0].hi);
+      }
+      return;
+    }
+    wide a0 = wzero(), a2 = wzero();
+    for (int j = threadIdx.x; j < len / 2; j += blockDim.x) {
+      f128 w0 = W[2 * j], w1 = W[2 * j + 1], v0 = V[2 * j], v1 = V[2 * j + 1];
+      wacc(a0, gmul_wide(w0, v0));
+      wacc(a2, gmul_wide(gadd(w0, w1), gadd(v0, v1)));
+    }
+    f128 s0 = greduce(a0), s2 = greduce(a2);
+    uint64_t vv[4] = {s0.lo, s0.hi, s2.lo, s2.hi};
+    block_xor_reduce<4>(vv);
+    if (threadIdx.x == 0)
+      for (int k = 0; k < 4; k++) mailbox_post(mb, seq, k, vv[k]);
+  }
+}
+
 static Publish arm(PostGkrScratch &sc) {
   return sc.channel ? sc.channel->arm() : Publish{nullptr, nullptr, 0};
 }
@@ -232,6 +297,13 @@ int post_gkr_prove(const PostGkrArgs &a, Transcript &ts, PostGkrScratch &sc, cud
     }
   }
   size_t len = n1;
+  RoundChannel *ch = sc.channel;
+  bool tail = false;  // pg_tail is resident and runs the remaining rounds
+  static const bool resident = [] {
+    const char *e = getenv("BITZ_RESIDENT_ROUNDS");
+    return !(e && e[0] == '0');
+  }();
+  try {
   for (int k = 0; k < rounds; k++) {
     unsigned long long *ak = acc + 8 * (k + 1);
     round_read(sc, ak, 4, s);
@@ -242,6 +314,19 @@ int post_gkr_prove(const PostGkrArgs &a, Transcript &ts, PostGkrScratch &sc, cud
     f128 rr = ts.challenge_f128();
     claim = advance(claim, m0, m2, rr);
     point_out[1 + k] = rr;
+    if (!tail && ch && resident && len <= (size_t)2 * kPgTailN) {
+      pg_tail<<<1, kThreads, 0, s>>>(w, v, (int)len, ch->dev, ch->next + 1, ch->down_dev,
+                                     ch->down_next + 1);
+      BZ_LAUNCH_CHECK();
+      tail = true;
+    }
+    if (tail) {
+      const uint64_t rw[2] = {rr.lo, rr.hi};
+      ch->send(rw, 2);
+      ch->arm();
+      len /= 2;
+      continue;
+    }
     size_t nout = len / 2;
     int emit = nout >= 2;
     pg_round<<<grid_for((nout + 1) / 2), kThreads, 0, s>>>(w, v, rr, w2, v2, nout, emit,
@@ -256,10 +341,25 @@ int post_gkr_prove(const PostGkrArgs &a, Transcript &ts, PostGkrScratch &sc, cud
     v2 = t;
     len = nout;
   }
+  } catch (...) {
+    if (tail) {  // release the waiting kernel before the lane is reused
+      ch->abort();
+      cudaStreamSynchronize(s);
+      ch->clear_down();
+    }
+    throw;
+  }
   f128 fin[2];
-  BZ_CUDA(cudaMemcpyAsync(fin, w, 16, cudaMemcpyDeviceToHost, s));
-  BZ_CUDA(cudaMemcpyAsync(fin + 1, v, 16, cudaMemcpyDeviceToHost, s));
-  BZ_CUDA(cudaStreamSynchronize(s));
+  if (tail) {
+    // the tail's last publication is the closing pair
+    ch->wait(s, sc.host, 4);
+    fin[0] = mk(sc.host[0], sc.host[1]);
+    fin[1] = mk(sc.host[2], sc.host[3]);
+  } else {
+    BZ_CUDA(cudaMemcpyAsync(fin, w, 16, cudaMemcpyDeviceToHost, s));
+    BZ_CUDA(cudaMemcpyAsync(fin + 1, v, 16, cudaMemcpyDeviceToHost, s));
+    BZ_CUDA(cudaStreamSynchronize(s));
+  }
   *value_out = fin[1];
   ts.prover_f128(fin[1]);
   return geq(gmul(fin[0], fin[1]), claim) ? BZ_OK : BZ_ERR_INTERNAL;

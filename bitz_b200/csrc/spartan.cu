@@ -253,6 +253,134 @@ __global__ void k_bind_bits(const uint32_t *__restrict__ rows, int n, const fp *
   if (threadIdx.x == 0) D[0] = fp_add(D[0], fp_mul(out[0], rho2, c), c);
 }
 
+// The last rounds of each sumcheck in one resident block, fed through the
+// lane's downbox (bounded waits; a missing challenge ends the kernel without
+// a post). The tables (at most kSpTailN entries each) sit in shared memory.
+// Each round folds at the previous round's challenge (when `fold`), sums the
+// round's coefficients and posts them; after the last round the final fold's
+// single entries are posted.
+constexpr int kSpTailN = 512;
+constexpr unsigned long long kSpWaitNs = 2000000000ull;
+
+// Folds T tables of len entries in place at r (all reads, then all writes).
+template <int T>
+__device__ __forceinline__ int sp_fold(fp (*tab)[kSpTailN], int len, fp r, const FpCtx &c) {
+  const int nout = len / 2;
+  fp f[T][2];
+  int cnt = 0;
+  for (int o = threadIdx.x; o < nout; o += blockDim.x, cnt++)
+    for (int t = 0; t < T; t++) f[t][cnt] = interp(tab[t][2 * o], tab[t][2 * o + 1], r, c);
+  __syncthreads();
+  cnt = 0;
+  for (int o = threadIdx.x; o < nout; o += blockDim.x, cnt++)
+    for (int t = 0; t < T; t++) tab[t][o] = f[t][cnt];
+  __syncthreads();
+  return nout;
+}
+
+__device__ __forceinline__ bool sp_challenge(const Mailbox *down, unsigned long long dseq,
+                                             const FpCtx &c, fp &r) {
+  __shared__ unsigned long long chal[2];
+  __shared__ int ok;
+  if (threadIdx.x == 0) ok = mailbox_wait_device(down, dseq, 2, chal, kSpWaitNs);
+  __syncthreads();
+  r = fp{chal[0], chal[1]};
+  bool good = ok;
+  __syncthreads();
+  return good;
+}
+
+template <int N>
+__device__ __forceinline__ void sp_post(fp (&acc)[N], const FpCtx &c, Mailbox *mb,
+                                        unsigned long long seq) {
+  __shared__ fp red[N];
+  block_fp_sum<N>(acc, c, red);
+  if (threadIdx.x == 0)
+    for (int k = 0; k < N; k++) {
+      mailbox_post(mb, seq, 2 * k, red[k].lo);
+      mailbox_post(mb, seq, 2 * k + 1, red[k].hi);
+    }
+  __syncthreads();
+}
+
+// Outer rounds round0 .. rounds-1 over E, A, B, C (len0 entries each).
+__global__ void __launch_bounds__(kThreads) sp_outer_tail(const fp *E, const fp *A, const fp *B,
+                                                          const fp *C, int len0, int fold0,
+                                                          int nrounds, FpCtx c, Mailbox *mb,
+                                                          unsigned long long seq0,
+                                                          const Mailbox *down,
+                                                          unsigned long long dseq0) {
+  __shared__ fp tab[4][kSpTailN];
+  for (int k = threadIdx.x; k < len0; k += blockDim.x) {
+    tab[0][k] = E[k];
+    tab[1][k] = A[k];
+    tab[2][k] = B[k];
+    tab[3][k] = C[k];
+  }
+  __syncthreads();
+  int len = len0, nd = 0, np = 0;
+  for (int round = 0; round < nrounds; round++) {
+    if (round > 0 || fold0) {
+      fp r;
+      if (!sp_challenge(down, dseq0 + nd++, c, r)) return;
+      len = sp_fold<4>(tab, len, r, c);
+    }
+    fp acc[3] = {fp_zero(), fp_zero(), fp_zero()};
+    for (int j = threadIdx.x; j < len / 2; j += blockDim.x)
+      cubic(tab[0][2 * j], tab[0][2 * j + 1], tab[1][2 * j], tab[1][2 * j + 1], tab[2][2 * j],
+            tab[2][2 * j + 1], tab[3][2 * j], tab[3][2 * j + 1], c, acc);
+    sp_post<3>(acc, c, mb, seq0 + np++);
+  }
+  fp r;
+  if (!sp_challenge(down, dseq0 + nd, c, r)) return;
+  sp_fold<4>(tab, len, r, c);
+  if (threadIdx.x == 0)
+    for (int k = 0; k < 3; k++) {
+      mailbox_post(mb, seq0 + np, 2 * k, tab[k + 1][0].lo);
+      mailbox_post(mb, seq0 + np, 2 * k + 1, tab[k + 1][0].hi);
+    }
+}
+
+// Inner rounds over D and W (W from the packed h bits when w_bits).
+__global__ void __launch_bounds__(kThreads) sp_inner_tail(const fp *D, const fp *W,
+                                                          const uint32_t *hbits, int w_bits,
+                                                          int len0, int fold0, int nrounds,
+                                                          FpCtx c, Mailbox *mb,
+                                                          unsigned long long seq0,
+                                                          const Mailbox *down,
+                                                          unsigned long long dseq0) {
+  __shared__ fp tab[2][kSpTailN];
+  for (int k = threadIdx.x; k < len0; k += blockDim.x) {
+    tab[0][k] = D[k];
+    tab[1][k] = w_bits ? (((hbits[k >> 5] >> (k & 31)) & 1) ? c.one : fp_zero()) : W[k];
+  }
+  __syncthreads();
+  int len = len0, nd = 0, np = 0;
+  for (int round = 0; round < nrounds; round++) {
+    if (round > 0 || fold0) {
+      fp r;
+      if (!sp_challenge(down, dseq0 + nd++, c, r)) return;
+      len = sp_fold<2>(tab, len, r, c);
+    }
+    fp acc[2] = {fp_zero(), fp_zero()};
+    for (int j = threadIdx.x; j < len / 2; j += blockDim.x) {
+      fp d0 = tab[0][2 * j], d1 = tab[0][2 * j + 1], w0 = tab[1][2 * j], w1 = tab[1][2 * j + 1];
+      acc[0] = fp_add(acc[0], fp_mul(d0, w0, c), c);
+      acc[1] = fp_add(acc[1], fp_mul(fp_sub(d1, d0, c), fp_sub(w1, w0, c), c), c);
+    }
+    sp_post<2>(acc, c, mb, seq0 + np++);
+  }
+  fp r;
+  if (!sp_challenge(down, dseq0 + nd, c, r)) return;
+  sp_fold<2>(tab, len, r, c);
+  if (threadIdx.x == 0) {
+    mailbox_post(mb, seq0 + np, 0, tab[0][0].lo);
+    mailbox_post(mb, seq0 + np, 1, tab[0][0].hi);
+    mailbox_post(mb, seq0 + np, 2, tab[1][0].lo);
+    mailbox_post(mb, seq0 + np, 3, tab[1][0].hi);
+  }
+}
+
 // ------------------------------------------------------------------- host
 
 static fp host_partial_sum(const fp *d_partial, int nblocks, int N, fp *d_out, fp *h_out,
@@ -321,33 +449,76 @@ void spartan_prove(const SpartanArgs &a, Transcript &ts, SpartanScratch &sc, cud
   out.rx.resize(nr);
   size_t len = R;
   fp r = fp_zero();
+  RoundChannel *ch = sc.channel;
+  static const bool resident = [] {
+    const char *e = getenv("BITZ_RESIDENT_ROUNDS");
+    return !(e && e[0] == '0');
+  }();
+  bool tail = false;  // a resident tail kernel runs the remaining rounds
+  auto send_r = [&](fp x) {
+    const uint64_t w[2] = {x.lo, x.hi};
+    ch->send(w, 2);
+  };
+  fp fin[3];
+  try {
   for (int round = 0; round < nr; round++) {
     int fold = round > 0;
-    size_t npairs = fold ? (len / 2 + 1) / 2 : len / 2;
-    int g = grid_for(npairs);
-    k_outer_round<<<g, kThreads, 0, s>>>(E, A, B, C, E2, A2, B2, C2, len, fold, 1, r, c, sc.partial);
-    BZ_LAUNCH_CHECK();
-    host_partial_sum(sc.partial, g, 3, sc.sums, sc.host, c, s, sc.channel);
-    if (fold) {
-      std::swap(E, E2);
-      std::swap(A, A2);
-      std::swap(B, B2);
-      std::swap(C, C2);
-      len /= 2;
+    if (!tail && ch && resident && len <= (size_t)kSpTailN) {
+      sp_outer_tail<<<1, kThreads, 0, s>>>(E, A, B, C, (int)len, fold, nr - round, c, ch->dev,
+                                           ch->next + 1, ch->down_dev, ch->down_next + 1);
+      BZ_LAUNCH_CHECK();
+      tail = true;
+    }
+    if (tail) {
+      if (fold) {
+        send_r(r);
+        len /= 2;
+      }
+      ch->arm();
+      ch->wait(s, reinterpret_cast<uint64_t *>(sc.host), 6);
+    } else {
+      size_t npairs = fold ? (len / 2 + 1) / 2 : len / 2;
+      int g = grid_for(npairs);
+      k_outer_round<<<g, kThreads, 0, s>>>(E, A, B, C, E2, A2, B2, C2, len, fold, 1, r, c,
+                                           sc.partial);
+      BZ_LAUNCH_CHECK();
+      host_partial_sum(sc.partial, g, 3, sc.sums, sc.host, c, s, sc.channel);
+      if (fold) {
+        std::swap(E, E2);
+        std::swap(A, A2);
+        std::swap(B, B2);
+        std::swap(C, C2);
+        len /= 2;
+      }
     }
     fp co[4];
     r = round_message(ts, c, claim, sc.host, 4, a.q, co);
     for (int i = 0; i < 4; i++) out.outer[4 * round + i] = co[i];
     out.rx[round] = r;
   }
-  // the last fold leaves one entry per table
-  k_outer_round<<<1, kThreads, 0, s>>>(E, A, B, C, E2, A2, B2, C2, len, 1, 0, r, c, sc.partial);
-  BZ_LAUNCH_CHECK();
-  fp fin[3];
-  BZ_CUDA(cudaMemcpyAsync(&fin[0], A2, sizeof(fp), cudaMemcpyDeviceToHost, s));
-  BZ_CUDA(cudaMemcpyAsync(&fin[1], B2, sizeof(fp), cudaMemcpyDeviceToHost, s));
-  BZ_CUDA(cudaMemcpyAsync(&fin[2], C2, sizeof(fp), cudaMemcpyDeviceToHost, s));
-  BZ_CUDA(cudaStreamSynchronize(s));
+  if (tail) {
+    // the tail's last publication: the single entries of A, B and C
+    send_r(r);
+    ch->arm();
+    ch->wait(s, reinterpret_cast<uint64_t *>(fin), 6);
+  } else {
+    // the last fold leaves one entry per table
+    k_outer_round<<<1, kThreads, 0, s>>>(E, A, B, C, E2, A2, B2, C2, len, 1, 0, r, c, sc.partial);
+    BZ_LAUNCH_CHECK();
+    BZ_CUDA(cudaMemcpyAsync(&fin[0], A2, sizeof(fp), cudaMemcpyDeviceToHost, s));
+    BZ_CUDA(cudaMemcpyAsync(&fin[1], B2, sizeof(fp), cudaMemcpyDeviceToHost, s));
+    BZ_CUDA(cudaMemcpyAsync(&fin[2], C2, sizeof(fp), cudaMemcpyDeviceToHost, s));
+    BZ_CUDA(cudaStreamSynchronize(s));
+  }
+  } catch (...) {
+    if (tail) {  // release the waiting kernel before the lane is reused
+      ch->abort();
+      cudaStreamSynchronize(s);
+      ch->clear_down();
+    }
+    throw;
+  }
+  tail = false;
   uint8_t msg[48];
   for (int k = 0; k < 3; k++) {
     out.abc[k] = fin[k];
@@ -384,31 +555,63 @@ void spartan_prove(const SpartanArgs &a, Transcript &ts, SpartanScratch &sc, cud
   out.ry.resize(nc);
   len = Cn;
   int w_bits = 1;
+  fp dw[2];
+  try {
   for (int round = 0; round < nc; round++) {
     int fold = round > 0;
-    size_t npairs = fold ? (len / 2 + 1) / 2 : len / 2;
-    int g = grid_for(npairs);
-    k_inner_round<<<g, kThreads, 0, s>>>(D, W, a.hbits, w_bits, D2, W2, len, fold, 1, r, c,
-                                         sc.partial);
-    BZ_LAUNCH_CHECK();
-    host_partial_sum(sc.partial, g, 2, sc.sums, sc.host, c, s, sc.channel);
-    if (fold) {
-      std::swap(D, D2);
-      std::swap(W, W2);
-      len /= 2;
-      w_bits = 0;
+    if (!tail && ch && resident && len <= (size_t)kSpTailN) {
+      sp_inner_tail<<<1, kThreads, 0, s>>>(D, W, a.hbits, w_bits, (int)len, fold, nc - round, c,
+                                           ch->dev, ch->next + 1, ch->down_dev,
+                                           ch->down_next + 1);
+      BZ_LAUNCH_CHECK();
+      tail = true;
+    }
+    if (tail) {
+      if (fold) {
+        send_r(r);
+        len /= 2;
+      }
+      ch->arm();
+      ch->wait(s, reinterpret_cast<uint64_t *>(sc.host), 4);
+    } else {
+      size_t npairs = fold ? (len / 2 + 1) / 2 : len / 2;
+      int g = grid_for(npairs);
+      k_inner_round<<<g, kThreads, 0, s>>>(D, W, a.hbits, w_bits, D2, W2, len, fold, 1, r, c,
+                                           sc.partial);
+      BZ_LAUNCH_CHECK();
+      host_partial_sum(sc.partial, g, 2, sc.sums, sc.host, c, s, sc.channel);
+      if (fold) {
+        std::swap(D, D2);
+        std::swap(W, W2);
+        len /= 2;
+        w_bits = 0;
+      }
     }
     fp co[3];
     r = round_message(ts, c, claim, sc.host, 3, a.q, co);
     for (int i = 0; i < 3; i++) out.inner[3 * round + i] = co[i];
     out.ry[round] = r;
   }
-  k_inner_round<<<1, kThreads, 0, s>>>(D, W, a.hbits, w_bits, D2, W2, len, 1, 0, r, c, sc.partial);
-  BZ_LAUNCH_CHECK();
-  fp dw[2];
-  BZ_CUDA(cudaMemcpyAsync(&dw[0], D2, sizeof(fp), cudaMemcpyDeviceToHost, s));
-  BZ_CUDA(cudaMemcpyAsync(&dw[1], W2, sizeof(fp), cudaMemcpyDeviceToHost, s));
-  BZ_CUDA(cudaStreamSynchronize(s));
+  if (tail) {
+    send_r(r);
+    ch->arm();
+    ch->wait(s, reinterpret_cast<uint64_t *>(dw), 4);
+  } else {
+    k_inner_round<<<1, kThreads, 0, s>>>(D, W, a.hbits, w_bits, D2, W2, len, 1, 0, r, c,
+                                         sc.partial);
+    BZ_LAUNCH_CHECK();
+    BZ_CUDA(cudaMemcpyAsync(&dw[0], D2, sizeof(fp), cudaMemcpyDeviceToHost, s));
+    BZ_CUDA(cudaMemcpyAsync(&dw[1], W2, sizeof(fp), cudaMemcpyDeviceToHost, s));
+    BZ_CUDA(cudaStreamSynchronize(s));
+  }
+  } catch (...) {
+    if (tail) {
+      ch->abort();
+      cudaStreamSynchronize(s);
+      ch->clear_down();
+    }
+    throw;
+  }
   out.d_at_ry = dw[0];
   out.final_claim = claim;
   out.ok = fp_mul(dw[0], dw[1], c).lo == claim.lo && fp_mul(dw[0], dw[1], c).hi == claim.hi;
