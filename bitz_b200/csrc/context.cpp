@@ -54,10 +54,12 @@ void RoundChannel::wait(cudaStream_t s, uint64_t *out, int n) {
 void RoundChannel::send(const uint64_t *words, int n) {
   if (n > kMailboxWords) throw CudaError("downbox write too long");
   const unsigned long long tag = (++down_next & 0xffffffffull) << 32;
-  volatile unsigned long long *s = down_host->slot;
+  // one aligned 16-byte store per word, so a device poll sees both halves
+  unsigned long long *s = down_host->slot;
   for (int k = 0; k < n; k++) {
-    s[2 * k] = tag | (words[k] & 0xffffffffull);
-    s[2 * k + 1] = tag | (words[k] >> 32);
+    __m128i v = _mm_set_epi64x((long long)(tag | (words[k] >> 32)),
+                               (long long)(tag | (words[k] & 0xffffffffull)));
+    _mm_store_si128(reinterpret_cast<__m128i *>(s + 2 * k), v);
   }
   std::atomic_thread_fence(std::memory_order_release);
 }

@@ -58,12 +58,14 @@ struct Mailbox {
 };
 
 #if defined(__CUDACC__)
+// One 16-byte store per word: both tagged halves leave in one transaction.
 __device__ __forceinline__ void mailbox_post(Mailbox *mb, unsigned long long seq, int k,
                                              unsigned long long v) {
   const unsigned long long tag = seq << 32;
-  volatile unsigned long long *s = mb->slot;
-  s[2 * k] = tag | (v & 0xffffffffull);
-  s[2 * k + 1] = tag | (v >> 32);
+  unsigned long long *p = mb->slot + 2 * k;
+  asm volatile("st.volatile.global.v2.u64 [%0], {%1, %2};" ::"l"(p),
+               "l"(tag | (v & 0xffffffffull)), "l"(tag | (v >> 32))
+               : "memory");
 }
 #endif
 
@@ -243,25 +245,39 @@ __device__ __forceinline__ unsigned long long globaltimer_ns() {
 __device__ __forceinline__ bool mailbox_wait_device(const Mailbox *mb, unsigned long long seq,
                                                     int n, unsigned long long *out,
                                                     unsigned long long limit_ns) {
-  const volatile unsigned long long *s = mb->slot;
+  // Every poll issues all of its 16-byte loads before looking at any, so one
+  // poll costs one round trip to host memory, and the words of a successful
+  // poll are used as read.
+  const unsigned long long *s = mb->slot;
   const unsigned long long tag = seq & 0xffffffffull;
   const unsigned long long t0 = globaltimer_ns();
   for (;;) {
-    bool ready = true;
-    for (int k = 0; k < 2 * n; k++) {
-      unsigned long long t = s[k] >> 32;
-      if (t == kDownAbortTag) return false;
-      if (t != tag) {
-        ready = false;
-        break;
+    unsigned long long x[kMailboxWords], y[kMailboxWords];
+#pragma unroll
+    for (int k = 0; k < kMailboxWords; k++)
+      if (k < n)
+        asm volatile("ld.volatile.global.v2.u64 {%0, %1}, [%2];"
+                     : "=l"(x[k]), "=l"(y[k])
+                     : "l"(s + 2 * k)
+                     : "memory");
+    bool ready = true, aborted = false;
+#pragma unroll
+    for (int k = 0; k < kMailboxWords; k++)
+      if (k < n) {
+        const unsigned long long tx = x[k] >> 32, ty = y[k] >> 32;
+        aborted |= tx == kDownAbortTag || ty == kDownAbortTag;
+        ready &= tx == tag && ty == tag;
       }
+    if (aborted) return false;
+    if (ready) {
+#pragma unroll
+      for (int k = 0; k < kMailboxWords; k++)
+        if (k < n) out[k] = (x[k] & 0xffffffffull) | (y[k] << 32);
+      return true;
     }
-    if (ready) break;
     if (globaltimer_ns() - t0 > limit_ns) return false;
-    __nanosleep(64);
+    __nanosleep(32);
   }
-  for (int k = 0; k < n; k++) out[k] = (s[2 * k] & 0xffffffffull) | (s[2 * k + 1] << 32);
-  return true;
 }
 #endif
 
