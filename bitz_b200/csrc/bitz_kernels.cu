@@ -78,6 +78,7 @@ __global__ void k_mt_transpose(const uint32_t *__restrict__ off, const uint32_t 
   __syncthreads();
   for (size_t c = blockIdx.x * (size_t)blockDim.x + threadIdx.x; c <= padded;
        c += (size_t)gridDim.x * blockDim.x) {
+    if (c == 0) continue;  // the constant column: k_mt_col0
     f128 v = mk(0, 0);
     if (c < ncols) {
       wide acc = wzero();
@@ -87,17 +88,31 @@ __global__ void k_mt_transpose(const uint32_t *__restrict__ off, const uint32_t 
       }
       v = greduce(acc);
     }
-    if (c == 0)
-      *w0 = v;
-    else
-      st(weights + (c - 1), v);
+    st(weights + (c - 1), v);
   }
+}
+
+// The constant column holds one entry per lift with a constant term (hundreds
+// where the others hold under ten), so one block shares it out.
+__global__ void k_mt_col0(const uint32_t *__restrict__ off, const uint32_t *__restrict__ row,
+                          const f128 *__restrict__ u1, const f128 *__restrict__ u2, f128 *w0) {
+  wide acc = wzero();
+  for (uint32_t e = off[0] + threadIdx.x; e < off[1]; e += blockDim.x) {
+    uint32_t r = row[e];
+    wacc(acc, gmul_wide(ld(u1 + (r & 127)), ld(u2 + (r >> 7))));
+  }
+  f128 v = greduce(acc);
+  uint64_t w[2] = {v.lo, v.hi};
+  block_xor_reduce<2>(w);
+  if (threadIdx.x == 0) st(w0, mk(w[0], w[1]));
 }
 
 void mt_transpose(const uint32_t *off, const uint32_t *row, size_t ncols, const f128 *u1,
                   const f128 *u2, f128 *weights, size_t padded, f128 *w0, cudaStream_t s) {
   k_mt_transpose<<<grid_for(padded + 1), kThreads, 0, s>>>(off, row, ncols, u1, u2, weights,
                                                            padded, w0);
+  BZ_LAUNCH_CHECK();
+  k_mt_col0<<<1, kThreads, 0, s>>>(off, row, u1, u2, w0);
   BZ_LAUNCH_CHECK();
 }
 

@@ -646,11 +646,14 @@ std::vector<uint8_t> ProofSystem::ligerito(cudaStream_t s, f128 target) {
     for (int q = 0; q < L.queries; q++) {
       sq[q] = gmul(mu, beta[q]);
       claim = gadd(claim, gmul(sq[q], vals[q]));
+      // Wh_t(x_q) = sum over the set bits s >= t of idx of Wh_t(X^s)
       for (int tt = 0; tt < kMaxRsDim; tt++) {
         f128 w = mk(0, 0);
         if (tt < l)
-          for (int sb = tt; sb < kMaxRsDim; sb++)
-            if ((idx[q] >> sb) & 1) w = gadd(w, T.wh_host[tt * kMaxRsDim + sb]);
+          for (uint64_t bits = idx[q] >> tt; bits; bits &= bits - 1) {
+            int sb = tt + __builtin_ctzll(bits);
+            w = gadd(w, T.wh_host[tt * kMaxRsDim + sb]);
+          }
         wq[(size_t)q * kMaxRsDim + tt] = w;
       }
     }
