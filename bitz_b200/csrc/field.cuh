@@ -15,6 +15,9 @@
 // the canonical residue, so the transcript sees exactly the reference's bytes.
 #pragma once
 #include <stdint.h>
+#if !defined(__CUDA_ARCH__)
+#include <immintrin.h>
+#endif
 
 #if defined(__CUDACC__)
 #define BZ_HD __host__ __device__ __forceinline__
@@ -76,8 +79,38 @@ BZ_HD void clmul64(uint64_t a, uint64_t b, uint64_t &lo, uint64_t &hi) {
   hi = h ^ (m >> 32);
 }
 
+#if !defined(__CUDA_ARCH__)
+// The host's scalar steps use the CPU's carryless multiply (PCLMULQDQ) when
+// it has one; the result is the same 256-bit product.
+__attribute__((target("pclmul,sse4.1"))) inline wide gmul_wide_pclmul(f128 a, f128 b) {
+  const __m128i A = _mm_set_epi64x((long long)a.hi, (long long)a.lo);
+  const __m128i B = _mm_set_epi64x((long long)b.hi, (long long)b.lo);
+  const __m128i lo = _mm_clmulepi64_si128(A, B, 0x00);
+  const __m128i hi = _mm_clmulepi64_si128(A, B, 0x11);
+  const __m128i mid = _mm_xor_si128(_mm_clmulepi64_si128(A, B, 0x10),
+                                    _mm_clmulepi64_si128(A, B, 0x01));
+  wide r;
+  r.w0 = (uint64_t)_mm_cvtsi128_si64(lo);
+  r.w1 = (uint64_t)_mm_extract_epi64(lo, 1) ^ (uint64_t)_mm_cvtsi128_si64(mid);
+  r.w2 = (uint64_t)_mm_cvtsi128_si64(hi) ^ (uint64_t)_mm_extract_epi64(mid, 1);
+  r.w3 = (uint64_t)_mm_extract_epi64(hi, 1);
+  return r;
+}
+inline bool host_has_pclmul() {
+  static const bool yes = __builtin_cpu_supports("pclmul") && __builtin_cpu_supports("sse4.1");
+  return yes;
+}
+#endif
+
 // 128x128 -> 256 carryless product, second Karatsuba level.
+BZ_HD wide gmul_wide_portable(f128 a, f128 b);
 BZ_HD wide gmul_wide(f128 a, f128 b) {
+#if !defined(__CUDA_ARCH__)
+  if (host_has_pclmul()) return gmul_wide_pclmul(a, b);
+#endif
+  return gmul_wide_portable(a, b);
+}
+BZ_HD wide gmul_wide_portable(f128 a, f128 b) {
   uint64_t l0, l1, h0, h1, m0, m1;
   clmul64(a.lo, b.lo, l0, l1);
   clmul64(a.hi, b.hi, h0, h1);

@@ -500,6 +500,7 @@ std::vector<uint8_t> ProofSystem::ligerito(cudaStream_t s, f128 target) {
   Tables &T = tables(s);
   Transcript &t = *ts_;
   const PcsConfig &cfg = pcs_;
+  Phases ph(s, lane_->channel());
   // challenger schedule (ligerito.rs:47-63)
   std::vector<uint32_t> sched;
   for (int i = 0; i < cfg.nlevels; i++) {
@@ -606,6 +607,7 @@ std::vector<uint8_t> ProofSystem::ligerito(cudaStream_t s, f128 target) {
       t.prover_message(&cnt, 4);
       t.prover_message(hf, n * 16);  // one f128 message per entry, no framing between
     }
+    ph.mark("lig sumcheck+encode");
     // queries into this level's codeword: the rows and Merkle paths are
     // gathered on the device and only they cross to the host
     grind();
@@ -662,6 +664,7 @@ std::vector<uint8_t> ProofSystem::ligerito(cudaStream_t s, f128 target) {
     BZ_CUDA(cudaMemcpyAsync(W.qw.get(), wq, nwq * 16, cudaMemcpyHostToDevice, s));
     BZ_CUDA(cudaMemcpyAsync(W.qs.get(), sq, (size_t)L.queries * 16, cudaMemcpyHostToDevice, s));
     query_basis(W.qw.get(), W.qs.get(), L.queries, l, b, s);
+    ph.mark("lig queries+glue");
     if (!last) {
       cw = next_cw[flip].get();
       nodes = next_nodes[flip].get();
