@@ -139,16 +139,26 @@ __global__ void gkr_final_bind(const f128 *__restrict__ c, size_t n_half, f128 r
 // and sums exactly as gkr_bind_sums / gkr_final_bind, and posts the round's
 // four words to the mailbox (publication seq0 + i0 - i). A missing challenge
 // ends the kernel without a post, which the host reads as a failed round.
+//
+// A round is a chain of three dependent products per element (the bind,
+// e * L, then * R); with few elements one thread per element leaves the
+// block idle behind that chain, so the round is spread by product instead:
+// the 4h binds (and the eq update) across the block, then the 2h products
+// with e, then the 2h wide products, each level one product per thread.
 constexpr int kTailH = 256;
+constexpr int kTailThreads = 512;
 constexpr unsigned long long kTailWaitNs = 2000000000ull;  // 2 s per challenge
 
-__global__ void __launch_bounds__(kThreads) gkr_tail(const f128 *__restrict__ c, size_t n_half,
-                                                     int i0, const f128 *__restrict__ eq,
-                                                     uint32_t at_one_mask, Mailbox *mb,
-                                                     unsigned long long seq0, const Mailbox *down,
-                                                     unsigned long long dseq0, size_t colmask,
-                                                     size_t live_cols) {
+__global__ void __launch_bounds__(kTailThreads) gkr_tail(const f128 *__restrict__ c,
+                                                         size_t n_half, int i0,
+                                                         const f128 *__restrict__ eq,
+                                                         uint32_t at_one_mask, Mailbox *mb,
+                                                         unsigned long long seq0,
+                                                         const Mailbox *down,
+                                                         unsigned long long dseq0, size_t colmask,
+                                                         size_t live_cols) {
   __shared__ f128 L[4 * kTailH], R[4 * kTailH], E[2 * kTailH];
+  __shared__ uint64_t red[4][kTailThreads / 32];
   __shared__ unsigned long long chal[2];
   __shared__ int ok;
   const int h0 = i0 > 0 ? 1 << (i0 - 1) : 1;
@@ -177,34 +187,79 @@ __global__ void __launch_bounds__(kThreads) gkr_tail(const f128 *__restrict__ c,
     }
     const int h = 1 << (i - 1), h2 = 2 * h;
     const int at_one = (at_one_mask >> (i - 1)) & 1;
-    wide sb = wzero(), si = wzero();
-    for (int x = threadIdx.x; x < h; x += blockDim.x) {
-      if (padded((size_t)x, colmask, live_cols)) {
-        f128 e = gadd(E[x], E[x + h]);
-        E[x] = e;
-        sb.w0 ^= e.lo;
-        sb.w1 ^= e.hi;
+    // level 1: the binds of round i+1 at r; entry (x, q) is L[x], L[x+h],
+    // R[x], R[x+h] for q = 0..3, each read and written by one thread only;
+    // the q = 0 thread also sums the eq table down
+    for (int t = threadIdx.x; t < 4 * h; t += blockDim.x) {
+      const int x = t >> 2, q = t & 3;
+      if (q == 0) E[x] = gadd(E[x], E[x + h]);
+      if (padded((size_t)x, colmask, live_cols)) continue;  // stays one
+      f128 *T = q < 2 ? L : R;
+      const int at = x + (q & 1) * h;
+      T[at] = gadd(T[at], gmul(r, gadd(T[at + h2], T[at])));
+    }
+    __syncthreads();
+    // level 2: P = e * L_b, Q = e * (L_1 + L_0), kept in the halves' upper
+    // quarters [2h, 3h), which the binds above have consumed
+    f128 *P = L + h2, *Q = R + h2;
+    for (int t = threadIdx.x; t < 2 * h; t += blockDim.x) {
+      const int x = t >> 1;
+      const f128 e = E[x];
+      if (padded((size_t)x, colmask, live_cols)) {  // e * 1 and e * 0
+        if (t & 1)
+          Q[x] = mk(0, 0);
+        else
+          P[x] = e;
         continue;
       }
-      f128 l0 = gadd(L[x], gmul(r, gadd(L[x + h2], L[x])));
-      f128 l1 = gadd(L[x + h], gmul(r, gadd(L[x + h + h2], L[x + h])));
-      f128 r0 = gadd(R[x], gmul(r, gadd(R[x + h2], R[x])));
-      f128 r1 = gadd(R[x + h], gmul(r, gadd(R[x + h + h2], R[x + h])));
-      L[x] = l0;
-      L[x + h] = l1;
-      R[x] = r0;
-      R[x + h] = r1;
-      f128 e = gadd(E[x], E[x + h]);
-      E[x] = e;
-      f128 lb = at_one ? l1 : l0, rb = at_one ? r1 : r0;
-      wacc(sb, gmul_wide(gmul(e, lb), rb));
-      wacc(si, gmul_wide(gmul(e, gadd(l1, l0)), gadd(r1, r0)));
+      if (t & 1)
+        Q[x] = gmul(e, gadd(L[x + h], L[x]));
+      else
+        P[x] = gmul(e, at_one ? L[x + h] : L[x]);
     }
-    f128 a = greduce(sb), b = greduce(si);
-    uint64_t v[4] = {a.lo, a.hi, b.lo, b.hi};
-    block_xor_reduce<4>(v);  // also orders this round's table writes before the next
-    if (threadIdx.x == 0)
-      for (int k = 0; k < 4; k++) mailbox_post(mb, seq, k, v[k]);
+    __syncthreads();
+    // level 3: P * R_b into the first sum, Q * (R_1 + R_0) into the second
+    uint64_t v[4] = {0, 0, 0, 0};
+    for (int t = threadIdx.x; t < 2 * h; t += blockDim.x) {
+      const int x = t >> 1;
+      if (padded((size_t)x, colmask, live_cols)) {  // P * 1 and Q * 0
+        if (!(t & 1)) {
+          v[0] ^= P[x].lo;
+          v[1] ^= P[x].hi;
+        }
+        continue;
+      }
+      if (t & 1) {
+        f128 p = gmul(Q[x], gadd(R[x + h], R[x]));
+        v[2] ^= p.lo;
+        v[3] ^= p.hi;
+      } else {
+        f128 p = gmul(P[x], at_one ? R[x + h] : R[x]);
+        v[0] ^= p.lo;
+        v[1] ^= p.hi;
+      }
+    }
+    // block XOR-reduction of the four words; thread 0 posts
+#pragma unroll
+    for (int k = 0; k < 4; k++)
+#pragma unroll
+      for (int off = 16; off > 0; off >>= 1) v[k] ^= __shfl_xor_sync(0xffffffffu, v[k], off);
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    if (lane == 0)
+      for (int k = 0; k < 4; k++) red[k][warp] = v[k];
+    __syncthreads();
+    if (warp == 0) {
+      const int nw = blockDim.x >> 5;
+      for (int k = 0; k < 4; k++) {
+        uint64_t x = lane < nw ? red[k][lane] : 0;
+#pragma unroll
+        for (int off = 16; off > 0; off >>= 1) x ^= __shfl_xor_sync(0xffffffffu, x, off);
+        v[k] = x;
+      }
+      if (lane == 0)
+        for (int k = 0; k < 4; k++) mailbox_post(mb, seq, k, v[k]);
+    }
+    __syncthreads();  // this round's tables before the next round's reads
   }
 }
 
@@ -286,7 +341,7 @@ f128 gkr_prove(int s, const f128 *zeta, uint32_t grind_bits, Transcript &ts, Gkr
       if (!tail && ch && resident && (i == 0 || ((size_t)1 << (i - 1)) <= (size_t)kTailH)) {
         uint32_t mask = 0;
         for (int k = 1; k <= i; k++) mask |= (uint32_t)gis_zero(point[k - 1]) << (k - 1);
-        gkr_tail<<<1, kThreads, 0, st_>>>(c, n_half, i, sc.eq, mask, ch->dev, ch->next + 1,
+        gkr_tail<<<1, kTailThreads, 0, st_>>>(c, n_half, i, sc.eq, mask, ch->dev, ch->next + 1,
                                           ch->down_dev, ch->down_next + 1, colmask, live);
         BZ_LAUNCH_CHECK();
         tail = true;
