@@ -417,7 +417,10 @@ int bitz_l2_flush(void) {
   std::lock_guard<std::mutex> lk(mu);
   try {
     cudaStream_t s = Context::get().stream();
-    if (!buf) BZ_CUDA(cudaMalloc(&buf, bytes));
+    if (!buf) {
+      AllocScope gate;
+      BZ_CUDA(cudaMalloc(&buf, bytes));
+    }
     static unsigned char v = 0;
     BZ_CUDA(cudaMemsetAsync(buf, ++v, bytes, s));
     BZ_CUDA(cudaStreamSynchronize(s));

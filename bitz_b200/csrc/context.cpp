@@ -75,7 +75,64 @@ void RoundChannel::clear_down() {
   for (int k = 0; k < 2 * kMailboxWords; k++) s[k] = 0;
 }
 
+// ------------------------------------------------------------ DeviceGate
+
+static thread_local int resident_depth = 0;
+static thread_local int alloc_depth = 0;
+
+DeviceGate &DeviceGate::get() {
+  static DeviceGate *g = new DeviceGate();
+  return *g;
+}
+
+void DeviceGate::enter_resident() {
+  std::unique_lock<std::mutex> lk(mu_);
+  cv_.wait(lk, [&] { return !alloc_ && allocs_waiting_ == 0; });
+  residents_++;
+}
+
+void DeviceGate::leave_resident() {
+  std::lock_guard<std::mutex> lk(mu_);
+  if (--residents_ == 0) cv_.notify_all();
+}
+
+void DeviceGate::enter_alloc() {
+  std::unique_lock<std::mutex> lk(mu_);
+  allocs_waiting_++;
+  cv_.wait(lk, [&] { return !alloc_ && residents_ == 0; });
+  allocs_waiting_--;
+  alloc_ = true;
+}
+
+void DeviceGate::leave_alloc() {
+  std::lock_guard<std::mutex> lk(mu_);
+  alloc_ = false;
+  cv_.notify_all();
+}
+
+ResidentScope::ResidentScope(bool on) : on_(on) {
+  if (on_ && resident_depth++ == 0) DeviceGate::get().enter_resident();
+}
+
+ResidentScope::~ResidentScope() {
+  if (on_ && --resident_depth == 0) DeviceGate::get().leave_resident();
+}
+
+AllocScope::AllocScope(bool strict) {
+  if (resident_depth > 0) {
+    if (strict) throw CudaError("device allocation while a round kernel of this lane may wait");
+    return;  // unwinding out of a resident stretch: free without the gate
+  }
+  on_ = true;
+  if (alloc_depth++ == 0) DeviceGate::get().enter_alloc();
+}
+
+AllocScope::~AllocScope() {
+  if (on_ && --alloc_depth == 0) DeviceGate::get().leave_alloc();
+}
+
 Context::Context() {
+  AllocScope gate;
   BZ_CUDA(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking));
   acc_.resize(8 * 128);
   BZ_CUDA(cudaMallocHost(&host_, 64 * sizeof(uint64_t)));
@@ -85,6 +142,8 @@ Context::Context() {
   gk_.acc = acc_.get();
   gk_.host = host_;
   gk_.pair = gk_pair_.get();
+  gk_ctl_.resize(kMaxPointGkr);
+  gk_.ctl = gk_ctl_.get();
   // the round mailbox: one mapped pinned page and a device block counter
   void *mb = nullptr;
   BZ_CUDA(cudaHostAlloc(&mb, 4096, cudaHostAllocMapped));
@@ -105,6 +164,7 @@ Context::Context() {
 Context::~Context() {
   if (stream_) cudaStreamSynchronize(stream_);
   workspace.reset();
+  AllocScope gate(false);
   if (channel_.host) cudaFreeHost(channel_.host);
   if (host_) cudaFreeHost(host_);
   if (stream_) cudaStreamDestroy(stream_);
@@ -117,7 +177,14 @@ std::atomic<unsigned long long> &launch_counter() {
 
 Context &Context::get() {
   // One default lane per process, created on first use on the current device.
-  static Context *ctx = new Context();
+  // It proves one statement at a time with the GPU to itself, so it keeps the
+  // middle GKR rounds in one resident kernel; pool lanes, which share the GPU,
+  // launch them one by one.
+  static Context *ctx = [] {
+    Context *c = new Context();
+    c->gk_.resident_middle = true;
+    return c;
+  }();
   return *ctx;
 }
 

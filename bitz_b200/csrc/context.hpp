@@ -31,12 +31,16 @@ class DeviceBuffer {
   }
   void resize(size_t n) {
     if (n <= n_) return;
+    AllocScope gate;
     release();
     BZ_CUDA(cudaMalloc(&p_, (n ? n : 1) * sizeof(T)));
     n_ = n;
   }
   void release() {
-    if (p_) cudaFree(p_);
+    if (p_) {
+      AllocScope gate(false);
+      cudaFree(p_);
+    }
     p_ = nullptr;
     n_ = 0;
   }
@@ -61,12 +65,16 @@ class PinnedBuffer {
  public:
   PinnedBuffer() = default;
   ~PinnedBuffer() {
-    if (p_) cudaFreeHost(p_);
+    if (p_) {
+      AllocScope gate(false);
+      cudaFreeHost(p_);
+    }
   }
   PinnedBuffer(const PinnedBuffer &) = delete;
   PinnedBuffer &operator=(const PinnedBuffer &) = delete;
   T *get(size_t n) {
     if (n > n_) {
+      AllocScope gate;
       if (p_) cudaFreeHost(p_);
       p_ = nullptr;
       n_ = 0;
@@ -144,6 +152,7 @@ class Context {
   uint64_t *host_ = nullptr;
   GkrScratch gk_;
   DeviceBuffer<f128> gk_layers_, gk_eq_, gk_eq_scratch_, gk_pair_;
+  DeviceBuffer<RoundCtl> gk_ctl_;
   RoundChannel channel_;
   DeviceBuffer<unsigned int> counter_;
 };

@@ -6,6 +6,8 @@
 #include <stdio.h>
 
 #include <atomic>
+#include <condition_variable>
+#include <mutex>
 #include <stdexcept>
 #include <string>
 
@@ -229,6 +231,56 @@ struct RoundChannel {
   void clear_down();
 };
 
+// Kernels that wait for their lane's host thread, and calls that wait for the
+// whole device. Such a kernel must never be in flight while another thread
+// is inside cudaFree, cudaFreeHost, cudaMalloc, cudaMallocHost or
+// cudaHostAlloc: the call waits for the kernel, the driver can hold the
+// lane's host thread (its next launch or stream query) behind the call, and
+// neither moves until the kernel's time limit ends the proof. A lane holds a
+// ResidentScope from before it launches the first such kernel of a stretch
+// until the stretch has ended; those calls run under an AllocScope, which
+// waits until no ResidentScope is held and holds new ones back meanwhile.
+// Scopes nest within a thread; an allocation inside a ResidentScope of its
+// own thread is a bug and throws.
+class DeviceGate {
+ public:
+  static DeviceGate &get();
+  void enter_resident();
+  void leave_resident();
+  void enter_alloc();
+  void leave_alloc();
+
+ private:
+  std::mutex mu_;
+  std::condition_variable cv_;
+  int residents_ = 0, allocs_waiting_ = 0;
+  bool alloc_ = false;
+};
+
+class ResidentScope {
+ public:
+  explicit ResidentScope(bool on = true);
+  ~ResidentScope();
+  ResidentScope(const ResidentScope &) = delete;
+  ResidentScope &operator=(const ResidentScope &) = delete;
+
+ private:
+  bool on_;
+};
+
+class AllocScope {
+ public:
+  // `strict`: throw when this thread holds a ResidentScope (false in
+  // destructors, which must not throw and then free without the gate).
+  explicit AllocScope(bool strict = true);
+  ~AllocScope();
+  AllocScope(const AllocScope &) = delete;
+  AllocScope &operator=(const AllocScope &) = delete;
+
+ private:
+  bool on_ = false;
+};
+
 #if defined(__CUDACC__)
 // The host's abort marker: every slot tagged 0xffffffff.
 constexpr unsigned long long kDownAbortTag = 0xffffffffull;
@@ -282,6 +334,55 @@ __device__ __forceinline__ bool mailbox_wait_device(const Mailbox *mb, unsigned 
 #endif
 
 #if defined(__CUDACC__)
+// Products by one fixed element r through 4-bit windows: b = sum over j of
+// v_j X^(4j) (v_j the j-th nibble of b), so r b = XOR over j of the entry
+// r v_j X^(4j). The 32 x 16 entries live in shared memory as separate low and
+// high 64-bit words: a row of 16 words spans the 32 banks once, so the lanes
+// of a half-warp never conflict, whatever nibbles they look up. A product is
+// 32 independent lookups instead of about 550 dependent integer instructions.
+struct MulTable {
+  uint64_t lo[32][16], hi[32][16];
+};
+
+// Every thread of the block calls it; it synchronises the block twice.
+__device__ __forceinline__ void mul_table_build(MulTable &T, f128 r) {
+  for (int k = threadIdx.x; k < 128; k += blockDim.x) {
+    const f128 b = gmul_xk(r, k);  // r X^k: the single-bit entry of window k / 4
+    T.lo[k >> 2][1 << (k & 3)] = b.lo;
+    T.hi[k >> 2][1 << (k & 3)] = b.hi;
+  }
+  __syncthreads();
+  for (int e = threadIdx.x; e < 512; e += blockDim.x) {
+    const int j = e >> 4, v = e & 15;
+    if (v != 0 && (v & (v - 1)) == 0) continue;  // written above
+    uint64_t lo = 0, hi = 0;
+#pragma unroll
+    for (int b = 0; b < 4; b++)
+      if ((v >> b) & 1) {
+        lo ^= T.lo[j][1 << b];
+        hi ^= T.hi[j][1 << b];
+      }
+    T.lo[j][v] = lo;
+    T.hi[j][v] = hi;
+  }
+  __syncthreads();
+}
+
+__device__ __forceinline__ f128 mul_table(const MulTable &T, f128 b) {
+  const uint32_t w[4] = {(uint32_t)b.lo, (uint32_t)(b.lo >> 32), (uint32_t)b.hi,
+                         (uint32_t)(b.hi >> 32)};
+  uint64_t lo = 0, hi = 0;
+#pragma unroll
+  for (int i = 0; i < 4; i++)
+#pragma unroll
+    for (int n = 0; n < 8; n++) {
+      const uint32_t v = (w[i] >> (4 * n)) & 15u;
+      lo ^= T.lo[8 * i + n][v];
+      hi ^= T.hi[8 * i + n][v];
+    }
+  return mk(lo, hi);
+}
+
 __device__ __forceinline__ f128 ld(const f128 *p) {
   ulonglong2 v = *reinterpret_cast<const ulonglong2 *>(p);
   return mk(v.x, v.y);

@@ -133,6 +133,21 @@ BZ_HD f128 greduce(const wide &r) {
 
 BZ_HD f128 gmul(f128 a, f128 b) { return greduce(gmul_wide(a, b)); }
 
+// r * X^k for 0 <= k < 128: the 256-bit shift of r, reduced.
+BZ_HD f128 gmul_xk(f128 r, int k) {
+  if (k == 0) return r;
+  wide w;
+  if (k < 64) {
+    w = wide{r.lo << k, (r.hi << k) | (r.lo >> (64 - k)), r.hi >> (64 - k), 0};
+  } else if (k == 64) {
+    w = wide{0, r.lo, r.hi, 0};
+  } else {
+    const int s = k - 64;
+    w = wide{0, r.lo << s, (r.hi << s) | (r.lo >> (64 - s)), r.hi >> (64 - s)};
+  }
+  return greduce(w);
+}
+
 // ------------------------------------------------------------ prime field
 
 struct fp {

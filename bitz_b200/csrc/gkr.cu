@@ -14,6 +14,9 @@
 // down to round i's (eq_i[x] = eq_{i+1}[x] + eq_{i+1}[x + 2^i], summing out
 // coordinate i), and accumulates round i's two sums from the freshly bound
 // values; 32 bytes leave the device per round.
+#include <chrono>
+#include <cstdio>
+
 #include "context.hpp"
 #include "eq.cuh"
 #include "gkr.hpp"
@@ -49,10 +52,69 @@ __global__ void gkr_parent(const f128 *__restrict__ child, size_t half, f128 *__
     st(out + k, padded(k, colmask, live) ? mk(1, 0) : gmul(ld(child + k), ld(child + half + k)));
 }
 
+// Queued rounds. With the host's challenges delivered to the device, every
+// bind round of a layer is queued at the layer's start, so no round waits for
+// a launch from the host: the last block of each round kernel posts the
+// round's sums, then waits (bounded) for the next challenge in the lane's
+// downbox and leaves it in `out` for the next kernel in the stream, which
+// reads it from `in`. Only that one block waits; the next kernel starts when
+// it has left. A missing challenge (time limit or the host's abort marker)
+// leaves flag 2, and every later kernel of the chain passes it on and does
+// no work.
+struct RoundLink {
+  const RoundCtl *in;       // this round's challenge; null: the launch argument
+  RoundCtl *out;            // the next challenge; null: no wait
+  const Mailbox *down;      // the host's downbox
+  unsigned long long dseq;  // the host's publication of the next challenge
+};
+constexpr unsigned long long kRoundWaitNs = 2000000000ull;  // 2 s per challenge
+
+// Every thread calls it; false when the chain has stopped (the block returns).
+__device__ __forceinline__ bool round_begin(const RoundLink &lk, f128 r_arg, f128 &r) {
+  __shared__ unsigned long long s[3];
+  if (!lk.in) {
+    r = r_arg;
+    return true;
+  }
+  if (threadIdx.x == 0) {
+    s[0] = lk.in->r_lo;
+    s[1] = lk.in->r_hi;
+    s[2] = lk.in->flag;
+  }
+  __syncthreads();
+  r = mk(s[0], s[1]);
+  if (s[2] == 1) return true;
+  if (blockIdx.x == 0 && threadIdx.x == 0 && lk.out) lk.out->flag = 2;
+  return false;
+}
+
+// publish<4>, then the last block fetches the next challenge for `out`.
+__device__ __forceinline__ void round_end(unsigned long long *acc, const Publish &p,
+                                          const RoundLink &lk) {
+  if (!p.counter) return;
+  if (threadIdx.x == 0) {
+    __threadfence();
+    const unsigned int prev = atomicAdd(p.counter, 1u);
+    if (prev == gridDim.x - 1) {
+      __threadfence();
+#pragma unroll
+      for (int k = 0; k < 4; k++) mailbox_post(p.mailbox, p.seq, k, atomicExch(acc + k, 0ull));
+      *p.counter = 0;
+      if (lk.out) {
+        unsigned long long w[2] = {0, 0};
+        const bool ok = mailbox_wait_device(lk.down, lk.dseq, 2, w, kRoundWaitNs);
+        lk.out->r_lo = w[0];
+        lk.out->r_hi = w[1];
+        lk.out->flag = ok ? 1u : 2u;
+      }
+    }
+  }
+}
+
 // Round i's sums (round_sums, lib.rs:164-216) before any bind: the top round.
 __global__ void gkr_top_sums(const f128 *__restrict__ c, size_t n_half, size_t h,
                              const f128 *__restrict__ eq, int at_one, unsigned long long *acc,
-                             Publish pub, size_t colmask, size_t live) {
+                             Publish pub, RoundLink lk, size_t colmask, size_t live) {
   const f128 *L = c, *R = c + n_half;
   wide sb = wzero(), si = wzero();
   for (size_t x = blockIdx.x * (size_t)blockDim.x + threadIdx.x; x < h;
@@ -71,14 +133,17 @@ __global__ void gkr_top_sums(const f128 *__restrict__ c, size_t n_half, size_t h
   }
   f128 a = greduce(sb), b = greduce(si);
   uint64_t v[4] = {a.lo, a.hi, b.lo, b.hi};
-  block_xor_publish<4>(v, acc, pub);
+  block_xor_atomic<4>(v, acc);
+  round_end(acc, pub, lk);
 }
 
 // Bind round i+1 at r (halves of 2^(i+1)), derive eq_i in place, and sum
 // round i (halves of 2^i). Thread x < 2^i owns entries x and x + 2^i.
-__global__ void gkr_bind_sums(f128 *__restrict__ c, size_t n_half, size_t h, f128 r,
+__global__ void gkr_bind_sums(f128 *__restrict__ c, size_t n_half, size_t h, f128 r_arg,
                               f128 *__restrict__ eq, int at_one, unsigned long long *acc,
-                              Publish pub, size_t colmask, size_t live) {
+                              Publish pub, RoundLink lk, size_t colmask, size_t live) {
+  f128 r;
+  if (!round_begin(lk, r_arg, r)) return;
   f128 *L = c, *R = c + n_half;
   const size_t h2 = 2 * h;
   wide sb = wzero(), si = wzero();
@@ -109,7 +174,217 @@ __global__ void gkr_bind_sums(f128 *__restrict__ c, size_t n_half, size_t h, f12
   }
   f128 a = greduce(sb), b = greduce(si);
   uint64_t v[4] = {a.lo, a.hi, b.lo, b.hi};
-  block_xor_publish<4>(v, acc, pub);
+  block_xor_atomic<4>(v, acc);
+  round_end(acc, pub, lk);
+}
+
+// gkr_bind_sums by tiles, for rounds where few elements leave each thread's
+// chain of eight products (four binds, two with e, two wide) as the round's
+// latency. A block takes a tile of kMidTile elements and works it in three
+// levels, each product of a level on its own thread: the 4 * kMidTile binds
+// by r through the block's window table (2 per thread), then the
+// 2 * kMidTile products with e, then the 2 * kMidTile wide products. Same
+// values, same sums as gkr_bind_sums.
+constexpr int kMidThreads = 256;
+constexpr int kMidTile = 128;
+constexpr size_t kMidMaxH = (size_t)1 << 15;  // larger rounds are issue bound: gkr_bind_sums
+static_assert(kMidThreads == 2 * kMidTile && kMidThreads == kThreads, "one product per thread");
+constexpr size_t kMidGrid = 128;  // blocks of a resident gkr_mid
+
+// Shared memory of one tile: the window table of r, the tile's bound
+// entries L[x], L[x+h], R[x], R[x+h], its eq entries and the products with e.
+struct TileShared {
+  MulTable T;
+  f128 B[4][kMidTile];
+  f128 E[kMidTile], P[kMidTile], Q[kMidTile];
+};
+
+// L2 loads: a resident kernel reads entries that other blocks wrote in its
+// previous round, which this SM's L1 may hold stale.
+__device__ __forceinline__ f128 ld_cg(const f128 *p) {
+  const ulonglong2 v = __ldcg(reinterpret_cast<const ulonglong2 *>(p));
+  return mk(v.x, v.y);
+}
+
+// Elements [x0, x0 + kMidTile) of a bind round with S.T built for r: the
+// three levels, the tile's share of the first message summed by even
+// threads into acc_w, of the second by odd ones. Every thread calls it; it
+// ends with the block synchronised.
+__device__ __forceinline__ void bind_tile(TileShared &S, f128 *L, f128 *R, f128 *eq, size_t h,
+                                          size_t x0, int at_one, size_t colmask, size_t live,
+                                          wide &acc_w) {
+  const size_t h2 = 2 * h;
+  const int t = threadIdx.x;
+  // level 1: entry (k, q) of the tile is L[x], L[x+h], R[x], R[x+h] for q = 0..3
+#pragma unroll
+  for (int it = 0; it < 4 * kMidTile / kMidThreads; it++) {
+    const int u = t + it * kMidThreads;
+    const int k = u >> 2, q = u & 3;
+    const size_t x = x0 + k;
+    if (x >= h) continue;
+    if (q == 0) {
+      const f128 e = gadd(ld_cg(eq + x), ld_cg(eq + x + h));
+      st(eq + x, e);
+      S.E[k] = e;
+    }
+    f128 v = mk(1, 0);  // a padded column stays one
+    if (!padded(x, colmask, live)) {
+      f128 *tab = q < 2 ? L : R;
+      const size_t at = x + (q & 1) * h;
+      const f128 a0 = ld_cg(tab + at), a1 = ld_cg(tab + at + h2);
+      v = gadd(a0, mul_table(S.T, gadd(a1, a0)));
+      st(tab + at, v);
+    }
+    S.B[q][k] = v;
+  }
+  __syncthreads();
+  // level 2: P = e * L_b, Q = e * (L_1 + L_0)
+  {
+    const int k = t >> 1;
+    const size_t x = x0 + k;
+    if (x < h) {
+      const f128 e = S.E[k];
+      if (padded(x, colmask, live)) {  // e * 1 and e * 0
+        if (t & 1)
+          S.Q[k] = mk(0, 0);
+        else
+          S.P[k] = e;
+      } else if (t & 1) {
+        S.Q[k] = gmul(e, gadd(S.B[1][k], S.B[0][k]));
+      } else {
+        S.P[k] = gmul(e, at_one ? S.B[1][k] : S.B[0][k]);
+      }
+    }
+  }
+  __syncthreads();
+  // level 3: P * R_b into the first sum, Q * (R_1 + R_0) into the second
+  {
+    const int k = t >> 1;
+    const size_t x = x0 + k;
+    if (x < h) {
+      if (padded(x, colmask, live)) {  // P * 1 and Q * 0
+        if (!(t & 1)) {
+          acc_w.w0 ^= S.P[k].lo;
+          acc_w.w1 ^= S.P[k].hi;
+        }
+      } else if (t & 1) {
+        wacc(acc_w, gmul_wide(S.Q[k], gadd(S.B[3][k], S.B[2][k])));
+      } else {
+        wacc(acc_w, gmul_wide(S.P[k], at_one ? S.B[3][k] : S.B[2][k]));
+      }
+    }
+  }
+  __syncthreads();  // the tile's tables before the next tile overwrites them
+}
+
+// The block's four words of the round's sums (even threads hold the first
+// message, odd ones the second).
+__device__ __forceinline__ void tile_words(const wide &acc_w, uint64_t (&v)[4]) {
+  const f128 s = greduce(acc_w);
+  const bool odd = threadIdx.x & 1;
+  v[0] = odd ? 0 : s.lo;
+  v[1] = odd ? 0 : s.hi;
+  v[2] = odd ? s.lo : 0;
+  v[3] = odd ? s.hi : 0;
+}
+
+__global__ void __launch_bounds__(kMidThreads) gkr_round(
+    f128 *__restrict__ c, size_t n_half, size_t h, f128 r_arg, f128 *__restrict__ eq, int at_one,
+    unsigned long long *acc, Publish pub, RoundLink lk, size_t colmask, size_t live) {
+  f128 r;
+  if (!round_begin(lk, r_arg, r)) return;
+  __shared__ TileShared S;
+  mul_table_build(S.T, r);
+  wide acc_w = wzero();
+  for (size_t x0 = (size_t)blockIdx.x * kMidTile; x0 < h; x0 += (size_t)gridDim.x * kMidTile)
+    bind_tile(S, c, c + n_half, eq, h, x0, at_one, colmask, live, acc_w);
+  uint64_t v[4];
+  tile_words(acc_w, v);
+  block_xor_atomic<4>(v, acc);
+  round_end(acc, pub, lk);
+}
+
+// Block 0's relay of a challenge to the other blocks of a resident kernel:
+// flag written last with release semantics, read with acquire (bounded).
+__device__ __forceinline__ void relay_post(RoundCtl *cl, const unsigned long long w[2], bool ok) {
+  cl->r_lo = w[0];
+  cl->r_hi = w[1];
+  asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(&cl->flag), "r"(ok ? 1u : 2u)
+               : "memory");
+}
+
+__device__ __forceinline__ bool relay_wait(const RoundCtl *cl, unsigned long long w[2]) {
+  const unsigned long long t0 = globaltimer_ns();
+  for (;;) {
+    unsigned int f;
+    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(f) : "l"(&cl->flag) : "memory");
+    if (f == 1) {
+      asm volatile("ld.relaxed.gpu.global.u64 %0, [%1];" : "=l"(w[0]) : "l"(&cl->r_lo) : "memory");
+      asm volatile("ld.relaxed.gpu.global.u64 %0, [%1];" : "=l"(w[1]) : "l"(&cl->r_hi) : "memory");
+      return true;
+    }
+    if (f == 2 || globaltimer_ns() - t0 > kRoundWaitNs) return false;
+    __nanosleep(64);
+  }
+}
+
+// The middle rounds of a layer (bind r_i for i = i_hi .. i_lo) in one
+// cooperative launch that stays resident: no launch between rounds, and the
+// round code stays in the instruction cache. Block 0 reads r_i from the
+// downbox (publication d0 + n - 1 - i) and relays it through ctl; every block
+// binds its tiles; the last block through the round posts the sums as
+// publication p0 + n - i. Round i - 1 reads what every block wrote in round
+// i, which is in L2 before the host can answer the post with r_{i-1}: each
+// thread fences its stores before its block counts itself done. All blocks
+// are resident together (cooperative launch), so the relay waits end; each is
+// bounded all the same.
+__global__ void __launch_bounds__(kMidThreads) gkr_mid(
+    f128 *__restrict__ c, size_t n_half, int n, int i_hi, int i_lo, f128 *__restrict__ eq,
+    unsigned long long at_one_mask, unsigned long long *acc_base, Mailbox *mb,
+    unsigned long long p0, const Mailbox *down, unsigned long long d0, RoundCtl *ctl,
+    size_t colmask, size_t live) {
+  __shared__ TileShared S;
+  __shared__ unsigned long long rs[2];
+  __shared__ int ok_s;
+  const int t = threadIdx.x;
+  for (int i = i_hi; i >= i_lo; i--) {
+    RoundCtl *cl = ctl + (n - 1 - i);
+    if (t == 0) {
+      unsigned long long w[2] = {0, 0};
+      bool ok;
+      if (blockIdx.x == 0) {
+        ok = mailbox_wait_device(down, d0 + (n - 1 - i), 2, w, kRoundWaitNs);
+        relay_post(cl, w, ok);
+      } else {
+        ok = relay_wait(cl, w);
+      }
+      rs[0] = w[0];
+      rs[1] = w[1];
+      ok_s = ok;
+    }
+    __syncthreads();
+    if (!ok_s) return;
+    mul_table_build(S.T, mk(rs[0], rs[1]));
+    const size_t h = (size_t)1 << (i - 1);
+    const int at_one = (int)((at_one_mask >> (i - 1)) & 1);
+    wide acc_w = wzero();
+    for (size_t x0 = (size_t)blockIdx.x * kMidTile; x0 < h; x0 += (size_t)gridDim.x * kMidTile)
+      bind_tile(S, c, c + n_half, eq, h, x0, at_one, colmask, live, acc_w);
+    __threadfence();  // this thread's bound entries before the block counts itself done
+    uint64_t v[4];
+    tile_words(acc_w, v);
+    unsigned long long *acc = acc_base + 4 * (n - i);
+    block_xor_atomic<4>(v, acc);
+    if (t == 0) {
+      __threadfence();
+      const unsigned int prev = atomicAdd(&cl->done, 1u);
+      if (prev == gridDim.x - 1) {
+        __threadfence();
+#pragma unroll
+        for (int k = 0; k < 4; k++) mailbox_post(mb, p0 + (n - i), k, atomicExch(acc + k, 0ull));
+      }
+    }
+  }
 }
 
 // The bind after round 0: one pair left in each half. Delivered through the
@@ -295,6 +570,50 @@ void gkr_build(const f128 *cols, int s, const f128 *images, GkrScratch &sc, cuda
 
 static f128 eq_factor(f128 r, f128 z) { return gadd(gadd(mk(1, 0), r), z); }
 
+// One bind round of hh elements per half: by tiles up to kMidMaxH, one
+// element per thread above (issue bound there).
+static void launch_bind(f128 *c, size_t n_half, size_t hh, f128 r, f128 *eq, int at_one,
+                        unsigned long long *acc, const Publish &pub, const RoundLink &lk,
+                        size_t colmask, size_t live, cudaStream_t st) {
+  if (hh <= kMidMaxH)
+    gkr_round<<<(unsigned)((hh + kMidTile - 1) / kMidTile), kMidThreads, 0, st>>>(
+        c, n_half, hh, r, eq, at_one, acc, pub, lk, colmask, live);
+  else
+    gkr_bind_sums<<<grid_for(hh), kThreads, 0, st>>>(c, n_half, hh, r, eq, at_one, acc, pub, lk,
+                                                      colmask, live);
+  BZ_LAUNCH_CHECK();
+}
+
+// gkr_mid over bind rounds i_hi .. i_lo, as a cooperative launch: one block
+// per tile of the first round, at most as many as stay resident together.
+static void launch_mid(f128 *c, size_t n_half, int n, int i_hi, int i_lo, const f128 *point,
+                       GkrScratch &sc, unsigned long long p0, unsigned long long d0,
+                       size_t colmask, size_t live, cudaStream_t st) {
+  static const int capacity = [] {
+    int dev = 0, sms = 0, per_sm = 0;
+    BZ_CUDA(cudaGetDevice(&dev));
+    BZ_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    BZ_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, gkr_mid, kMidThreads, 0));
+    return sms * per_sm;
+  }();
+  const size_t tiles = (((size_t)1 << (i_hi - 1)) + kMidTile - 1) / kMidTile;
+  const int grid = (int)std::min<size_t>(std::min<size_t>(tiles, kMidGrid), (size_t)capacity);
+  if (grid < 1) throw CudaError("gkr_mid: no resident block fits");
+  unsigned long long mask = 0;
+  for (int i = i_lo; i <= i_hi; i++) mask |= (unsigned long long)gis_zero(point[i - 1]) << (i - 1);
+  RoundChannel *ch = sc.channel;
+  f128 *eq = sc.eq;
+  unsigned long long *acc = sc.acc;
+  Mailbox *mb = ch->dev;
+  const Mailbox *down = ch->down_dev;
+  RoundCtl *ctl = sc.ctl;
+  void *args[] = {&c,   &n_half, &n,  &i_hi, &i_lo, &eq,  &mask,    &acc,
+                  &mb,  &p0,     &down, &d0,  &ctl,  &colmask, &live};
+  BZ_CUDA(cudaLaunchCooperativeKernel((const void *)gkr_mid, dim3(grid), dim3(kMidThreads), args,
+                                      0, st));
+  BZ_LAUNCH_CHECK();
+}
+
 f128 gkr_prove(int s, const f128 *zeta, uint32_t grind_bits, Transcript &ts, GkrScratch &sc,
                cudaStream_t st_, f128 *point_out) {
   f128 point[kMaxPoint], next[kMaxPoint];
@@ -313,6 +632,11 @@ f128 gkr_prove(int s, const f128 *zeta, uint32_t grind_bits, Transcript &ts, Gkr
     const char *e = getenv("BITZ_RESIDENT_ROUNDS");
     return !(e && e[0] == '0');
   }();
+  // BITZ_GKR_TRACE=1 prints the host time between consecutive round results
+  static const bool trace = getenv("BITZ_GKR_TRACE") != nullptr;
+  auto t_prev = std::chrono::steady_clock::now();
+  // no other thread's device allocation while a round kernel waits for this one
+  ResidentScope gate(ch && resident);
   try {
   for (int j = 6; j >= 0; j--) {
     f128 *c = sc.layer[j];
@@ -322,14 +646,65 @@ f128 gkr_prove(int s, const f128 *zeta, uint32_t grind_bits, Transcript &ts, Gkr
     // eq over the coordinates below the top one: 2^(n-1) entries
     eq_table_device(point, n - 1, sc.eq, sc.eq_scratch, st_);
     size_t h = n_half / 2;
-    gkr_top_sums<<<grid_for(h), kThreads, 0, st_>>>(c, n_half, h, sc.eq,
-                                                    gis_zero(point[n - 1]), sc.acc, arm(sc),
-                                                    colmask, live);
+    // Queued mode: the bind rounds above the tail's first (h <= kTailH) and
+    // the tail itself are all queued behind the top sums, each round's
+    // challenge fetched on the device. Publication p0 + (n - i) carries the
+    // sums after binding r_i, which the host posts as downbox publication
+    // d0 + (n - 1 - i). The kernel probe times kernels alone, so it runs
+    // every round as its own launch.
+    const bool queued = ch && resident && !probe.on("gkr_bind_sums");
+    int i_tail = n - 1;
+    while (i_tail > 0 && ((size_t)1 << (i_tail - 1)) > (size_t)kTailH) i_tail--;
+    const Publish top = arm(sc);
+    const unsigned long long p0 = top.seq, d0 = ch ? ch->down_next + 1 : 0;
+    RoundLink none{nullptr, nullptr, nullptr, 0};
+    // Bind round i > i_tail runs in gkr_mid (which reads r_i from the downbox
+    // itself) when the lane keeps the middle rounds resident and 2^(i-1) <=
+    // kMidMaxH; otherwise as a queued launch that reads r_i from ctl, left
+    // there by the kernel before it.
+    auto in_mid = [&](int i) {
+      return sc.resident_middle && ((size_t)1 << (i - 1)) <= kMidMaxH;
+    };
+    auto link_for = [&](int i) {  // where the kernel before bind round i leaves r_i
+      return queued && i > i_tail && !in_mid(i) ? sc.ctl + (n - 1 - i) : nullptr;
+    };
+    RoundLink top_link = none;
+    if (queued && n - 1 > i_tail) {
+      BZ_CUDA(cudaMemsetAsync(sc.ctl, 0, sizeof(RoundCtl) * rounds, st_));
+      top_link = RoundLink{nullptr, link_for(n - 1), ch->down_dev, d0};
+    }
+    gkr_top_sums<<<grid_for(h), kThreads, 0, st_>>>(c, n_half, h, sc.eq, gis_zero(point[n - 1]),
+                                                    sc.acc, top, top_link, colmask, live);
     BZ_LAUNCH_CHECK();
+    if (queued) {
+      int i = n - 1;
+      for (; i > i_tail && !in_mid(i); i--) {
+        const size_t hh = (size_t)1 << (i - 1);
+        RoundLink lk{sc.ctl + (n - 1 - i), link_for(i - 1), ch->down_dev, d0 + (n - i)};
+        const Publish pub{ch->counter, ch->dev, p0 + (n - i)};
+        launch_bind(c, n_half, hh, mk(0, 0), sc.eq, gis_zero(point[i - 1]),
+                    sc.acc + 4 * (n - i), pub, lk, colmask, live, st_);
+      }
+      if (i > i_tail) launch_mid(c, n_half, n, i, i_tail + 1, point, sc, p0, d0, colmask, live, st_);
+      uint32_t mask = 0;
+      for (int k = 1; k <= i_tail; k++) mask |= (uint32_t)gis_zero(point[k - 1]) << (k - 1);
+      gkr_tail<<<1, kTailThreads, 0, st_>>>(c, n_half, i_tail, sc.eq, mask, ch->dev,
+                                            p0 + (n - i_tail), ch->down_dev,
+                                            d0 + (n - 1 - i_tail), colmask, live);
+      BZ_LAUNCH_CHECK();
+      tail = true;
+    }
     f128 eq_bound = mk(1, 0);
     for (int i = n - 1; i >= 0; i--) {
       unsigned long long *acc = sc.acc + 4 * (n - 1 - i);
       round_read(sc, acc, st_);
+      if (trace) {
+        const auto now = std::chrono::steady_clock::now();
+        fprintf(stderr, "[gkr] layer %d round %2d h %8zu %s %7.2f us\n", j, i, (size_t)1 << i,
+                i == n - 1 ? "top " : (queued && i < i_tail) ? "tail" : "bind",
+                std::chrono::duration<double, std::micro>(now - t_prev).count());
+        t_prev = now;
+      }
       f128 sb = mk(sc.host[0], sc.host[1]), si = mk(sc.host[2], sc.host[3]);
       f128 msg[2] = {gmul(eq_bound, sb), gmul(eq_bound, si)};
       ts.prover_message(msg, 32);
@@ -338,25 +713,15 @@ f128 gkr_prove(int s, const f128 *zeta, uint32_t grind_bits, Transcript &ts, Gkr
       next[i] = r;
       eq_bound = gmul(eq_bound, eq_factor(r, point[i]));
       const uint64_t rw[2] = {r.lo, r.hi};
-      if (!tail && ch && resident && (i == 0 || ((size_t)1 << (i - 1)) <= (size_t)kTailH)) {
-        uint32_t mask = 0;
-        for (int k = 1; k <= i; k++) mask |= (uint32_t)gis_zero(point[k - 1]) << (k - 1);
-        gkr_tail<<<1, kTailThreads, 0, st_>>>(c, n_half, i, sc.eq, mask, ch->dev, ch->next + 1,
-                                          ch->down_dev, ch->down_next + 1, colmask, live);
-        BZ_LAUNCH_CHECK();
-        tail = true;
-      }
-      if (tail) {
+      if (queued) {
         ch->send(rw, 2);
         ch->arm();
       } else if (i > 0) {
         size_t hh = (size_t)1 << (i - 1);
         const bool probed = probe.on("gkr_bind_sums");
         if (probed) probe.before(st_);
-        gkr_bind_sums<<<grid_for(hh), kThreads, 0, st_>>>(c, n_half, hh, r, sc.eq,
-                                                          gis_zero(point[i - 1]), acc + 4, arm(sc),
-                                                          colmask, live);
-        BZ_LAUNCH_CHECK();
+        launch_bind(c, n_half, hh, r, sc.eq, gis_zero(point[i - 1]), acc + 4, arm(sc), none,
+                    colmask, live, st_);
         // reads 8 child and 2 eq entries per thread, writes 4 and 1
         if (probed) {
           // live threads move 15 entries, padded ones the eq table's 3

@@ -8,6 +8,15 @@
 
 namespace bz {
 
+// The challenge of one bind round in device memory (flag 1: valid, 2: the
+// chain stopped), left by the kernel before it or relayed by block 0 of a
+// resident kernel; `done` counts the resident kernel's blocks through the round.
+struct RoundCtl {
+  unsigned long long r_lo, r_hi;
+  unsigned int flag, done;
+  unsigned long long pad;
+};
+
 struct GkrScratch {
   size_t capacity = 0;         // leaves the layer tables can hold: 2^(7+s)
   f128 *layer[8] = {nullptr};  // layer j holds 2^(7+s-j) nodes; layer 7 is the output
@@ -15,12 +24,17 @@ struct GkrScratch {
   f128 *eq_scratch = nullptr;
   f128 *pair = nullptr;               // 2 entries
   unsigned long long *acc = nullptr;  // 4 words per round
+  RoundCtl *ctl = nullptr;            // one per round of a layer
   uint64_t *host = nullptr;           // pinned, 4 words
   RoundChannel *channel = nullptr;    // mailbox for round results; null: copy + sync
   // Columns at or beyond live_cols hold no set bit (the padding of h), so
   // every node of theirs is one in every layer; the kernels skip their
   // products and add their known contribution. 0: every column is live.
   size_t live_cols = 0;
+  // Run the middle rounds of each layer in one cooperative kernel that stays
+  // resident across them (a lane proving alone); otherwise one queued launch
+  // per round.
+  bool resident_middle = false;
 };
 
 // Builds every layer from the packed columns (2^s F128, bit b of column c is

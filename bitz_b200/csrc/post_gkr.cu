@@ -303,6 +303,8 @@ int post_gkr_prove(const PostGkrArgs &a, Transcript &ts, PostGkrScratch &sc, cud
     const char *e = getenv("BITZ_RESIDENT_ROUNDS");
     return !(e && e[0] == '0');
   }();
+  // no other thread's device allocation while a round kernel waits for this one
+  ResidentScope gate(ch && resident);
   try {
   for (int k = 0; k < rounds; k++) {
     unsigned long long *ak = acc + 8 * (k + 1);

@@ -265,12 +265,14 @@ struct Workspace {
   uint64_t staged_serial = 0;  // the system whose statement these hold
   cudaEvent_t ev_cols = nullptr, ev_folds = nullptr;
   Workspace() {
+    AllocScope gate;
     BZ_CUDA(cudaMallocHost(&host_fp, 8 * sizeof(fp)));
     BZ_CUDA(cudaMallocHost(&host_acc, 512 * sizeof(uint64_t)));
     BZ_CUDA(cudaEventCreateWithFlags(&ev_cols, cudaEventDisableTiming));
     BZ_CUDA(cudaEventCreateWithFlags(&ev_folds, cudaEventDisableTiming));
   }
   ~Workspace() {
+    AllocScope gate(false);
     if (host_fp) cudaFreeHost(host_fp);
     if (host_acc) cudaFreeHost(host_acc);
     if (ev_cols) cudaEventDestroy(ev_cols);

@@ -455,6 +455,8 @@ void spartan_prove(const SpartanArgs &a, Transcript &ts, SpartanScratch &sc, cud
     return !(e && e[0] == '0');
   }();
   bool tail = false;  // a resident tail kernel runs the remaining rounds
+  // no other thread's device allocation while a tail kernel waits for this one
+  ResidentScope gate(ch && resident);
   auto send_r = [&](fp x) {
     const uint64_t w[2] = {x.lo, x.hi};
     ch->send(w, 2);
