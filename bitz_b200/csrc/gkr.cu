@@ -111,28 +111,71 @@ __device__ __forceinline__ void round_end(unsigned long long *acc, const Publish
   }
 }
 
+// A layer's start. The eq table over the n - 1 coordinates below the top one
+// is the product of two factor tables, lo over the first a coordinates and
+// hi over the other b: block 0 builds lo and clears the layer's round
+// accumulators, block 1 builds hi and clears the round controls; the top
+// sums kernel multiplies the factors out as it reads them. Each doubling
+// level multiplies every entry by the same coordinate z, through z's window
+// table once the level is wide enough to repay building it.
+__device__ void eq_factor_block(const Point &p, int first, int n, f128 *out, MulTable &T) {
+  if (threadIdx.x == 0) out[0] = mk(1, 0);
+  __syncthreads();
+  for (int i = 0; i < n; i++) {
+    const f128 z = p.c[first + i];
+    const int half = 1 << i;
+    const bool tab = half >= 64;  // uniform across the block
+    if (tab) mul_table_build(T, z);
+    for (int k = threadIdx.x; k < half; k += blockDim.x) {
+      const f128 par = out[k];
+      const f128 one = tab ? mul_table(T, par) : gmul(par, z);
+      out[k] = gadd(par, one);
+      out[k + half] = one;
+    }
+    __syncthreads();
+  }
+}
+
+__global__ void __launch_bounds__(kThreads) gkr_layer_setup(Point p, int a, int b, f128 *lo,
+                                                            f128 *hi, unsigned long long *acc,
+                                                            int acc_words, RoundCtl *ctl,
+                                                            int nctl) {
+  __shared__ MulTable T;
+  if (blockIdx.x == 0) {
+    for (int k = threadIdx.x; k < acc_words; k += blockDim.x) acc[k] = 0;
+    eq_factor_block(p, 0, a, lo, T);
+  } else {
+    for (int k = threadIdx.x; k < nctl; k += blockDim.x) ctl[k] = RoundCtl{0, 0, 0, 0, 0};
+    eq_factor_block(p, a, b, hi, T);
+  }
+}
+
 // Round i's sums (round_sums, lib.rs:164-216) before any bind: the top round.
+// Entry x of the eq table is lo[x mod 2^a] * hi[x >> a]; it is stored for the
+// bind rounds as it is formed.
 __global__ void gkr_top_sums(const f128 *__restrict__ c, size_t n_half, size_t h,
-                             const f128 *__restrict__ eq, int at_one, unsigned long long *acc,
+                             const f128 *__restrict__ lo, int a, const f128 *__restrict__ hi,
+                             f128 *__restrict__ eq, int at_one, unsigned long long *acc,
                              Publish pub, RoundLink lk, size_t colmask, size_t live) {
   const f128 *L = c, *R = c + n_half;
+  const size_t amask = ((size_t)1 << a) - 1;
   wide sb = wzero(), si = wzero();
   for (size_t x = blockIdx.x * (size_t)blockDim.x + threadIdx.x; x < h;
        x += (size_t)gridDim.x * blockDim.x) {
+    const f128 e = gmul(ld(lo + (x & amask)), ld(hi + (x >> a)));
+    st(eq + x, e);
     if (padded(x, colmask, live)) {
-      f128 e = ld(eq + x);
       sb.w0 ^= e.lo;
       sb.w1 ^= e.hi;
       continue;
     }
     f128 l0 = ld(L + x), l1 = ld(L + h + x), r0 = ld(R + x), r1 = ld(R + h + x);
-    f128 e = ld(eq + x);
     f128 lb = at_one ? l1 : l0, rb = at_one ? r1 : r0;
     wacc(sb, gmul_wide(gmul(e, lb), rb));
     wacc(si, gmul_wide(gmul(e, gadd(l1, l0)), gadd(r1, r0)));
   }
-  f128 a = greduce(sb), b = greduce(si);
-  uint64_t v[4] = {a.lo, a.hi, b.lo, b.hi};
+  f128 sa = greduce(sb), sbb = greduce(si);
+  uint64_t v[4] = {sa.lo, sa.hi, sbb.lo, sbb.hi};
   block_xor_atomic<4>(v, acc);
   round_end(acc, pub, lk);
 }
@@ -185,11 +228,11 @@ __global__ void gkr_bind_sums(f128 *__restrict__ c, size_t n_half, size_t h, f12
 // by r through the block's window table (2 per thread), then the
 // 2 * kMidTile products with e, then the 2 * kMidTile wide products. Same
 // values, same sums as gkr_bind_sums.
+constexpr int kTailH = 256;  // gkr_tail's first round binds at most 4 kTailH entries per half
 constexpr int kMidThreads = 256;
 constexpr int kMidTile = 128;
 constexpr size_t kMidMaxH = (size_t)1 << 15;  // larger rounds are issue bound: gkr_bind_sums
 static_assert(kMidThreads == 2 * kMidTile && kMidThreads == kThreads, "one product per thread");
-constexpr size_t kMidGrid = 128;  // blocks of a resident gkr_mid
 
 // Shared memory of one tile: the window table of r, the tile's bound
 // entries L[x], L[x+h], R[x], R[x+h], its eq entries and the products with e.
@@ -329,24 +372,59 @@ __device__ __forceinline__ bool relay_wait(const RoundCtl *cl, unsigned long lon
 }
 
 // The middle rounds of a layer (bind r_i for i = i_hi .. i_lo) in one
-// cooperative launch that stays resident: no launch between rounds, and the
-// round code stays in the instruction cache. Block 0 reads r_i from the
-// downbox (publication d0 + n - 1 - i) and relays it through ctl; every block
-// binds its tiles; the last block through the round posts the sums as
-// publication p0 + n - i. Round i - 1 reads what every block wrote in round
-// i, which is in L2 before the host can answer the post with r_{i-1}: each
-// thread fences its stores before its block counts itself done. All blocks
-// are resident together (cooperative launch), so the relay waits end; each is
-// bounded all the same.
+// cooperative launch that stays resident, with the layer's live entries in
+// shared memory from the first round to the last. Block b of kMidBlocks owns
+// the positions whose residue mod kMidPeriod lies in [b kMidRuns,
+// (b + 1) kMidRuns); slot m of the block is position
+// kMidPeriod (m / kMidRuns) + b kMidRuns + m % kMidRuns. Every h of these
+// rounds is a multiple of kMidPeriod, so positions y, y + h, y + 2h, y + 3h
+// belong to one block and sit at slots m, m + E, m + 2E, m + 3E (E = h /
+// kMidBlocks elements per block): each round binds slot m < 2E from slots m
+// and m + 2E in place and sums elements j < E from slots j and j + E. Blocks
+// share nothing but the challenge and the sums: block 0 reads r_i from the
+// downbox (publication d0 + n - 1 - i) and relays it through ctl; each block
+// adds its share of the sums into acc and the last one through the round
+// posts them as publication p0 + n - i. The entries the tail kernel reads are
+// written back at the end. All blocks are resident together (cooperative
+// launch), so the relay waits end; each is bounded all the same.
+constexpr int kMidBlocks = 128;
+constexpr int kMidRuns = 4;
+constexpr size_t kMidPeriod = (size_t)kMidBlocks * kMidRuns;
+static_assert(kMidPeriod <= 2 * (size_t)kTailH, "the tail starts below the middle rounds");
+
+__device__ __forceinline__ size_t mid_pos(size_t m) {
+  return kMidPeriod * (m / kMidRuns) + (size_t)blockIdx.x * kMidRuns + m % kMidRuns;
+}
+
+// Dynamic shared memory for e0 elements: L and R at slots < 2 e0 (lo) and
+// [2 e0, 4 e0) (hi), eq at slots < 2 e0, and the products with e.
+__host__ __device__ constexpr size_t mid_smem_bytes(size_t e0) { return 12 * e0 * sizeof(f128); }
+
 __global__ void __launch_bounds__(kMidThreads) gkr_mid(
     f128 *__restrict__ c, size_t n_half, int n, int i_hi, int i_lo, f128 *__restrict__ eq,
     unsigned long long at_one_mask, unsigned long long *acc_base, Mailbox *mb,
     unsigned long long p0, const Mailbox *down, unsigned long long d0, RoundCtl *ctl,
     size_t colmask, size_t live) {
-  __shared__ TileShared S;
+  extern __shared__ f128 dyn[];
+  __shared__ MulTable T;
   __shared__ unsigned long long rs[2];
   __shared__ int ok_s;
   const int t = threadIdx.x;
+  const size_t e0 = ((size_t)1 << (i_hi - 1)) / kMidBlocks;
+  f128 *SL = dyn, *SL1 = dyn + 2 * e0, *SR = dyn + 4 * e0, *SR1 = dyn + 6 * e0;
+  f128 *EQ = dyn + 8 * e0, *P = dyn + 10 * e0, *Q = dyn + 11 * e0;
+  f128 *L = c, *R = c + n_half;
+  {
+    const size_t h0 = (size_t)1 << (i_hi - 1);
+    for (size_t m = t; m < 2 * e0; m += kMidThreads) {
+      const size_t y = mid_pos(m);
+      SL[m] = ld(L + y);
+      SL1[m] = ld(L + y + 2 * h0);
+      SR[m] = ld(R + y);
+      SR1[m] = ld(R + y + 2 * h0);
+      EQ[m] = ld(eq + y);
+    }
+  }
   for (int i = i_hi; i >= i_lo; i--) {
     RoundCtl *cl = ctl + (n - 1 - i);
     if (t == 0) {
@@ -364,17 +442,58 @@ __global__ void __launch_bounds__(kMidThreads) gkr_mid(
     }
     __syncthreads();
     if (!ok_s) return;
-    mul_table_build(S.T, mk(rs[0], rs[1]));
-    const size_t h = (size_t)1 << (i - 1);
+    mul_table_build(T, mk(rs[0], rs[1]));
+    const size_t e = ((size_t)1 << (i - 1)) / kMidBlocks;
     const int at_one = (int)((at_one_mask >> (i - 1)) & 1);
+    // the upper half of the live slots: separate arrays in the first round,
+    // slots [2e, 4e) of the lower ones after it
+    const f128 *hl = i == i_hi ? SL1 : SL + 2 * e, *hr = i == i_hi ? SR1 : SR + 2 * e;
+    // level 1: the 2e slots of L and of R bound at r; the eq table summed down
+    for (size_t u = t; u < 4 * e; u += kMidThreads) {
+      const bool right = u >= 2 * e;
+      const size_t m = right ? u - 2 * e : u;
+      if (padded(mid_pos(m), colmask, live)) continue;  // stays one
+      f128 *lo = right ? SR : SL;
+      const f128 a0 = lo[m];
+      lo[m] = gadd(a0, mul_table(T, gadd((right ? hr : hl)[m], a0)));
+    }
+    for (size_t j = t; j < e; j += kMidThreads) EQ[j] = gadd(EQ[j], EQ[j + e]);
+    __syncthreads();
+    // level 2: P = e * L_b, Q = e * (L_1 + L_0) for the e elements
+    for (size_t u = t; u < 2 * e; u += kMidThreads) {
+      const size_t j = u >> 1;
+      const f128 ev = EQ[j];
+      if (padded(mid_pos(j), colmask, live)) {  // e * 1 and e * 0
+        if (u & 1)
+          Q[j] = mk(0, 0);
+        else
+          P[j] = ev;
+      } else if (u & 1) {
+        Q[j] = gmul(ev, gadd(SL[j + e], SL[j]));
+      } else {
+        P[j] = gmul(ev, at_one ? SL[j + e] : SL[j]);
+      }
+    }
+    __syncthreads();
+    // level 3: P * R_b into the first sum, Q * (R_1 + R_0) into the second
     wide acc_w = wzero();
-    for (size_t x0 = (size_t)blockIdx.x * kMidTile; x0 < h; x0 += (size_t)gridDim.x * kMidTile)
-      bind_tile(S, c, c + n_half, eq, h, x0, at_one, colmask, live, acc_w);
-    __threadfence();  // this thread's bound entries before the block counts itself done
+    for (size_t u = t; u < 2 * e; u += kMidThreads) {
+      const size_t j = u >> 1;
+      if (padded(mid_pos(j), colmask, live)) {  // P * 1 and Q * 0
+        if (!(u & 1)) {
+          acc_w.w0 ^= P[j].lo;
+          acc_w.w1 ^= P[j].hi;
+        }
+      } else if (u & 1) {
+        wacc(acc_w, gmul_wide(Q[j], gadd(SR[j + e], SR[j])));
+      } else {
+        wacc(acc_w, gmul_wide(P[j], at_one ? SR[j + e] : SR[j]));
+      }
+    }
     uint64_t v[4];
-    tile_words(acc_w, v);
+    tile_words(acc_w, v);  // kMidThreads is even: thread parity = u parity
     unsigned long long *acc = acc_base + 4 * (n - i);
-    block_xor_atomic<4>(v, acc);
+    block_xor_atomic<4>(v, acc);  // synchronises the block: P, Q, SL, SR free again
     if (t == 0) {
       __threadfence();
       const unsigned int prev = atomicAdd(&cl->done, 1u);
@@ -385,6 +504,14 @@ __global__ void __launch_bounds__(kMidThreads) gkr_mid(
       }
     }
   }
+  // the live entries after round i_lo: L and R below 2 h, eq below h
+  const size_t e = ((size_t)1 << (i_lo - 1)) / kMidBlocks;
+  for (size_t m = t; m < 2 * e; m += kMidThreads) {
+    const size_t y = mid_pos(m);
+    st(L + y, SL[m]);
+    st(R + y, SR[m]);
+  }
+  for (size_t j = t; j < e; j += kMidThreads) st(eq + mid_pos(j), EQ[j]);
 }
 
 // The bind after round 0: one pair left in each half. Delivered through the
@@ -420,7 +547,6 @@ __global__ void gkr_final_bind(const f128 *__restrict__ c, size_t n_half, f128 r
 // block idle behind that chain, so the round is spread by product instead:
 // the 4h binds (and the eq update) across the block, then the 2h products
 // with e, then the 2h wide products, each level one product per thread.
-constexpr int kTailH = 256;
 constexpr int kTailThreads = 512;
 constexpr unsigned long long kTailWaitNs = 2000000000ull;  // 2 s per challenge
 
@@ -584,21 +710,26 @@ static void launch_bind(f128 *c, size_t n_half, size_t hh, f128 r, f128 *eq, int
   BZ_LAUNCH_CHECK();
 }
 
-// gkr_mid over bind rounds i_hi .. i_lo, as a cooperative launch: one block
-// per tile of the first round, at most as many as stay resident together.
+// gkr_mid over bind rounds i_hi .. i_lo as a cooperative launch of
+// kMidBlocks blocks (every block must be resident together).
 static void launch_mid(f128 *c, size_t n_half, int n, int i_hi, int i_lo, const f128 *point,
                        GkrScratch &sc, unsigned long long p0, unsigned long long d0,
                        size_t colmask, size_t live, cudaStream_t st) {
+  const size_t e0 = ((size_t)1 << (i_hi - 1)) / kMidBlocks;
+  const size_t smem = mid_smem_bytes(e0);
   static const int capacity = [] {
     int dev = 0, sms = 0, per_sm = 0;
     BZ_CUDA(cudaGetDevice(&dev));
     BZ_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-    BZ_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, gkr_mid, kMidThreads, 0));
+    BZ_CUDA(cudaFuncSetAttribute(gkr_mid, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)mid_smem_bytes(kMidMaxH / kMidBlocks)));
+    BZ_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, gkr_mid, kMidThreads,
+                                                          mid_smem_bytes(kMidMaxH / kMidBlocks)));
     return sms * per_sm;
   }();
-  const size_t tiles = (((size_t)1 << (i_hi - 1)) + kMidTile - 1) / kMidTile;
-  const int grid = (int)std::min<size_t>(std::min<size_t>(tiles, kMidGrid), (size_t)capacity);
-  if (grid < 1) throw CudaError("gkr_mid: no resident block fits");
+  if (capacity < kMidBlocks) throw CudaError("gkr_mid: the blocks do not fit resident together");
+  if (((size_t)1 << (i_lo - 1)) < kMidPeriod || ((size_t)1 << (i_hi - 1)) > kMidMaxH)
+    throw CudaError("gkr_mid: round sizes outside the resident range");
   unsigned long long mask = 0;
   for (int i = i_lo; i <= i_hi; i++) mask |= (unsigned long long)gis_zero(point[i - 1]) << (i - 1);
   RoundChannel *ch = sc.channel;
@@ -607,10 +738,10 @@ static void launch_mid(f128 *c, size_t n_half, int n, int i_hi, int i_lo, const 
   Mailbox *mb = ch->dev;
   const Mailbox *down = ch->down_dev;
   RoundCtl *ctl = sc.ctl;
-  void *args[] = {&c,   &n_half, &n,  &i_hi, &i_lo, &eq,  &mask,    &acc,
-                  &mb,  &p0,     &down, &d0,  &ctl,  &colmask, &live};
-  BZ_CUDA(cudaLaunchCooperativeKernel((const void *)gkr_mid, dim3(grid), dim3(kMidThreads), args,
-                                      0, st));
+  void *args[] = {&c,  &n_half, &n,    &i_hi, &i_lo, &eq,      &mask,  &acc,
+                  &mb, &p0,     &down, &d0,   &ctl,  &colmask, &live};
+  BZ_CUDA(cudaLaunchCooperativeKernel((const void *)gkr_mid, dim3(kMidBlocks),
+                                      dim3(kMidThreads), args, smem, st));
   BZ_LAUNCH_CHECK();
 }
 
@@ -642,9 +773,19 @@ f128 gkr_prove(int s, const f128 *zeta, uint32_t grind_bits, Transcript &ts, Gkr
     f128 *c = sc.layer[j];
     size_t n_half = (size_t)1 << n;
     int rounds = n;
-    BZ_CUDA(cudaMemsetAsync(sc.acc, 0, sizeof(unsigned long long) * 4 * (rounds + 1), st_));
-    // eq over the coordinates below the top one: 2^(n-1) entries
-    eq_table_device(point, n - 1, sc.eq, sc.eq_scratch, st_);
+    // eq over the coordinates below the top one (2^(n-1) entries) as the
+    // factors over the lower a and the upper b of them; the accumulators and
+    // round controls of the layer cleared
+    const int a = (n - 1) / 2, b = (n - 1) - a;
+    f128 *lo = sc.eq_scratch, *hi = sc.eq_scratch + ((size_t)1 << a);
+    {
+      Point pt;
+      pt.n = n - 1;
+      for (int k = 0; k < n - 1; k++) pt.c[k] = point[k];
+      gkr_layer_setup<<<2, kThreads, 0, st_>>>(pt, a, b, lo, hi, sc.acc, 4 * (rounds + 1),
+                                               sc.ctl, rounds);
+      BZ_LAUNCH_CHECK();
+    }
     size_t h = n_half / 2;
     // Queued mode: the bind rounds above the tail's first (h <= kTailH) and
     // the tail itself are all queued behind the top sums, each round's
@@ -669,12 +810,10 @@ f128 gkr_prove(int s, const f128 *zeta, uint32_t grind_bits, Transcript &ts, Gkr
       return queued && i > i_tail && !in_mid(i) ? sc.ctl + (n - 1 - i) : nullptr;
     };
     RoundLink top_link = none;
-    if (queued && n - 1 > i_tail) {
-      BZ_CUDA(cudaMemsetAsync(sc.ctl, 0, sizeof(RoundCtl) * rounds, st_));
-      top_link = RoundLink{nullptr, link_for(n - 1), ch->down_dev, d0};
-    }
-    gkr_top_sums<<<grid_for(h), kThreads, 0, st_>>>(c, n_half, h, sc.eq, gis_zero(point[n - 1]),
-                                                    sc.acc, top, top_link, colmask, live);
+    if (queued && n - 1 > i_tail) top_link = RoundLink{nullptr, link_for(n - 1), ch->down_dev, d0};
+    gkr_top_sums<<<grid_for(h), kThreads, 0, st_>>>(c, n_half, h, lo, a, hi, sc.eq,
+                                                    gis_zero(point[n - 1]), sc.acc, top, top_link,
+                                                    colmask, live);
     BZ_LAUNCH_CHECK();
     if (queued) {
       int i = n - 1;
