@@ -106,6 +106,8 @@ class Context {
 
   cudaStream_t stream() const { return stream_; }
   RoundChannel *channel() { return &channel_; }
+  // The lane's round controls (kMaxPointGkr entries), used by one phase at a time.
+  RoundCtl *round_ctl() { return gk_ctl_.get(); }
   // Prover workspace slot, owned by the lane (created by the prover).
   std::shared_ptr<Workspace> workspace;
 

@@ -231,6 +231,32 @@ struct RoundChannel {
   void clear_down();
 };
 
+// Queued sumcheck rounds. With the host's challenges delivered to the
+// device, the rounds of a sumcheck can all be queued at its start, so no
+// round waits for a launch from the host: the last block of each round
+// kernel posts the round's message, then waits (bounded) for the next
+// challenge in the lane's downbox and leaves it in `out` for the next kernel
+// in the stream, which reads it from `in`. Only that one block waits; the
+// next kernel starts when it has left. A missing challenge (time limit or
+// the host's abort marker) leaves flag 2, and every later kernel of the chain
+// passes it on and does no work.
+//
+// RoundCtl: one challenge in device memory (flag 1: valid, 2: the chain
+// stopped); `done` counts the blocks of a resident kernel through a round.
+struct RoundCtl {
+  unsigned long long r_lo, r_hi;
+  unsigned int flag, done;
+  unsigned long long pad;
+};
+
+struct RoundLink {
+  const RoundCtl *in;       // this round's challenge; null: the launch argument
+  RoundCtl *out;            // the next challenge; null: no wait
+  const Mailbox *down;      // the host's downbox
+  unsigned long long dseq;  // the host's publication of the next challenge
+};
+constexpr unsigned long long kRoundWaitNs = 2000000000ull;  // 2 s per challenge
+
 // Kernels that wait for their lane's host thread, and calls that wait for the
 // whole device. Such a kernel must never be in flight while another thread
 // is inside cudaFree, cudaFreeHost, cudaMalloc, cudaMallocHost or
@@ -330,6 +356,35 @@ __device__ __forceinline__ bool mailbox_wait_device(const Mailbox *mb, unsigned 
     if (globaltimer_ns() - t0 > limit_ns) return false;
     __nanosleep(32);
   }
+}
+
+// Every thread calls it: the challenge words from lk.in (lk.in not null);
+// false when the chain has stopped, which block 0 passes on to lk.out.
+__device__ __forceinline__ bool link_begin(const RoundLink &lk, unsigned long long &w0,
+                                           unsigned long long &w1) {
+  __shared__ unsigned long long s[3];
+  if (threadIdx.x == 0) {
+    s[0] = lk.in->r_lo;
+    s[1] = lk.in->r_hi;
+    s[2] = lk.in->flag;
+  }
+  __syncthreads();
+  w0 = s[0];
+  w1 = s[1];
+  if (s[2] == 1) return true;
+  if (blockIdx.x == 0 && threadIdx.x == 0 && lk.out) lk.out->flag = 2;
+  return false;
+}
+
+// One thread of a round's last block, after its post: the next challenge
+// from the downbox into lk.out (nothing without lk.out).
+__device__ __forceinline__ void link_fetch(const RoundLink &lk) {
+  if (!lk.out) return;
+  unsigned long long w[2] = {0, 0};
+  const bool ok = mailbox_wait_device(lk.down, lk.dseq, 2, w, kRoundWaitNs);
+  lk.out->r_lo = w[0];
+  lk.out->r_hi = w[1];
+  lk.out->flag = ok ? 1u : 2u;
 }
 #endif
 

@@ -52,40 +52,20 @@ __global__ void gkr_parent(const f128 *__restrict__ child, size_t half, f128 *__
     st(out + k, padded(k, colmask, live) ? mk(1, 0) : gmul(ld(child + k), ld(child + half + k)));
 }
 
-// Queued rounds. With the host's challenges delivered to the device, every
-// bind round of a layer is queued at the layer's start, so no round waits for
-// a launch from the host: the last block of each round kernel posts the
-// round's sums, then waits (bounded) for the next challenge in the lane's
-// downbox and leaves it in `out` for the next kernel in the stream, which
-// reads it from `in`. Only that one block waits; the next kernel starts when
-// it has left. A missing challenge (time limit or the host's abort marker)
-// leaves flag 2, and every later kernel of the chain passes it on and does
-// no work.
-struct RoundLink {
-  const RoundCtl *in;       // this round's challenge; null: the launch argument
-  RoundCtl *out;            // the next challenge; null: no wait
-  const Mailbox *down;      // the host's downbox
-  unsigned long long dseq;  // the host's publication of the next challenge
-};
-constexpr unsigned long long kRoundWaitNs = 2000000000ull;  // 2 s per challenge
+// Queued rounds (the round link in device.cuh): every bind round of a layer
+// is queued at the layer's start, so no round waits for a launch from the
+// host.
 
 // Every thread calls it; false when the chain has stopped (the block returns).
 __device__ __forceinline__ bool round_begin(const RoundLink &lk, f128 r_arg, f128 &r) {
-  __shared__ unsigned long long s[3];
   if (!lk.in) {
     r = r_arg;
     return true;
   }
-  if (threadIdx.x == 0) {
-    s[0] = lk.in->r_lo;
-    s[1] = lk.in->r_hi;
-    s[2] = lk.in->flag;
-  }
-  __syncthreads();
-  r = mk(s[0], s[1]);
-  if (s[2] == 1) return true;
-  if (blockIdx.x == 0 && threadIdx.x == 0 && lk.out) lk.out->flag = 2;
-  return false;
+  unsigned long long w0, w1;
+  const bool ok = link_begin(lk, w0, w1);
+  r = mk(w0, w1);
+  return ok;
 }
 
 // publish<4>, then the last block fetches the next challenge for `out`.
@@ -100,13 +80,7 @@ __device__ __forceinline__ void round_end(unsigned long long *acc, const Publish
 #pragma unroll
       for (int k = 0; k < 4; k++) mailbox_post(p.mailbox, p.seq, k, atomicExch(acc + k, 0ull));
       *p.counter = 0;
-      if (lk.out) {
-        unsigned long long w[2] = {0, 0};
-        const bool ok = mailbox_wait_device(lk.down, lk.dseq, 2, w, kRoundWaitNs);
-        lk.out->r_lo = w[0];
-        lk.out->r_hi = w[1];
-        lk.out->flag = ok ? 1u : 2u;
-      }
+      link_fetch(lk);
     }
   }
 }
@@ -763,8 +737,8 @@ f128 gkr_prove(int s, const f128 *zeta, uint32_t grind_bits, Transcript &ts, Gkr
     const char *e = getenv("BITZ_RESIDENT_ROUNDS");
     return !(e && e[0] == '0');
   }();
-  // BITZ_GKR_TRACE=1 prints the host time between consecutive round results
-  static const bool trace = getenv("BITZ_GKR_TRACE") != nullptr;
+  // BITZ_ROUND_TRACE=1 prints the host time between consecutive round results
+  static const bool trace = getenv("BITZ_ROUND_TRACE") != nullptr;
   auto t_prev = std::chrono::steady_clock::now();
   // no other thread's device allocation while a round kernel waits for this one
   ResidentScope gate(ch && resident);

@@ -8,15 +8,6 @@
 
 namespace bz {
 
-// The challenge of one bind round in device memory (flag 1: valid, 2: the
-// chain stopped), left by the kernel before it or relayed by block 0 of a
-// resident kernel; `done` counts the resident kernel's blocks through the round.
-struct RoundCtl {
-  unsigned long long r_lo, r_hi;
-  unsigned int flag, done;
-  unsigned long long pad;
-};
-
 struct GkrScratch {
   size_t capacity = 0;         // leaves the layer tables can hold: 2^(7+s)
   f128 *layer[8] = {nullptr};  // layer j holds 2^(7+s-j) nodes; layer 7 is the output

@@ -739,6 +739,7 @@ int ProofSystem::prove_after_commit(cudaStream_t s, std::vector<uint8_t> &proof)
   sc.tab = W.sp_tab.get();
   sc.host = W.host_fp;
   sc.channel = ctx.channel();
+  sc.ctl = ctx.round_ctl();
   SpartanArgs sa;
   sa.ctx = fc;
   sa.q = q;

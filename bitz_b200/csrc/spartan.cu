@@ -10,6 +10,9 @@
 #include "device.cuh"
 #include "spartan.hpp"
 
+#include <chrono>
+#include <cstdio>
+
 namespace bz {
 
 __global__ void k_fp_eq_factor(FpPoint p, int first, int n, FpCtx c, fp *out) {
@@ -94,12 +97,70 @@ __device__ __forceinline__ void cubic(fp e0, fp e1, fp a0, fp a1, fp b0, fp b1, 
   acc[2] = fp_add(acc[2], fp_mul(ed, rq, c), c);
 }
 
+// The round's message from the blocks' partial sums (block_fp_sum<N> left
+// them at partial[block * N + k], written by thread 0): the last block to
+// arrive adds every block's partials (mod q, in any order) and posts the N
+// totals as words 2k (low half) and 2k + 1 (high half) of publication
+// p.seq, then fetches the next challenge for the round link. Every thread
+// calls it.
+template <int N>
+__device__ void fp_round_end(const fp *partial, const FpCtx &c, const Publish &p,
+                             const RoundLink &lk) {
+  static_assert(2 * N <= kMailboxWords, "mailbox too small");
+  __shared__ int last_s;
+  __shared__ fp red[N][kThreads / 32];
+  if (threadIdx.x == 0) {
+    __threadfence();
+    last_s = atomicAdd(p.counter, 1u) == gridDim.x - 1;
+  }
+  __syncthreads();
+  if (!last_s) return;
+  __threadfence();
+  fp v[N];
+#pragma unroll
+  for (int k = 0; k < N; k++) v[k] = fp_zero();
+  for (unsigned b = threadIdx.x; b < gridDim.x; b += blockDim.x)
+#pragma unroll
+    for (int k = 0; k < N; k++) {
+      const ulonglong2 w = __ldcg(reinterpret_cast<const ulonglong2 *>(partial + b * N + k));
+      v[k] = fp_add(v[k], fp{w.x, w.y}, c);
+    }
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+  for (int k = 0; k < N; k++) {
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) {
+      fp o;
+      o.lo = __shfl_xor_sync(0xffffffffu, v[k].lo, off);
+      o.hi = __shfl_xor_sync(0xffffffffu, v[k].hi, off);
+      v[k] = fp_add(v[k], o, c);
+    }
+    if (lane == 0) red[k][warp] = v[k];
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    for (int k = 0; k < N; k++) {
+      fp x = red[k][0];
+      for (int w = 1; w < (int)(blockDim.x >> 5); w++) x = fp_add(x, red[k][w], c);
+      mailbox_post(p.mailbox, p.seq, 2 * k, x.lo);
+      mailbox_post(p.mailbox, p.seq, 2 * k + 1, x.hi);
+    }
+    *p.counter = 0;
+    link_fetch(lk);
+  }
+}
+
 // One outer round. fold = 0: sums over the pairs of the tables as they are.
 // fold = 1: fold every table at r (output at half length) and sum over the
 // folded pairs. emit = 0 only folds (the last fold).
 __global__ void k_outer_round(const fp *E, const fp *A, const fp *B, const fp *C, fp *E2, fp *A2,
                               fp *B2, fp *C2, size_t n, int fold, int emit, fp r, FpCtx c,
-                              fp *partial) {
+                              fp *partial, Publish pub, RoundLink lk) {
+  if (lk.in) {
+    unsigned long long w0, w1;
+    if (!link_begin(lk, w0, w1)) return;
+    r = fp{w0, w1};
+  }
   fp acc[3] = {fp_zero(), fp_zero(), fp_zero()};
   size_t npairs = fold ? (n / 2 + 1) / 2 : n / 2;
   for (size_t j = blockIdx.x * (size_t)blockDim.x + threadIdx.x; j < npairs;
@@ -131,13 +192,22 @@ __global__ void k_outer_round(const fp *E, const fp *A, const fp *B, const fp *C
     }
     if (emit) cubic(e[0], e[1], a[0], a[1], b[0], b[1], cc[0], cc[1], c, acc);
   }
-  if (emit) block_fp_sum<3>(acc, c, partial);
+  if (emit) {
+    block_fp_sum<3>(acc, c, partial);
+    if (pub.counter) fp_round_end<3>(partial, c, pub, lk);
+  }
 }
 
 // One inner round over D and the assignment W. W is read from the packed h
 // bits while w_bits is set (round 0, and the input of round 1's fold).
 __global__ void k_inner_round(const fp *D, const fp *W, const uint32_t *hbits, int w_bits, fp *D2,
-                              fp *W2, size_t n, int fold, int emit, fp r, FpCtx c, fp *partial) {
+                              fp *W2, size_t n, int fold, int emit, fp r, FpCtx c, fp *partial,
+                              Publish pub, RoundLink lk) {
+  if (lk.in) {
+    unsigned long long w0, w1;
+    if (!link_begin(lk, w0, w1)) return;
+    r = fp{w0, w1};
+  }
   fp acc[2] = {fp_zero(), fp_zero()};
   size_t npairs = fold ? (n / 2 + 1) / 2 : n / 2;
   for (size_t j = blockIdx.x * (size_t)blockDim.x + threadIdx.x; j < npairs;
@@ -173,7 +243,10 @@ __global__ void k_inner_round(const fp *D, const fp *W, const uint32_t *hbits, i
       acc[1] = fp_add(acc[1], fp_mul(fp_sub(d[1], d[0], c), fp_sub(w[1], w[0], c), c), c);
     }
   }
-  if (emit) block_fp_sum<2>(acc, c, partial);
+  if (emit) {
+    block_fp_sum<2>(acc, c, partial);
+    if (pub.counter) fp_round_end<2>(partial, c, pub, lk);
+  }
 }
 
 // One block adds the per-block partials; the totals go to out and, when
@@ -461,8 +534,67 @@ void spartan_prove(const SpartanArgs &a, Transcript &ts, SpartanScratch &sc, cud
     const uint64_t w[2] = {x.lo, x.hi};
     ch->send(w, 2);
   };
+  // BITZ_ROUND_TRACE=1 prints the host time between consecutive round results
+  static const bool trace = getenv("BITZ_ROUND_TRACE") != nullptr;
+  auto t_prev = std::chrono::steady_clock::now();
+  auto trace_round = [&](const char *what, int round, bool queued_kernel) {
+    if (!trace) return;
+    const auto now = std::chrono::steady_clock::now();
+    fprintf(stderr, "[spartan] %s round %2d %s %7.2f us\n", what, round,
+            queued_kernel ? "grid" : "tail",
+            std::chrono::duration<double, std::micro>(now - t_prev).count());
+    t_prev = now;
+  };
   fp fin[3];
+  // Queued mode: every outer round is queued now, then the tail. Round k > 0
+  // folds at r_{k-1}, which the host posts as downbox publication d0 + k - 1
+  // and the round before fetches into ctl[k-1] (the tail reads its first
+  // challenge from the downbox itself); round k posts its message as
+  // publication p0 + k.
+  const bool queued = ch && resident && sc.ctl;
   try {
+  if (queued) {
+    int t0 = 0;  // the tail's first round: its table fits in shared memory
+    while (t0 < nr && (t0 == 0 ? R : R >> (t0 - 1)) > (size_t)kSpTailN) t0++;
+    const unsigned long long p0 = ch->next + 1, d0 = ch->down_next + 1;
+    fp *set[2][4] = {{E, A, B, C}, {E2, A2, B2, C2}};
+    for (int k = 0; k < t0; k++) {
+      const int fold = k > 0;
+      const size_t n = k == 0 ? R : R >> (k - 1);
+      fp *const *in = set[fold ? (k - 1) % 2 : 0];
+      fp *const *to = set[k % 2];
+      const size_t npairs = fold ? (n / 2 + 1) / 2 : n / 2;
+      RoundLink lk{fold ? sc.ctl + (k - 1) : nullptr, k + 1 < t0 ? sc.ctl + k : nullptr,
+                   ch->down_dev, d0 + k};
+      k_outer_round<<<grid_for(npairs), kThreads, 0, s>>>(
+          in[0], in[1], in[2], in[3], to[0], to[1], to[2], to[3], n, fold, 1, fp_zero(), c,
+          sc.partial, Publish{ch->counter, ch->dev, p0 + k}, lk);
+      BZ_LAUNCH_CHECK();
+    }
+    {
+      fp *const *cur = set[t0 > 0 ? (t0 - 1) % 2 : 0];
+      const size_t n = t0 == 0 ? R : R >> (t0 - 1);
+      sp_outer_tail<<<1, kThreads, 0, s>>>(cur[0], cur[1], cur[2], cur[3], (int)n, t0 > 0,
+                                           nr - t0, c, ch->dev, p0 + t0, ch->down_dev,
+                                           d0 + (t0 > 0 ? t0 - 1 : 0));
+      BZ_LAUNCH_CHECK();
+      tail = true;
+    }
+    for (int round = 0; round < nr; round++) {
+      if (round > 0) send_r(r);
+      ch->arm();
+      ch->wait(s, reinterpret_cast<uint64_t *>(sc.host), 6);
+      trace_round("outer", round, round < t0);
+      fp co[4];
+      r = round_message(ts, c, claim, sc.host, 4, a.q, co);
+      for (int i = 0; i < 4; i++) out.outer[4 * round + i] = co[i];
+      out.rx[round] = r;
+    }
+    // the tail's last publication: the single entries of A, B and C
+    send_r(r);
+    ch->arm();
+    ch->wait(s, reinterpret_cast<uint64_t *>(fin), 6);
+  } else {
   for (int round = 0; round < nr; round++) {
     int fold = round > 0;
     if (!tail && ch && resident && len <= (size_t)kSpTailN) {
@@ -482,7 +614,8 @@ void spartan_prove(const SpartanArgs &a, Transcript &ts, SpartanScratch &sc, cud
       size_t npairs = fold ? (len / 2 + 1) / 2 : len / 2;
       int g = grid_for(npairs);
       k_outer_round<<<g, kThreads, 0, s>>>(E, A, B, C, E2, A2, B2, C2, len, fold, 1, r, c,
-                                           sc.partial);
+                                           sc.partial, Publish{nullptr, nullptr, 0},
+                                           RoundLink{nullptr, nullptr, nullptr, 0});
       BZ_LAUNCH_CHECK();
       host_partial_sum(sc.partial, g, 3, sc.sums, sc.host, c, s, sc.channel);
       if (fold) {
@@ -505,12 +638,15 @@ void spartan_prove(const SpartanArgs &a, Transcript &ts, SpartanScratch &sc, cud
     ch->wait(s, reinterpret_cast<uint64_t *>(fin), 6);
   } else {
     // the last fold leaves one entry per table
-    k_outer_round<<<1, kThreads, 0, s>>>(E, A, B, C, E2, A2, B2, C2, len, 1, 0, r, c, sc.partial);
+    k_outer_round<<<1, kThreads, 0, s>>>(E, A, B, C, E2, A2, B2, C2, len, 1, 0, r, c, sc.partial,
+                                         Publish{nullptr, nullptr, 0},
+                                         RoundLink{nullptr, nullptr, nullptr, 0});
     BZ_LAUNCH_CHECK();
     BZ_CUDA(cudaMemcpyAsync(&fin[0], A2, sizeof(fp), cudaMemcpyDeviceToHost, s));
     BZ_CUDA(cudaMemcpyAsync(&fin[1], B2, sizeof(fp), cudaMemcpyDeviceToHost, s));
     BZ_CUDA(cudaMemcpyAsync(&fin[2], C2, sizeof(fp), cudaMemcpyDeviceToHost, s));
     BZ_CUDA(cudaStreamSynchronize(s));
+  }
   }
   } catch (...) {
     if (tail) {  // release the waiting kernel before the lane is reused
@@ -559,6 +695,50 @@ void spartan_prove(const SpartanArgs &a, Transcript &ts, SpartanScratch &sc, cud
   int w_bits = 1;
   fp dw[2];
   try {
+  if (queued) {
+    // as the outer rounds: round k > 0 folds at r_{k-1} (downbox publication
+    // d0 + k - 1, fetched into ctl[k-1] by round k - 1) and posts p0 + k; W
+    // comes from the packed bits of h until round 1 has folded them
+    int t0 = 0;
+    while (t0 < nc && (t0 == 0 ? Cn : Cn >> (t0 - 1)) > (size_t)kSpTailN) t0++;
+    const unsigned long long p0 = ch->next + 1, d0 = ch->down_next + 1;
+    fp *set[2][2] = {{D, W}, {D2, W2}};
+    for (int k = 0; k < t0; k++) {
+      const int fold = k > 0;
+      const size_t n = k == 0 ? Cn : Cn >> (k - 1);
+      fp *const *in = set[fold ? (k - 1) % 2 : 0];
+      fp *const *to = set[k % 2];
+      const size_t npairs = fold ? (n / 2 + 1) / 2 : n / 2;
+      RoundLink lk{fold ? sc.ctl + (k - 1) : nullptr, k + 1 < t0 ? sc.ctl + k : nullptr,
+                   ch->down_dev, d0 + k};
+      k_inner_round<<<grid_for(npairs), kThreads, 0, s>>>(
+          in[0], in[1], a.hbits, k <= 1 ? 1 : 0, to[0], to[1], n, fold, 1, fp_zero(), c,
+          sc.partial, Publish{ch->counter, ch->dev, p0 + k}, lk);
+      BZ_LAUNCH_CHECK();
+    }
+    {
+      fp *const *cur = set[t0 > 0 ? (t0 - 1) % 2 : 0];
+      const size_t n = t0 == 0 ? Cn : Cn >> (t0 - 1);
+      sp_inner_tail<<<1, kThreads, 0, s>>>(cur[0], cur[1], a.hbits, t0 <= 1 ? 1 : 0, (int)n,
+                                           t0 > 0, nc - t0, c, ch->dev, p0 + t0, ch->down_dev,
+                                           d0 + (t0 > 0 ? t0 - 1 : 0));
+      BZ_LAUNCH_CHECK();
+      tail = true;
+    }
+    for (int round = 0; round < nc; round++) {
+      if (round > 0) send_r(r);
+      ch->arm();
+      ch->wait(s, reinterpret_cast<uint64_t *>(sc.host), 4);
+      trace_round("inner", round, round < t0);
+      fp co[3];
+      r = round_message(ts, c, claim, sc.host, 3, a.q, co);
+      for (int i = 0; i < 3; i++) out.inner[3 * round + i] = co[i];
+      out.ry[round] = r;
+    }
+    send_r(r);
+    ch->arm();
+    ch->wait(s, reinterpret_cast<uint64_t *>(dw), 4);
+  } else {
   for (int round = 0; round < nc; round++) {
     int fold = round > 0;
     if (!tail && ch && resident && len <= (size_t)kSpTailN) {
@@ -579,7 +759,8 @@ void spartan_prove(const SpartanArgs &a, Transcript &ts, SpartanScratch &sc, cud
       size_t npairs = fold ? (len / 2 + 1) / 2 : len / 2;
       int g = grid_for(npairs);
       k_inner_round<<<g, kThreads, 0, s>>>(D, W, a.hbits, w_bits, D2, W2, len, fold, 1, r, c,
-                                           sc.partial);
+                                           sc.partial, Publish{nullptr, nullptr, 0},
+                                           RoundLink{nullptr, nullptr, nullptr, 0});
       BZ_LAUNCH_CHECK();
       host_partial_sum(sc.partial, g, 2, sc.sums, sc.host, c, s, sc.channel);
       if (fold) {
@@ -600,11 +781,13 @@ void spartan_prove(const SpartanArgs &a, Transcript &ts, SpartanScratch &sc, cud
     ch->wait(s, reinterpret_cast<uint64_t *>(dw), 4);
   } else {
     k_inner_round<<<1, kThreads, 0, s>>>(D, W, a.hbits, w_bits, D2, W2, len, 1, 0, r, c,
-                                         sc.partial);
+                                         sc.partial, Publish{nullptr, nullptr, 0},
+                                         RoundLink{nullptr, nullptr, nullptr, 0});
     BZ_LAUNCH_CHECK();
     BZ_CUDA(cudaMemcpyAsync(&dw[0], D2, sizeof(fp), cudaMemcpyDeviceToHost, s));
     BZ_CUDA(cudaMemcpyAsync(&dw[1], W2, sizeof(fp), cudaMemcpyDeviceToHost, s));
     BZ_CUDA(cudaStreamSynchronize(s));
+  }
   }
   } catch (...) {
     if (tail) {

@@ -42,6 +42,7 @@ struct SpartanScratch {
   fp *tab;         // coefficient table, ntab entries
   fp *host;        // pinned, 4 entries
   RoundChannel *channel = nullptr;  // mailbox for round results; null: copy + sync
+  RoundCtl *ctl = nullptr;          // the lane's round controls (queued rounds)
 };
 
 struct SpartanOut {
