@@ -299,10 +299,56 @@ __global__ void k_rs_level(f128 *__restrict__ cw, int k, int d, int t,
   }
 }
 
+// The whole encode of a codeword that fits one block's shared memory: the
+// spread, then every level of k_rs_level in place, one launch instead of
+// l + 1 (the Ligerito levels' codewords are 2^8 .. 2^13 entries).
+constexpr int kRsBlockThreads = 1024;
+constexpr size_t kRsBlockMax = (size_t)1 << 13;  // 128 KiB of shared memory
+__global__ void __launch_bounds__(kRsBlockThreads) k_rs_encode_block(const f128 *__restrict__ msg,
+                                                                     int k, int l, int d,
+                                                                     const f128 *__restrict__ wh,
+                                                                     f128 *__restrict__ cw) {
+  extern __shared__ f128 sm[];
+  const size_t total = (size_t)1 << (d + k);
+  const size_t mmask = ((size_t)1 << (l + k)) - 1;
+  for (size_t i = threadIdx.x; i < total; i += blockDim.x) sm[i] = ld(msg + (i & mmask));
+  __syncthreads();
+  const size_t cmask = ((size_t)1 << k) - 1;
+  for (int t = l - 1; t >= 0; t--) {
+    const size_t half = (size_t)1 << t;
+    for (size_t i = threadIdx.x; i < total / 2; i += blockDim.x) {
+      const size_t c = i & cmask, p = i >> k;
+      const size_t base = (p >> t) << (t + 1);
+      const size_t j = p & (half - 1);
+      f128 lam = mk(0, 0);
+      for (int sb = t + 1; sb < d; sb++)
+        if ((base >> sb) & 1) lam = gadd(lam, wh[t * kMaxRsDim + sb]);
+      const size_t iu = ((base + j) << k) + c, iw = ((base + half + j) << k) + c;
+      const f128 u = sm[iu], w = sm[iw];
+      const f128 u2 = gadd(u, gmul(lam, w));
+      sm[iu] = u2;
+      sm[iw] = gadd(u2, w);
+    }
+    __syncthreads();
+  }
+  for (size_t i = threadIdx.x; i < total; i += blockDim.x) st(cw + i, sm[i]);
+}
+
 void rs_encode(const f128 *msg, int log_n, int k, int rate, const f128 *wh, f128 *cw,
                cudaStream_t s) {
   int l = log_n - k, d = l + rate;
   size_t total = (size_t)1 << (d + k);
+  if (total <= kRsBlockMax) {
+    static const bool attr = [] {
+      BZ_CUDA(cudaFuncSetAttribute(k_rs_encode_block, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   (int)(kRsBlockMax * sizeof(f128))));
+      return true;
+    }();
+    (void)attr;
+    k_rs_encode_block<<<1, kRsBlockThreads, total * sizeof(f128), s>>>(msg, k, l, d, wh, cw);
+    BZ_LAUNCH_CHECK();
+    return;
+  }
   k_rs_spread<<<grid_for(total), kThreads, 0, s>>>(msg, k, l, d, cw);
   BZ_LAUNCH_CHECK();
   for (int t = l - 1; t >= 0; t--) {
@@ -356,6 +402,55 @@ void merkle_build(const f128 *cw, size_t rows, int k, uint32_t *nodes, cudaStrea
     k_merkle_parents<<<grid_for(lo), kThreads, 0, s>>>(nodes, lo, 2 * lo);
     BZ_LAUNCH_CHECK();
   }
+}
+
+// A small tree in one block: the leaves, then each level of parents after a
+// block barrier (the nodes stay in global memory, which the block's barrier
+// orders), and the root (node 1) posted as four mailbox words.
+constexpr int kMerkleBlockThreads = 512;
+__global__ void __launch_bounds__(kMerkleBlockThreads) k_merkle_block(
+    const f128 *__restrict__ cw, size_t rows, int k, uint32_t *nodes, Publish pub) {
+  const uint32_t IV[8] = {0x6A09E667, 0xBB67AE85, 0x3C6EF372, 0xA54FF53A,
+                          0x510E527F, 0x9B05688C, 0x1F83D9AB, 0x5BE0CD19};
+  const int nbytes = 16 << k;
+  const int nblk = (nbytes + 63) / 64;
+  for (size_t i = threadIdx.x; i < rows; i += blockDim.x) {
+    const uint32_t *p = reinterpret_cast<const uint32_t *>(cw + (i << k));
+    uint32_t cv[8];
+    for (int j = 0; j < 8; j++) cv[j] = IV[j];
+    for (int b = 0; b < nblk; b++) {
+      uint32_t m[16];
+      const int len = nbytes - 64 * b < 64 ? nbytes - 64 * b : 64;
+      for (int j = 0; j < 16; j++) m[j] = 4 * j < len ? p[16 * b + j] : 0;
+      const uint32_t fl =
+          (b == 0 ? B3_CHUNK_START : 0) | (b == nblk - 1 ? B3_CHUNK_END | B3_ROOT : 0);
+      b3_compress(cv, m, 0, (uint32_t)len, fl, cv);
+    }
+    for (int j = 0; j < 8; j++) nodes[8 * (rows + i) + j] = cv[j];
+  }
+  __syncthreads();
+  for (size_t lo = rows / 2; lo >= 1; lo /= 2) {
+    for (size_t i = lo + threadIdx.x; i < 2 * lo; i += blockDim.x) {
+      uint32_t m[16], cv[8];
+      for (int j = 0; j < 16; j++) m[j] = nodes[16 * i + j];
+      b3_compress(IV, m, 0, 64, B3_CHUNK_START | B3_CHUNK_END | B3_ROOT, cv);
+      for (int j = 0; j < 8; j++) nodes[8 * i + j] = cv[j];
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0 && pub.counter)
+    for (int w = 0; w < 4; w++)
+      mailbox_post(pub.mailbox, pub.seq, w,
+                   (unsigned long long)nodes[8 + 2 * w] |
+                       ((unsigned long long)nodes[8 + 2 * w + 1] << 32));
+}
+
+bool merkle_build_posted(const f128 *cw, size_t rows, int k, uint32_t *nodes, Publish pub,
+                         cudaStream_t s) {
+  if (rows > kMerkleBlockMaxRows || !pub.counter) return false;
+  k_merkle_block<<<1, kMerkleBlockThreads, 0, s>>>(cw, rows, k, nodes, pub);
+  BZ_LAUNCH_CHECK();
+  return true;
 }
 
 // ----------------------------------------------------- Ligerito query glue

@@ -26,6 +26,12 @@ void dot(const f128 *a, const f128 *b, size_t n, unsigned long long *acc, Publis
 void rs_encode(const f128 *msg, int log_n, int k, int rate, const f128 *wh, f128 *cw,
                cudaStream_t s);
 void merkle_build(const f128 *cw, size_t rows, int k, uint32_t *nodes, cudaStream_t s);
+// A small tree (at most kMerkleBlockMaxRows rows) in one launch that posts
+// the root (node 1, 32 bytes) as four mailbox words of publication pub; false
+// (nothing launched) when the tree is larger or there is no mailbox.
+constexpr size_t kMerkleBlockMaxRows = 4096;
+bool merkle_build_posted(const f128 *cw, size_t rows, int k, uint32_t *nodes, Publish pub,
+                         cudaStream_t s);
 void query_basis(const f128 *w, const f128 *scale, int nq, int l, f128 *basis, cudaStream_t s);
 // Per query (idx[q] < rows): the codeword row and its Merkle siblings, packed
 // as width + 2 * depth 16-byte units.

@@ -579,10 +579,17 @@ std::vector<uint8_t> ProofSystem::ligerito(cudaStream_t s, f128 target) {
       next_cw[flip].resize(nrows << N.k);
       next_nodes[flip].resize(16 * nrows);
       rs_encode(f, l, N.k, N.log_inv_rate, T.wh.get(), next_cw[flip].get(), s);
-      merkle_build(next_cw[flip].get(), nrows, N.k, next_nodes[flip].get(), s);
       f128 *root_h = W.pin_small.get(kPinSmall) + kPinLevelRoot;
-      BZ_CUDA(cudaMemcpyAsync(root_h, next_nodes[flip].get() + 8, 32, cudaMemcpyDeviceToHost, s));
-      BZ_CUDA(cudaStreamSynchronize(s));
+      if (nrows <= kMerkleBlockMaxRows &&
+          merkle_build_posted(next_cw[flip].get(), nrows, N.k, next_nodes[flip].get(), ch->arm(),
+                              s)) {
+        ch->wait(s, reinterpret_cast<uint64_t *>(root_h), 4);
+      } else {
+        merkle_build(next_cw[flip].get(), nrows, N.k, next_nodes[flip].get(), s);
+        BZ_CUDA(cudaMemcpyAsync(root_h, next_nodes[flip].get() + 8, 32, cudaMemcpyDeviceToHost,
+                                s));
+        BZ_CUDA(cudaStreamSynchronize(s));
+      }
       uint8_t root[36];
       uint32_t len = 32;
       memcpy(root, &len, 4);
