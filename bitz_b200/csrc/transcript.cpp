@@ -1,6 +1,18 @@
 // Host transcript primitives: Keccak-f[1600], grinding and prime sampling.
 #include "transcript.hpp"
 
+#include <immintrin.h>
+
+#include <algorithm>
+#include <atomic>
+#include <condition_variable>
+#include <deque>
+#include <functional>
+#include <memory>
+#include <mutex>
+#include <thread>
+#include <vector>
+
 namespace bz {
 
 
@@ -90,8 +102,84 @@ static bool strong_round(const FpCtx &c, u128 q, u128 base) {
   return false;
 }
 
+// A few host threads for independent work items of one call (the
+// Miller-Rabin rounds of a candidate). The calling thread works on its own
+// job too, so a call finishes even when every pool thread is busy with
+// another lane's job; idle pool threads sleep on a condition variable.
+namespace {
+struct PoolJob {
+  const std::function<void(int)> *fn;
+  int n;
+  std::atomic<int> next{0}, done{0};
+};
+
+class HostPool {
+ public:
+  static HostPool &get() {
+    static HostPool *p = new HostPool();
+    return *p;
+  }
+  void run(int n, const std::function<void(int)> &fn) {
+    auto job = std::make_shared<PoolJob>();
+    job->fn = &fn;
+    job->n = n;
+    {
+      std::lock_guard<std::mutex> lk(mu_);
+      jobs_.push_back(job);
+    }
+    cv_.notify_all();
+    work(*job);
+    while (job->done.load(std::memory_order_acquire) < n) _mm_pause();
+  }
+
+ private:
+  HostPool() {
+    const unsigned hw = std::max(2u, std::thread::hardware_concurrency());
+    const unsigned nt = std::min(8u, hw - 1);
+    for (unsigned i = 0; i < nt; i++) std::thread([this] { loop(); }).detach();
+  }
+  static void work(PoolJob &j) {
+    for (;;) {
+      const int i = j.next.fetch_add(1);
+      if (i >= j.n) return;
+      (*j.fn)(i);
+      j.done.fetch_add(1, std::memory_order_release);
+    }
+  }
+  void loop() {
+    for (;;) {
+      std::shared_ptr<PoolJob> j;
+      {
+        std::unique_lock<std::mutex> lk(mu_);
+        cv_.wait(lk, [&] { return !jobs_.empty(); });
+        j = jobs_.front();
+        if (j->next.load() >= j->n) {  // handed out: drop it
+          jobs_.pop_front();
+          continue;
+        }
+      }
+      work(*j);
+    }
+  }
+  std::mutex mu_;
+  std::condition_variable cv_;
+  std::deque<std::shared_ptr<PoolJob>> jobs_;
+};
+}  // namespace
+
+// crates/transcript/src/challenge/prime.rs:33-61 with the strong test of
+// crates/field/src/helpers.rs:198-215: a candidate is the top bit, transcript
+// bits and the low bit; trial division by the primes to 41, then 80 rounds,
+// each on a base drawn from the transcript (rejection-sampled below q - 3)
+// and stopping at the first failure. The draws depend on the outcomes, so
+// they follow the reference exactly: once a candidate passes its first round
+// (almost surely a prime), the sponge state is saved, the other 79 bases are
+// drawn in order and their rounds run in parallel; if some round j failed,
+// the state goes back and exactly the bases up to j are drawn again, as the
+// sequential loop would have.
 u128 Transcript::prime(uint32_t bits) {
   static const int P[13] = {2, 3, 5, 7, 11, 13, 17, 19, 23, 29, 31, 37, 41};
+  constexpr int kRounds = 80;
   u128 bottom = (u128)1 << (bits - 1);
   for (;;) {
     u128 cand = bottom | (challenge_u128() & (bottom - 1)) | 1;
@@ -110,19 +198,40 @@ u128 Transcript::prime(uint32_t bits) {
       }
     }
     if (!decided) {
-      prime = true;
       FpCtx ctx = candidate_ctx(cand);
       u128 bound = cand - 3;
       u128 b = bound - 1;
       int lz = 0;
       while (lz < 128 && !((b >> (127 - lz)) & 1)) lz++;
       u128 mask = lz >= 128 ? 0 : (~(u128)0) >> lz;
-      for (int r = 0; r < 80 && prime; r++) {
+      auto draw = [&] {
         u128 c;
         do {
           c = challenge_u128() & mask;
         } while (c >= bound);
-        if (!strong_round(ctx, cand, 2 + c)) prime = false;
+        return c;
+      };
+      prime = strong_round(ctx, cand, 2 + draw());
+      if (prime) {
+        uint64_t st_saved[25];
+        memcpy(st_saved, st_, sizeof st_);
+        const int absorb_saved = absorb_pos_, squeeze_saved = squeeze_pos_;
+        std::vector<u128> base(kRounds);
+        for (int r = 1; r < kRounds; r++) base[r] = draw();
+        std::vector<char> pass(kRounds, 1);
+        HostPool::get().run(kRounds - 1, [&](int i) {
+          pass[i + 1] = strong_round(ctx, cand, 2 + base[i + 1]) ? 1 : 0;
+        });
+        int fail = 0;
+        for (int r = 1; r < kRounds && !fail; r++)
+          if (!pass[r]) fail = r;
+        if (fail) {
+          prime = false;
+          memcpy(st_, st_saved, sizeof st_);
+          absorb_pos_ = absorb_saved;
+          squeeze_pos_ = squeeze_saved;
+          for (int r = 1; r <= fail; r++) draw();
+        }
       }
     }
     if (prime) return cand;
