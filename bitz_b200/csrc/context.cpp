@@ -158,6 +158,7 @@ Context::Context() {
   BZ_CUDA(cudaMemset(counter_.get(), 0, sizeof(unsigned int)));
   channel_.counter = counter_.get();
   pg_.channel = &channel_;
+  pg_.ctl = gk_ctl_.get();
   gk_.channel = &channel_;
 }
 

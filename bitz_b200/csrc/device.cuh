@@ -386,6 +386,26 @@ __device__ __forceinline__ void link_fetch(const RoundLink &lk) {
   lk.out->r_hi = w[1];
   lk.out->flag = ok ? 1u : 2u;
 }
+
+// publish<N> (after the block's atomics), then the last block fetches the
+// next challenge for the round link.
+template <int N>
+__device__ __forceinline__ void publish_link(unsigned long long *acc, const Publish &p,
+                                             const RoundLink &lk) {
+  static_assert(N <= kMailboxWords, "mailbox too small");
+  if (!p.counter) return;
+  if (threadIdx.x == 0) {
+    __threadfence();
+    const unsigned int prev = atomicAdd(p.counter, 1u);
+    if (prev == gridDim.x - 1) {
+      __threadfence();
+#pragma unroll
+      for (int k = 0; k < N; k++) mailbox_post(p.mailbox, p.seq, k, atomicExch(acc + k, 0ull));
+      *p.counter = 0;
+      link_fetch(lk);
+    }
+  }
+}
 #endif
 
 #if defined(__CUDACC__)

@@ -71,18 +71,7 @@ __device__ __forceinline__ bool round_begin(const RoundLink &lk, f128 r_arg, f12
 // publish<4>, then the last block fetches the next challenge for `out`.
 __device__ __forceinline__ void round_end(unsigned long long *acc, const Publish &p,
                                           const RoundLink &lk) {
-  if (!p.counter) return;
-  if (threadIdx.x == 0) {
-    __threadfence();
-    const unsigned int prev = atomicAdd(p.counter, 1u);
-    if (prev == gridDim.x - 1) {
-      __threadfence();
-#pragma unroll
-      for (int k = 0; k < 4; k++) mailbox_post(p.mailbox, p.seq, k, atomicExch(acc + k, 0ull));
-      *p.counter = 0;
-      link_fetch(lk);
-    }
-  }
+  publish_link<4>(acc, p, lk);
 }
 
 // A layer's start. The eq table over the n - 1 coordinates below the top one
@@ -161,6 +150,8 @@ __global__ void gkr_bind_sums(f128 *__restrict__ c, size_t n_half, size_t h, f12
                               Publish pub, RoundLink lk, size_t colmask, size_t live) {
   f128 r;
   if (!round_begin(lk, r_arg, r)) return;
+  __shared__ MulTable T;  // the binds by r through r's window table
+  mul_table_build(T, r);
   f128 *L = c, *R = c + n_half;
   const size_t h2 = 2 * h;
   wide sb = wzero(), si = wzero();
@@ -174,11 +165,11 @@ __global__ void gkr_bind_sums(f128 *__restrict__ c, size_t n_half, size_t h, f12
       continue;
     }
     f128 a0 = ld(L + x), a1 = ld(L + x + h2), b0 = ld(L + x + h), b1 = ld(L + x + h + h2);
-    f128 l0 = gadd(a0, gmul(r, gadd(a1, a0)));
-    f128 l1 = gadd(b0, gmul(r, gadd(b1, b0)));
+    f128 l0 = gadd(a0, mul_table(T, gadd(a1, a0)));
+    f128 l1 = gadd(b0, mul_table(T, gadd(b1, b0)));
     f128 c0 = ld(R + x), c1 = ld(R + x + h2), d0 = ld(R + x + h), d1 = ld(R + x + h + h2);
-    f128 r0 = gadd(c0, gmul(r, gadd(c1, c0)));
-    f128 r1 = gadd(d0, gmul(r, gadd(d1, d0)));
+    f128 r0 = gadd(c0, mul_table(T, gadd(c1, c0)));
+    f128 r1 = gadd(d0, mul_table(T, gadd(d1, d0)));
     st(L + x, l0);
     st(L + x + h, l1);
     st(R + x, r0);
@@ -785,6 +776,7 @@ f128 gkr_prove(int s, const f128 *zeta, uint32_t grind_bits, Transcript &ts, Gkr
     };
     RoundLink top_link = none;
     if (queued && n - 1 > i_tail) top_link = RoundLink{nullptr, link_for(n - 1), ch->down_dev, d0};
+    if (queued) tail = true;  // from here a kernel of the lane may wait for this thread
     gkr_top_sums<<<grid_for(h), kThreads, 0, st_>>>(c, n_half, h, lo, a, hi, sc.eq,
                                                     gis_zero(point[n - 1]), sc.acc, top, top_link,
                                                     colmask, live);

@@ -74,9 +74,15 @@ __global__ void pg_first_message(const f128 *__restrict__ rows, int log_rows,
 __global__ void pg_first_fold(const f128 *__restrict__ rows, int log_rows,
                               const f128 *__restrict__ cols, const f128 *__restrict__ packed,
                               f128 r, f128 *__restrict__ w_out, f128 *__restrict__ v_out,
-                              size_t npairs_out, unsigned long long *acc, Publish pub) {
+                              size_t npairs_out, unsigned long long *acc, Publish pub,
+                              RoundLink lk) {
+  __shared__ MulTable T;  // products by r through r's window table
+  mul_table_build(T, r);
   const size_t half_rows = (size_t)1 << (log_rows - 1);
-  const f128 vals[4] = {mk(0, 0), mk(r.lo ^ 1, r.hi), r, mk(1, 0)};
+  // the bound bit pair (t = b0 + 2 b1) -> {0, 1 + r, r, 1}, by selects (no local array)
+  auto bound_pair = [&](int t) {
+    return t == 0 ? mk(0, 0) : t == 1 ? mk(r.lo ^ 1, r.hi) : t == 2 ? r : mk(1, 0);
+  };
   wide a0 = wzero(), a2 = wzero();
   for (size_t j = blockIdx.x * (size_t)blockDim.x + threadIdx.x; j < npairs_out;
        j += (size_t)gridDim.x * blockDim.x) {
@@ -85,13 +91,13 @@ __global__ void pg_first_fold(const f128 *__restrict__ rows, int log_rows,
     f128 col = ld(cols + c);
     f128 x0 = ld(rows + 2 * k), x1 = ld(rows + 2 * k + 1);
     f128 x2 = ld(rows + 2 * k + 2), x3 = ld(rows + 2 * k + 3);
-    f128 w0 = gmul(col, gadd(x0, gmul(r, gadd(x0, x1))));
-    f128 w1 = gmul(col, gadd(x2, gmul(r, gadd(x2, x3))));
+    f128 w0 = gmul(col, gadd(x0, mul_table(T, gadd(x0, x1))));
+    f128 w1 = gmul(col, gadd(x2, mul_table(T, gadd(x2, x3))));
     f128 word = ld(packed + (i0 >> 6));
     int p = (int)(i0 & 63);
     int t0 = bit128(word, 2 * p) | (bit128(word, 2 * p + 1) << 1);
     int t1 = bit128(word, 2 * p + 2) | (bit128(word, 2 * p + 3) << 1);
-    f128 v0 = vals[t0], v1 = vals[t1];
+    f128 v0 = bound_pair(t0), v1 = bound_pair(t1);
     st(w_out + i0, w0);
     st(w_out + i0 + 1, w1);
     st(v_out + i0, v0);
@@ -101,7 +107,8 @@ __global__ void pg_first_fold(const f128 *__restrict__ rows, int log_rows,
   }
   f128 r0 = greduce(a0), r2 = greduce(a2);
   uint64_t v[4] = {r0.lo, r0.hi, r2.lo, r2.hi};
-  block_xor_publish<4>(v, acc, pub);
+  block_xor_atomic<4>(v, acc);
+  publish_link<4>(acc, pub, lk);
 }
 
 // A quadratic round (sumcheck.rs:63-95,198-215): fold W and V at r (entry =
@@ -109,7 +116,14 @@ __global__ void pg_first_fold(const f128 *__restrict__ rows, int log_rows,
 // pairs. With emit == 0 only the fold runs (the last round).
 __global__ void pg_round(const f128 *__restrict__ w_in, const f128 *__restrict__ v_in, f128 r,
                          f128 *__restrict__ w_out, f128 *__restrict__ v_out, size_t nout,
-                         int emit, unsigned long long *acc, Publish pub) {
+                         int emit, unsigned long long *acc, Publish pub, RoundLink lk) {
+  if (lk.in) {  // a queued round: the challenge left by the kernel before
+    unsigned long long w0, w1;
+    if (!link_begin(lk, w0, w1)) return;
+    r = mk(w0, w1);
+  }
+  __shared__ MulTable T;  // products by r through r's window table
+  mul_table_build(T, r);
   wide a0 = wzero(), a2 = wzero();
   const size_t npairs = (nout + 1) / 2;
   for (size_t j = blockIdx.x * (size_t)blockDim.x + threadIdx.x; j < npairs;
@@ -117,15 +131,15 @@ __global__ void pg_round(const f128 *__restrict__ w_in, const f128 *__restrict__
     size_t o = 2 * j;
     f128 w0 = ld(w_in + 2 * o), w1 = ld(w_in + 2 * o + 1);
     f128 v0 = ld(v_in + 2 * o), v1 = ld(v_in + 2 * o + 1);
-    f128 fw0 = gadd(w0, gmul(r, gadd(w0, w1)));
-    f128 fv0 = gadd(v0, gmul(r, gadd(v0, v1)));
+    f128 fw0 = gadd(w0, mul_table(T, gadd(w0, w1)));
+    f128 fv0 = gadd(v0, mul_table(T, gadd(v0, v1)));
     st(w_out + o, fw0);
     st(v_out + o, fv0);
     if (o + 1 < nout) {
       f128 w2 = ld(w_in + 2 * o + 2), w3 = ld(w_in + 2 * o + 3);
       f128 v2 = ld(v_in + 2 * o + 2), v3 = ld(v_in + 2 * o + 3);
-      f128 fw1 = gadd(w2, gmul(r, gadd(w2, w3)));
-      f128 fv1 = gadd(v2, gmul(r, gadd(v2, v3)));
+      f128 fw1 = gadd(w2, mul_table(T, gadd(w2, w3)));
+      f128 fv1 = gadd(v2, mul_table(T, gadd(v2, v3)));
       st(w_out + o + 1, fw1);
       st(v_out + o + 1, fv1);
       if (emit) {
@@ -137,7 +151,8 @@ __global__ void pg_round(const f128 *__restrict__ w_in, const f128 *__restrict__
   if (emit) {
     f128 r0 = greduce(a0), r2 = greduce(a2);
     uint64_t v[4] = {r0.lo, r0.hi, r2.lo, r2.hi};
-    block_xor_publish<4>(v, acc, pub);
+    block_xor_atomic<4>(v, acc);
+    publish_link<4>(acc, pub, lk);
   }
 }
 
@@ -166,7 +181,8 @@ void quad_fold(const f128 *w, const f128 *v, f128 r, f128 *w2, f128 *v2, size_t 
                unsigned long long *acc, Publish pub, cudaStream_t s) {
   size_t nout = n / 2;
   pg_round<<<grid_for((nout + 1) / 2), kThreads, 0, s>>>(w, v, r, w2, v2, nout, emit && nout >= 2,
-                                                         acc, pub);
+                                                         acc, pub,
+                                                         RoundLink{nullptr, nullptr, nullptr, 0});
   BZ_LAUNCH_CHECK();
 }
 
@@ -287,15 +303,6 @@ int post_gkr_prove(const PostGkrArgs &a, Transcript &ts, PostGkrScratch &sc, cud
   // Round 1's fold fused with round 2's message.
   f128 *w = sc.w0, *v = sc.v0, *w2 = sc.w1, *v2 = sc.v1;
   const int rounds = m - 1;
-  {
-    unsigned long long *acc1 = acc + 8;
-    size_t npairs = n1 / 2;
-    if (rounds >= 1) {
-      pg_first_fold<<<grid_for(npairs), kThreads, 0, s>>>(a.rows, log_rows, a.cols, a.packed, r,
-                                                          w, v, npairs, acc1, arm(sc));
-      BZ_LAUNCH_CHECK();
-    }
-  }
   size_t len = n1;
   RoundChannel *ch = sc.channel;
   bool tail = false;  // pg_tail is resident and runs the remaining rounds
@@ -303,9 +310,64 @@ int post_gkr_prove(const PostGkrArgs &a, Transcript &ts, PostGkrScratch &sc, cud
     const char *e = getenv("BITZ_RESIDENT_ROUNDS");
     return !(e && e[0] == '0');
   }();
+  // Queued mode: the rounds above the tail are launched now behind the first
+  // fold, then the tail. Loop iteration k folds at r_k (point_out[1 + k]),
+  // which the host posts as downbox publication d0 + k; the kernel before
+  // the k-th queued fold fetches it into ctl[k] (the tail reads its first
+  // challenge itself), and the k-th fold posts publication p0 + k + 1.
+  const bool queued = ch && resident && sc.ctl && rounds >= 1;
+  int t0 = 0;  // the loop iteration at which the tail takes over
+  while (t0 < rounds && (n1 >> t0) > (size_t)2 * kPgTailN) t0++;
   // no other thread's device allocation while a round kernel waits for this one
   ResidentScope gate(ch && resident);
   try {
+  {
+    unsigned long long *acc1 = acc + 8;
+    size_t npairs = n1 / 2;
+    if (rounds >= 1) {
+      const unsigned long long d0 = queued ? ch->down_next + 1 : 0;
+      RoundLink lk{nullptr, queued && t0 > 0 ? sc.ctl : nullptr, queued ? ch->down_dev : nullptr,
+                   d0};
+      tail = queued;  // from here a kernel of the lane may wait for this thread
+      pg_first_fold<<<grid_for(npairs), kThreads, 0, s>>>(a.rows, log_rows, a.cols, a.packed, r,
+                                                          w, v, npairs, acc1, arm(sc), lk);
+      BZ_LAUNCH_CHECK();
+      if (queued) {
+        const unsigned long long p0 = ch->next;  // the first fold's publication
+        f128 *set[2][2] = {{sc.w0, sc.v0}, {sc.w1, sc.v1}};
+        for (int k = 0; k < t0; k++) {
+          const size_t nout = (n1 >> k) / 2;
+          f128 *const *in = set[k % 2];
+          f128 *const *to = set[(k + 1) % 2];
+          RoundLink lk2{sc.ctl + k, k + 1 < t0 ? sc.ctl + k + 1 : nullptr, ch->down_dev,
+                        d0 + k + 1};
+          pg_round<<<grid_for((nout + 1) / 2), kThreads, 0, s>>>(
+              in[0], in[1], mk(0, 0), to[0], to[1], nout, 1, acc + 8 * (k + 2),
+              Publish{ch->counter, ch->dev, p0 + k + 1}, lk2);
+          BZ_LAUNCH_CHECK();
+        }
+        f128 *const *cur = set[t0 % 2];
+        pg_tail<<<1, kThreads, 0, s>>>(cur[0], cur[1], (int)(n1 >> t0), ch->dev, p0 + t0 + 1,
+                                       ch->down_dev, d0 + t0);
+        BZ_LAUNCH_CHECK();
+      }
+    }
+  }
+  if (queued) {
+    for (int k = 0; k < rounds; k++) {
+      round_read(sc, nullptr, 4, s);
+      f128 m0 = mk(sc.host[0], sc.host[1]), m2 = mk(sc.host[2], sc.host[3]);
+      uint64_t mm[4] = {m0.lo, m0.hi, m2.lo, m2.hi};
+      ts.prover_message(mm, 32);
+      ts.grind("bitz/pcs/sumcheck/v1", a.grind_bits);
+      f128 rr = ts.challenge_f128();
+      claim = advance(claim, m0, m2, rr);
+      point_out[1 + k] = rr;
+      const uint64_t rw[2] = {rr.lo, rr.hi};
+      ch->send(rw, 2);
+      ch->arm();
+    }
+  } else {
   for (int k = 0; k < rounds; k++) {
     unsigned long long *ak = acc + 8 * (k + 1);
     round_read(sc, ak, 4, s);
@@ -333,7 +395,8 @@ int post_gkr_prove(const PostGkrArgs &a, Transcript &ts, PostGkrScratch &sc, cud
     int emit = nout >= 2;
     pg_round<<<grid_for((nout + 1) / 2), kThreads, 0, s>>>(w, v, rr, w2, v2, nout, emit,
                                                            acc + 8 * (k + 2),
-                                                           emit ? arm(sc) : Publish{nullptr, nullptr, 0});
+                                                           emit ? arm(sc) : Publish{nullptr, nullptr, 0},
+                                                           RoundLink{nullptr, nullptr, nullptr, 0});
     BZ_LAUNCH_CHECK();
     f128 *t = w;
     w = w2;
@@ -342,6 +405,7 @@ int post_gkr_prove(const PostGkrArgs &a, Transcript &ts, PostGkrScratch &sc, cud
     v = v2;
     v2 = t;
     len = nout;
+  }
   }
   } catch (...) {
     if (tail) {  // release the waiting kernel before the lane is reused

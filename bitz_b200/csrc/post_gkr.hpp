@@ -29,6 +29,7 @@ struct PostGkrScratch {
   uint64_t *host = nullptr;           // pinned, 8 words
   f128 claim_seen{0, 0};              // the weighted sum found when a claim fails
   RoundChannel *channel = nullptr;    // mailbox for round results; null: copy + sync
+  RoundCtl *ctl = nullptr;            // round controls for queued rounds; null: none
 };
 
 // The quadratic sumcheck round of <W, V> (shared with the Ligerito folds):

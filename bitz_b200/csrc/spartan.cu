@@ -557,6 +557,7 @@ void spartan_prove(const SpartanArgs &a, Transcript &ts, SpartanScratch &sc, cud
     int t0 = 0;  // the tail's first round: its table fits in shared memory
     while (t0 < nr && (t0 == 0 ? R : R >> (t0 - 1)) > (size_t)kSpTailN) t0++;
     const unsigned long long p0 = ch->next + 1, d0 = ch->down_next + 1;
+    tail = true;  // from here a kernel of the lane may wait for this thread
     fp *set[2][4] = {{E, A, B, C}, {E2, A2, B2, C2}};
     for (int k = 0; k < t0; k++) {
       const int fold = k > 0;
@@ -702,6 +703,7 @@ void spartan_prove(const SpartanArgs &a, Transcript &ts, SpartanScratch &sc, cud
     int t0 = 0;
     while (t0 < nc && (t0 == 0 ? Cn : Cn >> (t0 - 1)) > (size_t)kSpTailN) t0++;
     const unsigned long long p0 = ch->next + 1, d0 = ch->down_next + 1;
+    tail = true;  // from here a kernel of the lane may wait for this thread
     fp *set[2][2] = {{D, W}, {D2, W2}};
     for (int k = 0; k < t0; k++) {
       const int fold = k > 0;
