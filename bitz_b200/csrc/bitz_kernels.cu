@@ -151,22 +151,72 @@ __global__ void k_b3_parents(const uint32_t *__restrict__ in, size_t nout, Key8 
   }
 }
 
-// The non-root chaining value of a power-of-two number of whole chunks.
+// The last parent levels of a tree in one block: n chaining values (a power
+// of two, at most kB3BlockMax) reduced to one in shared memory, posted as
+// mailbox words 0-3, with the 16 bytes at `extra` (when given) as words 4-5.
+constexpr int kB3BlockThreads = 512;
+constexpr size_t kB3BlockMax = 1024;  // 2 x kB3BlockThreads: one compression per thread per level
+__global__ void __launch_bounds__(kB3BlockThreads) k_b3_top(const uint32_t *__restrict__ in,
+                                                            size_t n, Key8 key, uint32_t flags,
+                                                            const f128 *extra, Publish pub) {
+  __shared__ uint32_t cv[kB3BlockMax * 8];
+  for (size_t i = threadIdx.x; i < 8 * n; i += blockDim.x) cv[i] = in[i];
+  __syncthreads();
+  for (size_t m = n / 2; m >= 1; m /= 2) {
+    uint32_t out[8];
+    const bool mine = threadIdx.x < m;
+    if (mine) {
+      uint32_t msg[16];
+      for (int j = 0; j < 16; j++) msg[j] = cv[16 * threadIdx.x + j];
+      b3_compress(key.k, msg, 0, 64, flags | B3_PARENT, out);
+    }
+    __syncthreads();  // every read of this level before any write
+    if (mine)
+      for (int j = 0; j < 8; j++) cv[8 * threadIdx.x + j] = out[j];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    for (int w = 0; w < 4; w++)
+      mailbox_post(pub.mailbox, pub.seq, w,
+                   (unsigned long long)cv[2 * w] | ((unsigned long long)cv[2 * w + 1] << 32));
+    if (extra) {
+      const f128 e = ld(extra);
+      mailbox_post(pub.mailbox, pub.seq, 4, e.lo);
+      mailbox_post(pub.mailbox, pub.seq, 5, e.hi);
+    }
+  }
+}
+
+// The non-root chaining value of a power-of-two number of whole chunks. With
+// a channel, the last levels run in one block that posts the value (and the
+// 16 bytes at `extra`, returned in extra_out) through the lane's mailbox
+// instead of a copy and a stream synchronisation.
 void blake3_tree_cv(const uint8_t *data, size_t nchunks, const uint32_t key[8], uint32_t flags,
-                    uint32_t *scratch, uint32_t cv_out[8], cudaStream_t s) {
+                    uint32_t *scratch, uint32_t cv_out[8], cudaStream_t s, RoundChannel *ch,
+                    const f128 *extra, f128 *extra_out) {
   Key8 k;
   for (int i = 0; i < 8; i++) k.k[i] = key[i];
   uint32_t *a = scratch, *b = scratch + 8 * nchunks;
   k_b3_chunks<<<grid_for(nchunks), kThreads, 0, s>>>(data, nchunks, k, flags, a);
   BZ_LAUNCH_CHECK();
   size_t n = nchunks;
-  while (n > 1) {
+  while (n > 1 && (!ch || n > kB3BlockMax)) {
     k_b3_parents<<<grid_for(n / 2), kThreads, 0, s>>>(a, n / 2, k, flags, b);
     BZ_LAUNCH_CHECK();
     std::swap(a, b);
     n /= 2;
   }
+  if (ch) {
+    k_b3_top<<<1, kB3BlockThreads, 0, s>>>(a, n, k, flags, extra, ch->arm());
+    BZ_LAUNCH_CHECK();
+    uint64_t w[6];
+    ch->wait(s, w, extra ? 6 : 4);
+    memcpy(cv_out, w, 32);
+    if (extra) *extra_out = mk(w[4], w[5]);
+    return;
+  }
   BZ_CUDA(cudaMemcpyAsync(cv_out, a, 32, cudaMemcpyDeviceToHost, s));
+  if (extra) BZ_CUDA(cudaMemcpyAsync(extra_out, extra, 16, cudaMemcpyDeviceToHost, s));
   BZ_CUDA(cudaStreamSynchronize(s));
 }
 

@@ -13,8 +13,12 @@ void fold_columns(const f128 *cols, size_t ncols, const u128 *exps, u128 *folds,
 void comb_pow(const f128 *table, const u128 *exps, int n, f128 *out, cudaStream_t s);
 void mt_transpose(const uint32_t *off, const uint32_t *row, size_t ncols, const f128 *u1,
                   const f128 *u2, f128 *weights, size_t padded, f128 *w0, cudaStream_t s);
+// The non-root chaining value of nchunks (a power of two) whole 1 KiB chunks,
+// and the 16 bytes at `extra` (device, may be null) into extra_out. ch: the
+// lane's channel (null: a copy and a stream synchronisation).
 void blake3_tree_cv(const uint8_t *data, size_t nchunks, const uint32_t key[8], uint32_t flags,
-                    uint32_t *scratch, uint32_t cv_out[8], cudaStream_t s);
+                    uint32_t *scratch, uint32_t cv_out[8], cudaStream_t s, RoundChannel *ch,
+                    const f128 *extra, f128 *extra_out);
 void ring_claims(const f128 *f, const f128 *suffix, size_t n, unsigned long long *claims,
                  cudaStream_t s);
 void packed_basis(const f128 *suffix, size_t n, const f128 *bw, const f128 *eq_ood, f128 coef,

@@ -874,14 +874,14 @@ int ProofSystem::prove_after_commit(cudaStream_t s, std::vector<uint8_t> &proof)
   mt_transpose(dev_->csc_off.get(), dev_->csc_row.get(), S.f_bits + 1, W.u1.get(), W.u2.get(),
                W.weights.get(), nbits, W.w0.get(), s);
   f128 *w0_h = W.pin_small.get(kPinSmall) + kPinW0;
-  BZ_CUDA(cudaMemcpyAsync(w0_h, W.w0.get(), 16, cudaMemcpyDeviceToHost, s));
-  // the inner-product statement's weight digest (opening.rs:337-368)
+  // the inner-product statement's weight digest (opening.rs:337-368); the
+  // weight of column 0 comes back with it
   size_t nchunks = nbits * 16 / 1024;
   W.b3.resize(16 * nchunks);
   Blake3 dk = Blake3::derive_key("bitz/pcs/bit-inner-product-weights/v1");
   uint32_t left[8];
   blake3_tree_cv(reinterpret_cast<const uint8_t *>(W.weights.get()), nchunks, dk.key,
-                 B3_DERIVE_KEY_MATERIAL, W.b3.get(), left, s);
+                 B3_DERIVE_KEY_MATERIAL, W.b3.get(), left, s, ctx.channel(), W.w0.get(), w0_h);
   uint8_t digest[32];
   {
     // the column weight [1] is one more 16-byte chunk; the root joins the two
