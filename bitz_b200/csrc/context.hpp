@@ -108,6 +108,8 @@ class Context {
   RoundChannel *channel() { return &channel_; }
   // The lane's round controls (kMaxPointGkr entries), used by one phase at a time.
   RoundCtl *round_ctl() { return gk_ctl_.get(); }
+  // The lane proves alone: sumcheck middle rounds may run in resident kernels.
+  bool resident_middle() const { return gk_.resident_middle; }
   // Prover workspace slot, owned by the lane (created by the prover).
   std::shared_ptr<Workspace> workspace;
 

@@ -387,6 +387,59 @@ __device__ __forceinline__ void link_fetch(const RoundLink &lk) {
   lk.out->flag = ok ? 1u : 2u;
 }
 
+// Block 0's relay of a challenge to the other blocks of a resident kernel:
+// flag written last with release semantics, read with acquire (bounded).
+__device__ __forceinline__ void relay_post(RoundCtl *cl, const unsigned long long w[2], bool ok) {
+  cl->r_lo = w[0];
+  cl->r_hi = w[1];
+  asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(&cl->flag), "r"(ok ? 1u : 2u)
+               : "memory");
+}
+
+__device__ __forceinline__ bool relay_wait(const RoundCtl *cl, unsigned long long w[2]) {
+  const unsigned long long t0 = globaltimer_ns();
+  for (;;) {
+    unsigned int f;
+    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(f) : "l"(&cl->flag) : "memory");
+    if (f == 1) {
+      asm volatile("ld.relaxed.gpu.global.u64 %0, [%1];" : "=l"(w[0]) : "l"(&cl->r_lo) : "memory");
+      asm volatile("ld.relaxed.gpu.global.u64 %0, [%1];" : "=l"(w[1]) : "l"(&cl->r_hi) : "memory");
+      return true;
+    }
+    if (f == 2 || globaltimer_ns() - t0 > kRoundWaitNs) return false;
+    __nanosleep(64);
+  }
+}
+
+// Every thread of every block of a resident kernel calls it: block 0 waits
+// for host publication dseq in the downbox and relays it through cl; the
+// other blocks read the relay. The challenge words land in w (every thread);
+// false when it did not come (time limit or abort marker).
+__device__ __forceinline__ bool resident_challenge(const Mailbox *down, unsigned long long dseq,
+                                                   RoundCtl *cl, unsigned long long w[2]) {
+  __shared__ unsigned long long rs[2];
+  __shared__ int ok_s;
+  if (threadIdx.x == 0) {
+    unsigned long long v[2] = {0, 0};
+    bool ok;
+    if (blockIdx.x == 0) {
+      ok = mailbox_wait_device(down, dseq, 2, v, kRoundWaitNs);
+      relay_post(cl, v, ok);
+    } else {
+      ok = relay_wait(cl, v);
+    }
+    rs[0] = v[0];
+    rs[1] = v[1];
+    ok_s = ok;
+  }
+  __syncthreads();
+  w[0] = rs[0];
+  w[1] = rs[1];
+  const bool ok = ok_s;
+  __syncthreads();
+  return ok;
+}
+
 // publish<N> (after the block's atomics), then the last block fetches the
 // next challenge for the round link.
 template <int N>

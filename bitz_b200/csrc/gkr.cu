@@ -312,30 +312,6 @@ __global__ void __launch_bounds__(kMidThreads) gkr_round(
   round_end(acc, pub, lk);
 }
 
-// Block 0's relay of a challenge to the other blocks of a resident kernel:
-// flag written last with release semantics, read with acquire (bounded).
-__device__ __forceinline__ void relay_post(RoundCtl *cl, const unsigned long long w[2], bool ok) {
-  cl->r_lo = w[0];
-  cl->r_hi = w[1];
-  asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(&cl->flag), "r"(ok ? 1u : 2u)
-               : "memory");
-}
-
-__device__ __forceinline__ bool relay_wait(const RoundCtl *cl, unsigned long long w[2]) {
-  const unsigned long long t0 = globaltimer_ns();
-  for (;;) {
-    unsigned int f;
-    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(f) : "l"(&cl->flag) : "memory");
-    if (f == 1) {
-      asm volatile("ld.relaxed.gpu.global.u64 %0, [%1];" : "=l"(w[0]) : "l"(&cl->r_lo) : "memory");
-      asm volatile("ld.relaxed.gpu.global.u64 %0, [%1];" : "=l"(w[1]) : "l"(&cl->r_hi) : "memory");
-      return true;
-    }
-    if (f == 2 || globaltimer_ns() - t0 > kRoundWaitNs) return false;
-    __nanosleep(64);
-  }
-}
-
 // The middle rounds of a layer (bind r_i for i = i_hi .. i_lo) in one
 // cooperative launch that stays resident, with the layer's live entries in
 // shared memory from the first round to the last. Block b of kMidBlocks owns
@@ -372,8 +348,6 @@ __global__ void __launch_bounds__(kMidThreads) gkr_mid(
     size_t colmask, size_t live) {
   extern __shared__ f128 dyn[];
   __shared__ MulTable T;
-  __shared__ unsigned long long rs[2];
-  __shared__ int ok_s;
   const int t = threadIdx.x;
   const size_t e0 = ((size_t)1 << (i_hi - 1)) / kMidBlocks;
   f128 *SL = dyn, *SL1 = dyn + 2 * e0, *SR = dyn + 4 * e0, *SR1 = dyn + 6 * e0;
@@ -392,22 +366,9 @@ __global__ void __launch_bounds__(kMidThreads) gkr_mid(
   }
   for (int i = i_hi; i >= i_lo; i--) {
     RoundCtl *cl = ctl + (n - 1 - i);
-    if (t == 0) {
-      unsigned long long w[2] = {0, 0};
-      bool ok;
-      if (blockIdx.x == 0) {
-        ok = mailbox_wait_device(down, d0 + (n - 1 - i), 2, w, kRoundWaitNs);
-        relay_post(cl, w, ok);
-      } else {
-        ok = relay_wait(cl, w);
-      }
-      rs[0] = w[0];
-      rs[1] = w[1];
-      ok_s = ok;
-    }
-    __syncthreads();
-    if (!ok_s) return;
-    mul_table_build(T, mk(rs[0], rs[1]));
+    unsigned long long rw[2];
+    if (!resident_challenge(down, d0 + (n - 1 - i), cl, rw)) return;
+    mul_table_build(T, mk(rw[0], rw[1]));
     const size_t e = ((size_t)1 << (i - 1)) / kMidBlocks;
     const int at_one = (int)((at_one_mask >> (i - 1)) & 1);
     // the upper half of the live slots: separate arrays in the first round,

@@ -747,6 +747,7 @@ int ProofSystem::prove_after_commit(cudaStream_t s, std::vector<uint8_t> &proof)
   sc.host = W.host_fp;
   sc.channel = ctx.channel();
   sc.ctl = ctx.round_ctl();
+  sc.resident_middle = ctx.resident_middle();
   SpartanArgs sa;
   sa.ctx = fc;
   sa.q = q;

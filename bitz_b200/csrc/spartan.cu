@@ -99,22 +99,22 @@ __device__ __forceinline__ void cubic(fp e0, fp e1, fp a0, fp a1, fp b0, fp b1, 
 
 // The round's message from the blocks' partial sums (block_fp_sum<N> left
 // them at partial[block * N + k], written by thread 0): the last block to
-// arrive adds every block's partials (mod q, in any order) and posts the N
-// totals as words 2k (low half) and 2k + 1 (high half) of publication
-// p.seq, then fetches the next challenge for the round link. Every thread
-// calls it.
+// count itself in `counter` adds every block's partials (mod q, in any order)
+// and posts the N totals as words 2k (low half) and 2k + 1 (high half) of
+// publication seq. Every thread calls it; true in the last block (whose
+// threads are still together), false in the others.
 template <int N>
-__device__ void fp_round_end(const fp *partial, const FpCtx &c, const Publish &p,
-                             const RoundLink &lk) {
+__device__ bool fp_last_block_post(const fp *partial, const FpCtx &c, unsigned int *counter,
+                                   Mailbox *mb, unsigned long long seq) {
   static_assert(2 * N <= kMailboxWords, "mailbox too small");
   __shared__ int last_s;
   __shared__ fp red[N][kThreads / 32];
   if (threadIdx.x == 0) {
     __threadfence();
-    last_s = atomicAdd(p.counter, 1u) == gridDim.x - 1;
+    last_s = atomicAdd(counter, 1u) == gridDim.x - 1;
   }
   __syncthreads();
-  if (!last_s) return;
+  if (!last_s) return false;
   __threadfence();
   fp v[N];
 #pragma unroll
@@ -138,13 +138,23 @@ __device__ void fp_round_end(const fp *partial, const FpCtx &c, const Publish &p
     if (lane == 0) red[k][warp] = v[k];
   }
   __syncthreads();
-  if (threadIdx.x == 0) {
+  if (threadIdx.x == 0)
     for (int k = 0; k < N; k++) {
       fp x = red[k][0];
       for (int w = 1; w < (int)(blockDim.x >> 5); w++) x = fp_add(x, red[k][w], c);
-      mailbox_post(p.mailbox, p.seq, 2 * k, x.lo);
-      mailbox_post(p.mailbox, p.seq, 2 * k + 1, x.hi);
+      mailbox_post(mb, seq, 2 * k, x.lo);
+      mailbox_post(mb, seq, 2 * k + 1, x.hi);
     }
+  return true;
+}
+
+// fp_last_block_post through the lane's shared counter (reset by the last
+// block), then the last block fetches the next challenge for the round link.
+template <int N>
+__device__ void fp_round_end(const fp *partial, const FpCtx &c, const Publish &p,
+                             const RoundLink &lk) {
+  if (!fp_last_block_post<N>(partial, c, p.counter, p.mailbox, p.seq)) return;
+  if (threadIdx.x == 0) {
     *p.counter = 0;
     link_fetch(lk);
   }
@@ -501,6 +511,135 @@ static fp round_message(Transcript &ts, const FpCtx &c, fp &claim, const fp *wl,
   return r;
 }
 
+// The grid rounds k0 .. k1-1 of a sumcheck (outer: T = 4 tables E, A, B, C
+// and the cubic message, N = 3; inner: T = 2 tables D, W and N = 2) in one
+// cooperative launch that stays resident. Tables fold on their low
+// coordinate (pairs 2o, 2o + 1), so block b owns the contiguous chunk [b m,
+// (b + 1) m) of each input table (m = n_in / kSpMidBlocks) and, after each
+// fold, the first half of what it held: the chunk stays in the block's shared
+// memory from the first round to the last, and blocks share nothing but the
+// challenge (block 0 reads r_{k-1} from the downbox as publication
+// d0 + k - 1 and relays it through ctl[k - 1]) and the message (per-block
+// partial sums; the last block through round k, counted in ctl[k].done, adds
+// them and posts publication p0 + k). At the end each block writes its chunk
+// to `out` for the tail kernel. All blocks are resident together
+// (cooperative launch), so the relay waits end; each is bounded all the same.
+constexpr int kSpMidBlocks = 128;
+constexpr size_t kSpMidMaxChunk = 2048;  // entries per table per block
+struct SpTabs {
+  fp *t[4];
+};
+
+template <int T, int N>
+__global__ void __launch_bounds__(kThreads) sp_mid(SpTabs in, SpTabs out, size_t n_in, int k0,
+                                                   int k1, FpCtx c, fp *partial, Mailbox *mb,
+                                                   unsigned long long p0, const Mailbox *down,
+                                                   unsigned long long d0, RoundCtl *ctl) {
+  extern __shared__ fp chunk[];
+  const size_t m = n_in / gridDim.x;
+  fp *tab[T];
+#pragma unroll
+  for (int t = 0; t < T; t++) tab[t] = chunk + t * m;
+  const size_t base = (size_t)blockIdx.x * m;
+  for (size_t i = threadIdx.x; i < m; i += blockDim.x)
+#pragma unroll
+    for (int t = 0; t < T; t++) tab[t][i] = in.t[t][base + i];
+  __syncthreads();
+  size_t len = m;
+  for (int k = k0; k < k1; k++) {
+    if (k > 0) {
+      unsigned long long rw[2];
+      if (!resident_challenge(down, d0 + (k - 1), ctl + (k - 1), rw)) return;
+      const fp r = fp{rw[0], rw[1]};
+      // fold in place: every read of the level, then every write
+      constexpr int kPer = (int)(kSpMidMaxChunk / 2 / kThreads);
+      fp f[T][kPer];
+      const size_t nout = len / 2;
+#pragma unroll
+      for (int q = 0; q < kPer; q++) {
+        const size_t o = threadIdx.x + (size_t)q * kThreads;
+        if (o < nout)
+#pragma unroll
+          for (int t = 0; t < T; t++) f[t][q] = interp(tab[t][2 * o], tab[t][2 * o + 1], r, c);
+      }
+      __syncthreads();
+#pragma unroll
+      for (int q = 0; q < kPer; q++) {
+        const size_t o = threadIdx.x + (size_t)q * kThreads;
+        if (o < nout)
+#pragma unroll
+          for (int t = 0; t < T; t++) tab[t][o] = f[t][q];
+      }
+      __syncthreads();
+      len = nout;
+    }
+    fp acc[N];
+#pragma unroll
+    for (int q = 0; q < N; q++) acc[q] = fp_zero();
+    for (size_t j = threadIdx.x; j < len / 2; j += blockDim.x) {
+      if constexpr (T == 4) {
+        cubic(tab[0][2 * j], tab[0][2 * j + 1], tab[1][2 * j], tab[1][2 * j + 1], tab[2][2 * j],
+              tab[2][2 * j + 1], tab[3][2 * j], tab[3][2 * j + 1], c, acc);
+      } else {
+        const fp d0v = tab[0][2 * j], d1v = tab[0][2 * j + 1];
+        const fp w0v = tab[1][2 * j], w1v = tab[1][2 * j + 1];
+        acc[0] = fp_add(acc[0], fp_mul(d0v, w0v, c), c);
+        acc[1] = fp_add(acc[1], fp_mul(fp_sub(d1v, d0v, c), fp_sub(w1v, w0v, c), c), c);
+      }
+    }
+    block_fp_sum<N>(acc, c, partial);
+    fp_last_block_post<N>(partial, c, &ctl[k].done, mb, p0 + k);
+    __syncthreads();  // the chunk's reads of this round before the next fold
+  }
+  const size_t ob = (size_t)blockIdx.x * len;
+  for (size_t i = threadIdx.x; i < len; i += blockDim.x)
+#pragma unroll
+    for (int t = 0; t < T; t++) out.t[t][ob + i] = tab[t][i];
+}
+
+// sp_mid over rounds k0 .. k1-1 as a cooperative launch of kSpMidBlocks
+// blocks; n_in entries per input table.
+template <int T, int N>
+static void launch_sp_mid(const SpTabs &in, const SpTabs &out, size_t n_in, int k0, int k1,
+                          const FpCtx &c, const SpartanScratch &sc, unsigned long long p0,
+                          unsigned long long d0, cudaStream_t s) {
+  const size_t smem = T * (n_in / kSpMidBlocks) * sizeof(fp);
+  static const int capacity = [] {
+    int dev = 0, sms = 0, per_sm = 0;
+    const size_t most = T * kSpMidMaxChunk * sizeof(fp);
+    BZ_CUDA(cudaGetDevice(&dev));
+    BZ_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    BZ_CUDA(cudaFuncSetAttribute(sp_mid<T, N>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)most));
+    BZ_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, sp_mid<T, N>, kThreads, most));
+    return sms * per_sm;
+  }();
+  if (capacity < kSpMidBlocks) throw CudaError("sp_mid: the blocks do not fit resident together");
+  RoundChannel *ch = sc.channel;
+  SpTabs a = in, b = out;
+  FpCtx cc = c;
+  fp *partial = sc.partial;
+  Mailbox *mb = ch->dev;
+  const Mailbox *down = ch->down_dev;
+  RoundCtl *ctl = sc.ctl;
+  void *args[] = {&a, &b, &n_in, &k0, &k1, &cc, &partial, &mb, &p0, &down, &d0, &ctl};
+  BZ_CUDA(cudaLaunchCooperativeKernel((const void *)sp_mid<T, N>, dim3(kSpMidBlocks),
+                                      dim3(kThreads), args, smem, s));
+  BZ_LAUNCH_CHECK();
+}
+
+// The first round (>= kmin) from which sp_mid can run the rounds up to t0:
+// its input fits the blocks' chunks, and the last resident round still sums
+// whole pairs in every block. t0 when there is none.
+static int sp_mid_start(size_t n0, int kmin, int t0) {
+  for (int k = kmin; k < t0; k++) {
+    const size_t n_in = k == 0 ? n0 : n0 >> (k - 1);
+    const size_t last = (n0 >> (t0 - 1)) / kSpMidBlocks;  // per block after the last fold
+    if (n_in % kSpMidBlocks == 0 && n_in / kSpMidBlocks <= kSpMidMaxChunk && last >= 2) return k;
+  }
+  return t0;
+}
+
 void spartan_prove(const SpartanArgs &a, Transcript &ts, SpartanScratch &sc, cudaStream_t s,
                    SpartanOut &out) {
   const FpCtx &c = a.ctx;
@@ -559,21 +698,35 @@ void spartan_prove(const SpartanArgs &a, Transcript &ts, SpartanScratch &sc, cud
     const unsigned long long p0 = ch->next + 1, d0 = ch->down_next + 1;
     tail = true;  // from here a kernel of the lane may wait for this thread
     fp *set[2][4] = {{E, A, B, C}, {E2, A2, B2, C2}};
-    for (int k = 0; k < t0; k++) {
+    // rounds km .. t0-1 resident (sp_mid) when the lane proves alone and a
+    // round's input fits the blocks' shared memory; the rounds before them
+    // are queued launches
+    const int km = sc.resident_middle ? sp_mid_start(R, 0, t0) : t0;
+    BZ_CUDA(cudaMemsetAsync(sc.ctl, 0, sizeof(RoundCtl) * (nr + 1), s));
+    for (int k = 0; k < km; k++) {
       const int fold = k > 0;
       const size_t n = k == 0 ? R : R >> (k - 1);
       fp *const *in = set[fold ? (k - 1) % 2 : 0];
       fp *const *to = set[k % 2];
       const size_t npairs = fold ? (n / 2 + 1) / 2 : n / 2;
-      RoundLink lk{fold ? sc.ctl + (k - 1) : nullptr, k + 1 < t0 ? sc.ctl + k : nullptr,
+      RoundLink lk{fold ? sc.ctl + (k - 1) : nullptr, k + 1 < km ? sc.ctl + k : nullptr,
                    ch->down_dev, d0 + k};
       k_outer_round<<<grid_for(npairs), kThreads, 0, s>>>(
           in[0], in[1], in[2], in[3], to[0], to[1], to[2], to[3], n, fold, 1, fp_zero(), c,
           sc.partial, Publish{ch->counter, ch->dev, p0 + k}, lk);
       BZ_LAUNCH_CHECK();
     }
+    int cur_set = t0 > 0 ? (t0 - 1) % 2 : 0;
+    if (km < t0) {
+      const int si = km > 0 ? (km - 1) % 2 : 0;
+      const size_t n_in = km == 0 ? R : R >> (km - 1);
+      launch_sp_mid<4, 3>(SpTabs{{set[si][0], set[si][1], set[si][2], set[si][3]}},
+                          SpTabs{{set[1 - si][0], set[1 - si][1], set[1 - si][2], set[1 - si][3]}},
+                          n_in, km, t0, c, sc, p0, d0, s);
+      cur_set = 1 - si;
+    }
     {
-      fp *const *cur = set[t0 > 0 ? (t0 - 1) % 2 : 0];
+      fp *const *cur = set[cur_set];
       const size_t n = t0 == 0 ? R : R >> (t0 - 1);
       sp_outer_tail<<<1, kThreads, 0, s>>>(cur[0], cur[1], cur[2], cur[3], (int)n, t0 > 0,
                                            nr - t0, c, ch->dev, p0 + t0, ch->down_dev,
@@ -705,21 +858,33 @@ void spartan_prove(const SpartanArgs &a, Transcript &ts, SpartanScratch &sc, cud
     const unsigned long long p0 = ch->next + 1, d0 = ch->down_next + 1;
     tail = true;  // from here a kernel of the lane may wait for this thread
     fp *set[2][2] = {{D, W}, {D2, W2}};
-    for (int k = 0; k < t0; k++) {
+    // W is read from the packed bits of h through round 1: resident rounds
+    // start at 2 at the earliest
+    const int km = sc.resident_middle ? sp_mid_start(Cn, 2, t0) : t0;
+    BZ_CUDA(cudaMemsetAsync(sc.ctl, 0, sizeof(RoundCtl) * (nc + 1), s));
+    for (int k = 0; k < km; k++) {
       const int fold = k > 0;
       const size_t n = k == 0 ? Cn : Cn >> (k - 1);
       fp *const *in = set[fold ? (k - 1) % 2 : 0];
       fp *const *to = set[k % 2];
       const size_t npairs = fold ? (n / 2 + 1) / 2 : n / 2;
-      RoundLink lk{fold ? sc.ctl + (k - 1) : nullptr, k + 1 < t0 ? sc.ctl + k : nullptr,
+      RoundLink lk{fold ? sc.ctl + (k - 1) : nullptr, k + 1 < km ? sc.ctl + k : nullptr,
                    ch->down_dev, d0 + k};
       k_inner_round<<<grid_for(npairs), kThreads, 0, s>>>(
           in[0], in[1], a.hbits, k <= 1 ? 1 : 0, to[0], to[1], n, fold, 1, fp_zero(), c,
           sc.partial, Publish{ch->counter, ch->dev, p0 + k}, lk);
       BZ_LAUNCH_CHECK();
     }
+    int cur_set = t0 > 0 ? (t0 - 1) % 2 : 0;
+    if (km < t0) {
+      const int si = (km - 1) % 2;
+      launch_sp_mid<2, 2>(SpTabs{{set[si][0], set[si][1], nullptr, nullptr}},
+                          SpTabs{{set[1 - si][0], set[1 - si][1], nullptr, nullptr}},
+                          Cn >> (km - 1), km, t0, c, sc, p0, d0, s);
+      cur_set = 1 - si;
+    }
     {
-      fp *const *cur = set[t0 > 0 ? (t0 - 1) % 2 : 0];
+      fp *const *cur = set[cur_set];
       const size_t n = t0 == 0 ? Cn : Cn >> (t0 - 1);
       sp_inner_tail<<<1, kThreads, 0, s>>>(cur[0], cur[1], a.hbits, t0 <= 1 ? 1 : 0, (int)n,
                                            t0 > 0, nc - t0, c, ch->dev, p0 + t0, ch->down_dev,

@@ -43,6 +43,7 @@ struct SpartanScratch {
   fp *host;        // pinned, 4 entries
   RoundChannel *channel = nullptr;  // mailbox for round results; null: copy + sync
   RoundCtl *ctl = nullptr;          // the lane's round controls (queued rounds)
+  bool resident_middle = false;     // the grid rounds in one resident kernel (a lone lane)
 };
 
 struct SpartanOut {
