@@ -784,7 +784,8 @@ f128 gkr_prove(int s, const f128 *zeta, uint32_t grind_bits, Transcript &ts, Gkr
         ch->arm();
       } else if (i > 0) {
         size_t hh = (size_t)1 << (i - 1);
-        const bool probed = probe.on("gkr_bind_sums");
+        // the probe times gkr_bind_sums itself: the launches above kMidMaxH
+        const bool probed = probe.on("gkr_bind_sums") && hh > kMidMaxH;
         if (probed) probe.before(st_);
         launch_bind(c, n_half, hh, r, sc.eq, gis_zero(point[i - 1]), acc + 4, arm(sc), none,
                     colmask, live, st_);
