@@ -184,6 +184,7 @@ Context &Context::get() {
   static Context *ctx = [] {
     Context *c = new Context();
     c->gk_.resident_middle = true;
+    c->pg_.resident_middle = true;
     return c;
   }();
   return *ctx;

@@ -78,27 +78,7 @@ __device__ __forceinline__ void round_end(unsigned long long *acc, const Publish
 // is the product of two factor tables, lo over the first a coordinates and
 // hi over the other b: block 0 builds lo and clears the layer's round
 // accumulators, block 1 builds hi and clears the round controls; the top
-// sums kernel multiplies the factors out as it reads them. Each doubling
-// level multiplies every entry by the same coordinate z, through z's window
-// table once the level is wide enough to repay building it.
-__device__ void eq_factor_block(const Point &p, int first, int n, f128 *out, MulTable &T) {
-  if (threadIdx.x == 0) out[0] = mk(1, 0);
-  __syncthreads();
-  for (int i = 0; i < n; i++) {
-    const f128 z = p.c[first + i];
-    const int half = 1 << i;
-    const bool tab = half >= 64;  // uniform across the block
-    if (tab) mul_table_build(T, z);
-    for (int k = threadIdx.x; k < half; k += blockDim.x) {
-      const f128 par = out[k];
-      const f128 one = tab ? mul_table(T, par) : gmul(par, z);
-      out[k] = gadd(par, one);
-      out[k + half] = one;
-    }
-    __syncthreads();
-  }
-}
-
+// sums kernel multiplies the factors out as it reads them.
 __global__ void __launch_bounds__(kThreads) gkr_layer_setup(Point p, int a, int b, f128 *lo,
                                                             f128 *hi, unsigned long long *acc,
                                                             int acc_words, RoundCtl *ctl,

@@ -272,6 +272,132 @@ static void round_read(PostGkrScratch &sc, const unsigned long long *d_acc, int 
   BZ_CUDA(cudaStreamSynchronize(s));
 }
 
+// The post-GKR rounds km .. t0-1 in one cooperative launch that stays
+// resident (a lone lane). Tables fold on their low coordinate (pairs 2o,
+// 2o + 1), so block b owns the contiguous chunk [b m, (b + 1) m) of W and V
+// (m = n_in / kPgMidBlocks) and, after each fold, the first half of what it
+// held: the chunk stays in shared memory across rounds. Round k folds at r_k,
+// which block 0 reads from the downbox (publication d0 + k) and relays
+// through ctl[k]; each block XORs its share of the next message into
+// acc + 8 (k + 2) and the last block through the round (counted in
+// ctl[k].done) posts it as publication p0 + k + 1. At the end each block
+// writes its chunk to (w_out, v_out) for pg_tail. All blocks are resident
+// together (cooperative launch), so the relay waits end; each is bounded all
+// the same.
+constexpr int kPgMidBlocks = 128;
+constexpr size_t kPgMidMaxChunk = 2048;  // entries per table per block
+
+__global__ void __launch_bounds__(kThreads) pg_mid(const f128 *__restrict__ w_in,
+                                                   const f128 *__restrict__ v_in, size_t n_in,
+                                                   int km, int t0, f128 *__restrict__ w_out,
+                                                   f128 *__restrict__ v_out,
+                                                   unsigned long long *acc, Mailbox *mb,
+                                                   unsigned long long p0, const Mailbox *down,
+                                                   unsigned long long d0, RoundCtl *ctl) {
+  extern __shared__ f128 pgm[];
+  __shared__ MulTable T;
+  const size_t m = n_in / gridDim.x;
+  f128 *W = pgm, *V = pgm + m;
+  const size_t base = (size_t)blockIdx.x * m;
+  for (size_t i = threadIdx.x; i < m; i += blockDim.x) {
+    W[i] = ld(w_in + base + i);
+    V[i] = ld(v_in + base + i);
+  }
+  __syncthreads();
+  size_t len = m;
+  for (int k = km; k < t0; k++) {
+    unsigned long long rw[2];
+    if (!resident_challenge(down, d0 + k, ctl + k, rw)) return;
+    mul_table_build(T, mk(rw[0], rw[1]));
+    // fold in place: every read, then every write
+    constexpr int kPer = (int)(kPgMidMaxChunk / 2 / kThreads);
+    f128 fw[kPer], fv[kPer];
+    const size_t nout = len / 2;
+#pragma unroll
+    for (int q = 0; q < kPer; q++) {
+      const size_t o = threadIdx.x + (size_t)q * kThreads;
+      if (o < nout) {
+        const f128 w0 = W[2 * o], w1 = W[2 * o + 1], v0 = V[2 * o], v1 = V[2 * o + 1];
+        fw[q] = gadd(w0, mul_table(T, gadd(w0, w1)));
+        fv[q] = gadd(v0, mul_table(T, gadd(v0, v1)));
+      }
+    }
+    __syncthreads();
+#pragma unroll
+    for (int q = 0; q < kPer; q++) {
+      const size_t o = threadIdx.x + (size_t)q * kThreads;
+      if (o < nout) {
+        W[o] = fw[q];
+        V[o] = fv[q];
+      }
+    }
+    __syncthreads();
+    len = nout;
+    // the next message over the folded pairs
+    wide a0 = wzero(), a2 = wzero();
+    for (size_t j = threadIdx.x; j < len / 2; j += blockDim.x) {
+      const f128 w0 = W[2 * j], w1 = W[2 * j + 1], v0 = V[2 * j], v1 = V[2 * j + 1];
+      wacc(a0, gmul_wide(w0, v0));
+      wacc(a2, gmul_wide(gadd(w0, w1), gadd(v0, v1)));
+    }
+    const f128 r0 = greduce(a0), r2 = greduce(a2);
+    uint64_t v[4] = {r0.lo, r0.hi, r2.lo, r2.hi};
+    unsigned long long *ak = acc + 8 * (k + 2);
+    block_xor_atomic<4>(v, ak);
+    if (threadIdx.x == 0) {
+      __threadfence();
+      if (atomicAdd(&ctl[k].done, 1u) == gridDim.x - 1) {
+        __threadfence();
+#pragma unroll
+        for (int q = 0; q < 4; q++) mailbox_post(mb, p0 + k + 1, q, atomicExch(ak + q, 0ull));
+      }
+    }
+    __syncthreads();  // the chunk's reads of this round before the next fold
+  }
+  const size_t ob = (size_t)blockIdx.x * len;
+  for (size_t i = threadIdx.x; i < len; i += blockDim.x) {
+    st(w_out + ob + i, W[i]);
+    st(v_out + ob + i, V[i]);
+  }
+}
+
+// The first round pg_mid can start at: its input fits the blocks' chunks and
+// the last resident round still sums whole pairs in every block; t0 when
+// there is none.
+static int pg_mid_start(size_t n1, int t0) {
+  for (int k = 0; k < t0; k++) {
+    const size_t n_in = n1 >> k;
+    if (n_in % kPgMidBlocks == 0 && n_in / kPgMidBlocks <= kPgMidMaxChunk &&
+        (n1 >> t0) / kPgMidBlocks >= 2)
+      return k;
+  }
+  return t0;
+}
+
+static void launch_pg_mid(const f128 *w_in, const f128 *v_in, size_t n_in, int km, int t0,
+                          f128 *w_out, f128 *v_out, unsigned long long *acc, RoundChannel *ch,
+                          unsigned long long p0, unsigned long long d0, RoundCtl *ctl,
+                          cudaStream_t s) {
+  static const int capacity = [] {
+    int dev = 0, sms = 0, per_sm = 0;
+    const size_t most = 2 * kPgMidMaxChunk * sizeof(f128);
+    BZ_CUDA(cudaGetDevice(&dev));
+    BZ_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    BZ_CUDA(cudaFuncSetAttribute(pg_mid, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)most));
+    BZ_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, pg_mid, kThreads, most));
+    return sms * per_sm;
+  }();
+  if (capacity < kPgMidBlocks) throw CudaError("pg_mid: the blocks do not fit resident together");
+  const size_t smem = 2 * (n_in / kPgMidBlocks) * sizeof(f128);
+  Mailbox *mb = ch->dev;
+  const Mailbox *down = ch->down_dev;
+  void *args[] = {&w_in, &v_in, &n_in, &km, &t0, &w_out, &v_out,
+                  &acc, &mb,   &p0,   &down, &d0, &ctl};
+  BZ_CUDA(cudaLaunchCooperativeKernel((const void *)pg_mid, dim3(kPgMidBlocks), dim3(kThreads),
+                                      args, smem, s));
+  BZ_LAUNCH_CHECK();
+}
+
 int post_gkr_prove(const PostGkrArgs &a, Transcript &ts, PostGkrScratch &sc, cudaStream_t s,
                    f128 *point_out, f128 *value_out) {
   const int log_rows = a.log_rows, log_cols = a.log_cols;
@@ -326,7 +452,11 @@ int post_gkr_prove(const PostGkrArgs &a, Transcript &ts, PostGkrScratch &sc, cud
     size_t npairs = n1 / 2;
     if (rounds >= 1) {
       const unsigned long long d0 = queued ? ch->down_next + 1 : 0;
-      RoundLink lk{nullptr, queued && t0 > 0 ? sc.ctl : nullptr, queued ? ch->down_dev : nullptr,
+      // rounds km .. t0-1 resident (pg_mid) when the lane proves alone; the
+      // rounds before them are queued launches
+      const int km = queued && sc.resident_middle ? pg_mid_start(n1, t0) : t0;
+      if (queued) BZ_CUDA(cudaMemsetAsync(sc.ctl, 0, sizeof(RoundCtl) * (rounds + 1), s));
+      RoundLink lk{nullptr, queued && km > 0 ? sc.ctl : nullptr, queued ? ch->down_dev : nullptr,
                    d0};
       tail = queued;  // from here a kernel of the lane may wait for this thread
       pg_first_fold<<<grid_for(npairs), kThreads, 0, s>>>(a.rows, log_rows, a.cols, a.packed, r,
@@ -335,18 +465,25 @@ int post_gkr_prove(const PostGkrArgs &a, Transcript &ts, PostGkrScratch &sc, cud
       if (queued) {
         const unsigned long long p0 = ch->next;  // the first fold's publication
         f128 *set[2][2] = {{sc.w0, sc.v0}, {sc.w1, sc.v1}};
-        for (int k = 0; k < t0; k++) {
+        for (int k = 0; k < km; k++) {
           const size_t nout = (n1 >> k) / 2;
           f128 *const *in = set[k % 2];
           f128 *const *to = set[(k + 1) % 2];
-          RoundLink lk2{sc.ctl + k, k + 1 < t0 ? sc.ctl + k + 1 : nullptr, ch->down_dev,
+          RoundLink lk2{sc.ctl + k, k + 1 < km ? sc.ctl + k + 1 : nullptr, ch->down_dev,
                         d0 + k + 1};
           pg_round<<<grid_for((nout + 1) / 2), kThreads, 0, s>>>(
               in[0], in[1], mk(0, 0), to[0], to[1], nout, 1, acc + 8 * (k + 2),
               Publish{ch->counter, ch->dev, p0 + k + 1}, lk2);
           BZ_LAUNCH_CHECK();
         }
-        f128 *const *cur = set[t0 % 2];
+        int cur_set = t0 % 2;
+        if (km < t0) {
+          f128 *const *in = set[km % 2];
+          f128 *const *to = set[(km + 1) % 2];
+          launch_pg_mid(in[0], in[1], n1 >> km, km, t0, to[0], to[1], acc, ch, p0, d0, sc.ctl, s);
+          cur_set = (km + 1) % 2;
+        }
+        f128 *const *cur = set[cur_set];
         pg_tail<<<1, kThreads, 0, s>>>(cur[0], cur[1], (int)(n1 >> t0), ch->dev, p0 + t0 + 1,
                                        ch->down_dev, d0 + t0);
         BZ_LAUNCH_CHECK();

@@ -30,6 +30,7 @@ struct PostGkrScratch {
   f128 claim_seen{0, 0};              // the weighted sum found when a claim fails
   RoundChannel *channel = nullptr;    // mailbox for round results; null: copy + sync
   RoundCtl *ctl = nullptr;            // round controls for queued rounds; null: none
+  bool resident_middle = false;       // rounds above the tail in one resident kernel
 };
 
 // The quadratic sumcheck round of <W, V> (shared with the Ligerito folds):

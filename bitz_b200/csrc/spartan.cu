@@ -15,7 +15,11 @@
 
 namespace bz {
 
-__global__ void k_fp_eq_factor(FpPoint p, int first, int n, FpCtx c, fp *out) {
+// Both factor tables in one launch: block 0 the low a coordinates, block 1
+// the high b.
+__global__ void k_fp_eq_factor(FpPoint p, int a, int b, FpCtx c, fp *lo, fp *hi) {
+  const int first = blockIdx.x == 0 ? 0 : a, n = blockIdx.x == 0 ? a : b;
+  fp *out = blockIdx.x == 0 ? lo : hi;
   if (threadIdx.x == 0) out[0] = c.one;
   __syncthreads();
   for (int i = 0; i < n; i++) {
@@ -44,9 +48,7 @@ void fp_eq_table(const fp *point, int n, const FpCtx &c, fp *out, fp *scratch, c
   for (int i = 0; i < n; i++) p.c[i] = point[i];
   int a = n / 2, b = n - a;
   fp *lo = scratch, *hi = scratch + ((size_t)1 << a);
-  k_fp_eq_factor<<<1, kThreads, 0, s>>>(p, 0, a, c, lo);
-  BZ_LAUNCH_CHECK();
-  k_fp_eq_factor<<<1, kThreads, 0, s>>>(p, a, b, c, hi);
+  k_fp_eq_factor<<<2, kThreads, 0, s>>>(p, a, b, c, lo, hi);
   BZ_LAUNCH_CHECK();
   size_t total = (size_t)1 << n;
   k_fp_eq_expand<<<grid_for(total), kThreads, 0, s>>>(lo, a, hi, c, out, total);
