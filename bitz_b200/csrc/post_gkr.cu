@@ -279,8 +279,9 @@ static void round_read(PostGkrScratch &sc, const unsigned long long *d_acc, int 
 // held: the chunk stays in shared memory across rounds. Round k folds at r_k,
 // which block 0 reads from the downbox (publication d0 + k) and relays
 // through ctl[k]; each block XORs its share of the next message into
-// acc + 8 (k + 2) and the last block through the round (counted in
-// ctl[k].done) posts it as publication p0 + k + 1. At the end each block
+// acc + 8 (k + acc_off) and the last block through the round (counted in
+// ctl[k].done) posts it as publication p0 + k + 1 (the last round only with
+// emit_last; the Ligerito levels run their folds here too). At the end each block
 // writes its chunk to (w_out, v_out) for pg_tail. All blocks are resident
 // together (cooperative launch), so the relay waits end; each is bounded all
 // the same.
@@ -289,7 +290,8 @@ constexpr size_t kPgMidMaxChunk = 2048;  // entries per table per block
 
 __global__ void __launch_bounds__(kThreads) pg_mid(const f128 *__restrict__ w_in,
                                                    const f128 *__restrict__ v_in, size_t n_in,
-                                                   int km, int t0, f128 *__restrict__ w_out,
+                                                   int km, int t0, int emit_last, int acc_off,
+                                                   f128 *__restrict__ w_out,
                                                    f128 *__restrict__ v_out,
                                                    unsigned long long *acc, Mailbox *mb,
                                                    unsigned long long p0, const Mailbox *down,
@@ -333,6 +335,7 @@ __global__ void __launch_bounds__(kThreads) pg_mid(const f128 *__restrict__ w_in
     }
     __syncthreads();
     len = nout;
+    if (k + 1 == t0 && !emit_last) break;  // the last fold: no message after it
     // the next message over the folded pairs
     wide a0 = wzero(), a2 = wzero();
     for (size_t j = threadIdx.x; j < len / 2; j += blockDim.x) {
@@ -342,7 +345,7 @@ __global__ void __launch_bounds__(kThreads) pg_mid(const f128 *__restrict__ w_in
     }
     const f128 r0 = greduce(a0), r2 = greduce(a2);
     uint64_t v[4] = {r0.lo, r0.hi, r2.lo, r2.hi};
-    unsigned long long *ak = acc + 8 * (k + 2);
+    unsigned long long *ak = acc + 8 * (k + acc_off);
     block_xor_atomic<4>(v, ak);
     if (threadIdx.x == 0) {
       __threadfence();
@@ -364,7 +367,13 @@ __global__ void __launch_bounds__(kThreads) pg_mid(const f128 *__restrict__ w_in
 // The first round pg_mid can start at: its input fits the blocks' chunks and
 // the last resident round still sums whole pairs in every block; t0 when
 // there is none.
-static int pg_mid_start(size_t n1, int t0) {
+bool pg_mid_fits_folds(size_t n, int rounds) {
+  // a fold whose output is still summed needs two entries per block after it
+  return rounds >= 1 && n % kPgMidBlocks == 0 && n / kPgMidBlocks <= kPgMidMaxChunk &&
+         (rounds < 2 || (n >> (rounds - 1)) / kPgMidBlocks >= 2);
+}
+
+int pg_mid_start(size_t n1, int t0) {
   for (int k = 0; k < t0; k++) {
     const size_t n_in = n1 >> k;
     if (n_in % kPgMidBlocks == 0 && n_in / kPgMidBlocks <= kPgMidMaxChunk &&
@@ -374,10 +383,10 @@ static int pg_mid_start(size_t n1, int t0) {
   return t0;
 }
 
-static void launch_pg_mid(const f128 *w_in, const f128 *v_in, size_t n_in, int km, int t0,
-                          f128 *w_out, f128 *v_out, unsigned long long *acc, RoundChannel *ch,
-                          unsigned long long p0, unsigned long long d0, RoundCtl *ctl,
-                          cudaStream_t s) {
+void launch_pg_mid(const f128 *w_in, const f128 *v_in, size_t n_in, int km, int t0,
+                   int emit_last, int acc_off, f128 *w_out, f128 *v_out, unsigned long long *acc,
+                   RoundChannel *ch, unsigned long long p0, unsigned long long d0, RoundCtl *ctl,
+                   cudaStream_t s) {
   static const int capacity = [] {
     int dev = 0, sms = 0, per_sm = 0;
     const size_t most = 2 * kPgMidMaxChunk * sizeof(f128);
@@ -391,8 +400,8 @@ static void launch_pg_mid(const f128 *w_in, const f128 *v_in, size_t n_in, int k
   const size_t smem = 2 * (n_in / kPgMidBlocks) * sizeof(f128);
   Mailbox *mb = ch->dev;
   const Mailbox *down = ch->down_dev;
-  void *args[] = {&w_in, &v_in, &n_in, &km, &t0, &w_out, &v_out,
-                  &acc, &mb,   &p0,   &down, &d0, &ctl};
+  void *args[] = {&w_in, &v_in, &n_in, &km, &t0, &emit_last, &acc_off, &w_out,
+                  &v_out, &acc, &mb,   &p0,   &down, &d0, &ctl};
   BZ_CUDA(cudaLaunchCooperativeKernel((const void *)pg_mid, dim3(kPgMidBlocks), dim3(kThreads),
                                       args, smem, s));
   BZ_LAUNCH_CHECK();
@@ -480,7 +489,8 @@ int post_gkr_prove(const PostGkrArgs &a, Transcript &ts, PostGkrScratch &sc, cud
         if (km < t0) {
           f128 *const *in = set[km % 2];
           f128 *const *to = set[(km + 1) % 2];
-          launch_pg_mid(in[0], in[1], n1 >> km, km, t0, to[0], to[1], acc, ch, p0, d0, sc.ctl, s);
+          launch_pg_mid(in[0], in[1], n1 >> km, km, t0, 1, 2, to[0], to[1], acc, ch, p0, d0, sc.ctl,
+                        s);
           cur_set = (km + 1) % 2;
         }
         f128 *const *cur = set[cur_set];

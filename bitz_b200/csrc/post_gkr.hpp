@@ -33,6 +33,22 @@ struct PostGkrScratch {
   bool resident_middle = false;       // rounds above the tail in one resident kernel
 };
 
+// Folds k = km .. t0-1 of a quadratic sumcheck over <W, V> (n_in entries
+// each) in one resident cooperative launch (a lane that proves alone): fold
+// k takes its challenge from downbox publication d0 + k (relayed through
+// ctl[k], which must start zeroed), XORs the next message into
+// acc + 8 (k + acc_off) and posts it as publication p0 + k + 1 (the last fold
+// only with emit_last); the folded tables end in (w_out, v_out).
+// pg_mid_start gives the first fold it can take (t0 when none).
+int pg_mid_start(size_t n1, int t0);
+// All `rounds` folds of n-entry tables fit launch_pg_mid (the last without a
+// message).
+bool pg_mid_fits_folds(size_t n, int rounds);
+void launch_pg_mid(const f128 *w_in, const f128 *v_in, size_t n_in, int km, int t0,
+                   int emit_last, int acc_off, f128 *w_out, f128 *v_out, unsigned long long *acc,
+                   RoundChannel *ch, unsigned long long p0, unsigned long long d0, RoundCtl *ctl,
+                   cudaStream_t s);
+
 // The quadratic sumcheck round of <W, V> (shared with the Ligerito folds):
 // quad_sums accumulates (a0, a2) over the pairs as they are; quad_fold folds
 // both tables at r and, with emit, accumulates the next round's sums.

@@ -551,22 +551,57 @@ std::vector<uint8_t> ProofSystem::ligerito(cudaStream_t s, f128 target) {
     const PcsLevel &L = cfg.levels[i];
     std::vector<f128> rs;
     BZ_CUDA(cudaMemsetAsync(acc, 0, 8 * sizeof(unsigned long long) * (L.k + 1), s));
-    quad_sums(b, f, n, acc, ch->arm(), s);
-    for (int r = 0; r < L.k; r++) {
-      ch->wait(s, W.host_acc, 4);
-      f128 a0 = mk(W.host_acc[0], W.host_acc[1]), a2 = mk(W.host_acc[2], W.host_acc[3]);
-      t.prover_f128(a0);
-      t.prover_f128(a2);
-      grind();
-      f128 c = t.challenge_f128();
-      rs.push_back(c);
-      claim = gadd(a0, gmul(c, gadd(gadd(claim, a2), gmul(c, a2))));
-      bool more = r + 1 < L.k;
-      quad_fold(b, f, c, b2, f2, n, more, acc + 8 * (r + 1),
-                more ? ch->arm() : Publish{nullptr, nullptr, 0}, s);
+    if (lane_->resident_middle() && pg_mid_fits_folds(n, L.k)) {
+      // the level's folds in one resident kernel: fold r takes its challenge
+      // from the downbox and posts the next message itself
+      RoundCtl *ctl = lane_->round_ctl();
+      BZ_CUDA(cudaMemsetAsync(ctl, 0, sizeof(RoundCtl) * (L.k + 1), s));
+      // no other thread's device allocation while the kernel waits for this one
+      ResidentScope gate(true);
+      const unsigned long long d0 = ch->down_next + 1;
+      quad_sums(b, f, n, acc, ch->arm(), s);
+      launch_pg_mid(b, f, n, 0, L.k, 0, 1, b2, f2, acc, ch, ch->next, d0, ctl, s);
+      try {
+        for (int r = 0; r < L.k; r++) {
+          ch->wait(s, W.host_acc, 4);
+          f128 a0 = mk(W.host_acc[0], W.host_acc[1]), a2 = mk(W.host_acc[2], W.host_acc[3]);
+          t.prover_f128(a0);
+          t.prover_f128(a2);
+          grind();
+          f128 c = t.challenge_f128();
+          rs.push_back(c);
+          claim = gadd(a0, gmul(c, gadd(gadd(claim, a2), gmul(c, a2))));
+          const uint64_t cw[2] = {c.lo, c.hi};
+          ch->send(cw, 2);
+          if (r + 1 < L.k) ch->arm();
+        }
+      } catch (...) {  // release the waiting kernel before the lane is reused
+        ch->abort();
+        cudaStreamSynchronize(s);
+        ch->clear_down();
+        throw;
+      }
       std::swap(f, f2);
       std::swap(b, b2);
-      n /= 2;
+      n >>= L.k;
+    } else {
+      quad_sums(b, f, n, acc, ch->arm(), s);
+      for (int r = 0; r < L.k; r++) {
+        ch->wait(s, W.host_acc, 4);
+        f128 a0 = mk(W.host_acc[0], W.host_acc[1]), a2 = mk(W.host_acc[2], W.host_acc[3]);
+        t.prover_f128(a0);
+        t.prover_f128(a2);
+        grind();
+        f128 c = t.challenge_f128();
+        rs.push_back(c);
+        claim = gadd(a0, gmul(c, gadd(gadd(claim, a2), gmul(c, a2))));
+        bool more = r + 1 < L.k;
+        quad_fold(b, f, c, b2, f2, n, more, acc + 8 * (r + 1),
+                  more ? ch->arm() : Publish{nullptr, nullptr, 0}, s);
+        std::swap(f, f2);
+        std::swap(b, b2);
+        n /= 2;
+      }
     }
     int l = L.log_msg_cols;
     bool last = i + 1 == cfg.nlevels;
