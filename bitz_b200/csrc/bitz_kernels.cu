@@ -107,11 +107,52 @@ __global__ void k_mt_col0(const uint32_t *__restrict__ off, const uint32_t *__re
   if (threadIdx.x == 0) st(w0, mk(w[0], w[1]));
 }
 
+// The dense eq table of the rows, dense[lo << log_u2 | hi] = u1[lo] * u2[hi]
+// (row r = hi * 128 + lo): block (lo, part) takes a slice of hi through
+// u1[lo]'s window table, writing along hi.
+constexpr int kMtParts = 2;
+__global__ void k_mt_dense(const f128 *__restrict__ u1, const f128 *__restrict__ u2, int log_u2,
+                           f128 *__restrict__ dense) {
+  __shared__ MulTable T;
+  const int lo = blockIdx.x / kMtParts, part = blockIdx.x % kMtParts;
+  mul_table_build(T, ld(u1 + lo));
+  const size_t per = ((size_t)1 << log_u2) / kMtParts;
+  f128 *out = dense + ((size_t)lo << log_u2);
+  for (size_t hi = part * per + threadIdx.x; hi < (part + 1) * per; hi += blockDim.x)
+    st(out + hi, mul_table(T, ld(u2 + hi)));
+}
+
+// k_mt_transpose over the dense table: each column XORs its rows' entries.
+__global__ void k_mt_gather(const uint32_t *__restrict__ off, const uint32_t *__restrict__ row,
+                            size_t ncols, const f128 *__restrict__ dense, int log_u2,
+                            f128 *__restrict__ weights, size_t padded) {
+  for (size_t c = blockIdx.x * (size_t)blockDim.x + threadIdx.x; c <= padded;
+       c += (size_t)gridDim.x * blockDim.x) {
+    if (c == 0) continue;  // the constant column: k_mt_col0
+    f128 v = mk(0, 0);
+    if (c < ncols)
+      for (uint32_t e = off[c]; e < off[c + 1]; e++) {
+        const uint32_t r = row[e];
+        v = gadd(v, ld(dense + (((size_t)(r & 127) << log_u2) | (r >> 7))));
+      }
+    st(weights + (c - 1), v);
+  }
+}
+
 void mt_transpose(const uint32_t *off, const uint32_t *row, size_t ncols, const f128 *u1,
-                  const f128 *u2, f128 *weights, size_t padded, f128 *w0, cudaStream_t s) {
-  k_mt_transpose<<<grid_for(padded + 1), kThreads, 0, s>>>(off, row, ncols, u1, u2, weights,
-                                                           padded, w0);
-  BZ_LAUNCH_CHECK();
+                  const f128 *u2, f128 *weights, size_t padded, f128 *w0, cudaStream_t s,
+                  f128 *dense, int log_u2) {
+  if (dense && log_u2 >= 8) {
+    k_mt_dense<<<128 * kMtParts, kThreads, 0, s>>>(u1, u2, log_u2, dense);
+    BZ_LAUNCH_CHECK();
+    k_mt_gather<<<grid_for(padded + 1), kThreads, 0, s>>>(off, row, ncols, dense, log_u2, weights,
+                                                          padded);
+    BZ_LAUNCH_CHECK();
+  } else {
+    k_mt_transpose<<<grid_for(padded + 1), kThreads, 0, s>>>(off, row, ncols, u1, u2, weights,
+                                                             padded, w0);
+    BZ_LAUNCH_CHECK();
+  }
   k_mt_col0<<<1, kThreads, 0, s>>>(off, row, u1, u2, w0);
   BZ_LAUNCH_CHECK();
 }

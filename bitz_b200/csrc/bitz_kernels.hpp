@@ -11,8 +11,12 @@ constexpr int kMaxRsDim = 40;  // largest additive-FFT dimension (row bits of a 
 
 void fold_columns(const f128 *cols, size_t ncols, const u128 *exps, u128 *folds, cudaStream_t s);
 void comb_pow(const f128 *table, const u128 *exps, int n, f128 *out, cudaStream_t s);
+// weights[c - 1] = sum over the rows r of column c of u1[r & 127] u2[r >> 7]
+// (rows below 2^(7 + log_u2)); column 0 into w0. With `dense` (2^(7 + log_u2)
+// entries of scratch) the row table is formed once and the columns gather it.
 void mt_transpose(const uint32_t *off, const uint32_t *row, size_t ncols, const f128 *u1,
-                  const f128 *u2, f128 *weights, size_t padded, f128 *w0, cudaStream_t s);
+                  const f128 *u2, f128 *weights, size_t padded, f128 *w0, cudaStream_t s,
+                  f128 *dense, int log_u2);
 // The non-root chaining value of nchunks (a power of two) whole 1 KiB chunks,
 // and the 16 bytes at `extra` (device, may be null) into extra_out. ch: the
 // lane's channel (null: a copy and a stream synchronisation).

@@ -262,6 +262,7 @@ struct Workspace {
   DeviceBuffer<int64_t> prod;
   DeviceBuffer<uint8_t> bit_c;
   DeviceBuffer<f128> codeword0;
+  DeviceBuffer<f128> mt_dense;  // the rows' eq table for the M^T gather
   uint64_t staged_serial = 0;  // the system whose statement these hold
   cudaEvent_t ev_cols = nullptr, ev_folds = nullptr;
   Workspace() {
@@ -907,8 +908,9 @@ int ProofSystem::prove_after_commit(cudaStream_t s, std::vector<uint8_t> &proof)
   size_t nbits = (size_t)1 << S.committed_m;
   W.weights.resize(nbits);
   W.w0.resize(2);
+  W.mt_dense.resize((size_t)128 << sc_cols);
   mt_transpose(dev_->csc_off.get(), dev_->csc_row.get(), S.f_bits + 1, W.u1.get(), W.u2.get(),
-               W.weights.get(), nbits, W.w0.get(), s);
+               W.weights.get(), nbits, W.w0.get(), s, W.mt_dense.get(), sc_cols);
   f128 *w0_h = W.pin_small.get(kPinSmall) + kPinW0;
   // the inner-product statement's weight digest (opening.rs:337-368); the
   // weight of column 0 comes back with it

@@ -306,13 +306,22 @@ __global__ void k_bind(const uint32_t *__restrict__ off, const uint32_t *__restr
   }
 }
 
-// Column 0's entries [0, n) split across blocks; per-block partial sums.
+// Column 0's entries [0, n) split across blocks, and with them the
+// statement-dependent part of C on column 0: the bit constraints whose
+// expected value is one put rho^2 eq(r_x, row) there (each thread scales its
+// share of those rows, which sums to the same total mod q). Per-block
+// partial sums.
 __global__ void k_bind_col0(const uint32_t *__restrict__ row, const uint16_t *__restrict__ idx,
                             const fp *__restrict__ tab, const fp *__restrict__ eq, uint32_t n,
-                            FpCtx c, fp *partial) {
+                            const uint32_t *__restrict__ bit_rows, int n_bits, fp rho2, FpCtx c,
+                            fp *partial) {
   fp acc[1] = {fp_zero()};
   for (uint32_t e = blockIdx.x * blockDim.x + threadIdx.x; e < n; e += gridDim.x * blockDim.x)
     acc[0] = fp_add(acc[0], fp_mul(eq[row[e]], tab[idx[e]], c), c);
+  fp bits = fp_zero();
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n_bits; i += gridDim.x * blockDim.x)
+    bits = fp_add(bits, eq[bit_rows[i]], c);
+  acc[0] = fp_add(acc[0], fp_mul(bits, rho2, c), c);
   block_fp_sum<1>(acc, c, partial);
 }
 
@@ -326,17 +335,6 @@ __global__ void k_bind_col0_finish(const fp *partial, int nblocks, FpCtx c, fp *
   if (threadIdx.x == 0) D[0] = out[0];
 }
 
-// The statement-dependent part of C: the bit constraints whose expected value
-// is one put rho^2 eq(r_x, row) on column 0.
-__global__ void k_bind_bits(const uint32_t *__restrict__ rows, int n, const fp *__restrict__ eq,
-                            fp rho2, FpCtx c, fp *D) {
-  fp acc[1] = {fp_zero()};
-  for (int i = threadIdx.x; i < n; i += blockDim.x) acc[0] = fp_add(acc[0], eq[rows[i]], c);
-  __shared__ fp out[1];
-  block_fp_sum<1>(acc, c, out);
-  __syncthreads();
-  if (threadIdx.x == 0) D[0] = fp_add(D[0], fp_mul(out[0], rho2, c), c);
-}
 
 // The last rounds of each sumcheck in one resident block, fed through the
 // lane's downbox (bounded waits; a missing challenge ends the kernel without
@@ -834,14 +832,11 @@ void spartan_prove(const SpartanArgs &a, Transcript &ts, SpartanScratch &sc, cud
                                            c, D);
   BZ_LAUNCH_CHECK();
   {
-    int g = grid_for(a.col0_nnz);
-    k_bind_col0<<<g, kThreads, 0, s>>>(a.csc_row, a.csc_idx, sc.tab, eq, a.col0_nnz, c, sc.partial);
+    int g = grid_for(std::max<size_t>(a.col0_nnz, (size_t)a.n_bit_rows));
+    k_bind_col0<<<g, kThreads, 0, s>>>(a.csc_row, a.csc_idx, sc.tab, eq, a.col0_nnz, a.bit_rows,
+                                       a.n_bit_rows, rho2, c, sc.partial);
     BZ_LAUNCH_CHECK();
     k_bind_col0_finish<<<1, kThreads, 0, s>>>(sc.partial, g, c, D);
-    BZ_LAUNCH_CHECK();
-  }
-  if (a.n_bit_rows) {
-    k_bind_bits<<<1, kThreads, 0, s>>>(a.bit_rows, a.n_bit_rows, eq, rho2, c, D);
     BZ_LAUNCH_CHECK();
   }
   // inner sumcheck
