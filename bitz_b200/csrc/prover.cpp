@@ -1004,16 +1004,15 @@ int ProofSystem::prove_after_commit(cudaStream_t s, std::vector<uint8_t> &proof)
   for (auto &c : bpt) c = t.challenge_f128();
   std::vector<f128> bw(128);
   eq_table_host(bpt.data(), 7, bw.data());
-  // transpose.rs:14: out[u].bit(v) = claims[v].bit(u)
+  // transpose.rs:14: out[u].bit(v) = claims[v].bit(u), and the target is
+  // sum over u of out[u] bw[u] = sum over v of X^v (sum over the set bits u
+  // of claims[v] of bw[u]): one XOR per set bit and one shift per claim
   f128 ptarget = mk(0, 0);
-  for (int u = 0; u < 128; u++) {
-    f128 tu = mk(0, 0);
-    for (int vv = 0; vv < 128; vv++) {
-      f128 cv = claims[vv];
-      int bit = u < 64 ? (int)((cv.lo >> u) & 1) : (int)((cv.hi >> (u - 64)) & 1);
-      if (bit) (vv < 64 ? tu.lo : tu.hi) |= 1ull << (vv % 64);
-    }
-    ptarget = gadd(ptarget, gmul(tu, bw[u]));
+  for (int vv = 0; vv < 128; vv++) {
+    f128 sv = mk(0, 0);
+    for (uint64_t m = claims[vv].lo; m; m &= m - 1) sv = gadd(sv, bw[__builtin_ctzll(m)]);
+    for (uint64_t m = claims[vv].hi; m; m &= m - 1) sv = gadd(sv, bw[64 + __builtin_ctzll(m)]);
+    ptarget = gadd(ptarget, gmul_xk(sv, vv));
   }
   W.bw.upload(bw.data(), 128, s);
   W.lb.resize(np);
