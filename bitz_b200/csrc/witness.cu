@@ -112,7 +112,17 @@ __global__ void k_hbits(const uint32_t *__restrict__ off, const uint32_t *__rest
 __device__ __forceinline__ int hbit(const uint32_t *h, uint32_t c) { return (h[c >> 5] >> (c & 31)) & 1; }
 
 // Exact products per R1CS row and the integer satisfiability check. The bit
-// constraints' C constant is the statement's expected value (bit_c).
+// constraints' C constant is the statement's expected value (bit_c). One warp
+// per row: the lanes stride over the row's nonzeros of A, B and C (coalesced
+// loads of the columns and coefficients) and the warp adds the three sums with
+// shuffles. Two's-complement addition wraps the same in any order, so the
+// sums equal a row-serial loop's.
+__device__ __forceinline__ int64_t warp_sum64(int64_t v) {
+#pragma unroll
+  for (int off = 16; off > 0; off >>= 1) v += __shfl_xor_sync(0xffffffffu, v, off);
+  return v;
+}
+
 __global__ void k_products(const uint32_t *__restrict__ aoff, const uint32_t *__restrict__ acol,
                            const int64_t *__restrict__ acoef, const uint32_t *__restrict__ boff,
                            const uint32_t *__restrict__ bcol, const int64_t *__restrict__ bcoef,
@@ -120,18 +130,24 @@ __global__ void k_products(const uint32_t *__restrict__ aoff, const uint32_t *__
                            const int64_t *__restrict__ ccoef, const uint32_t *__restrict__ h,
                            size_t rows, size_t n_in, const uint8_t *__restrict__ bit_c,
                            int64_t *prod, int *unsat) {
-  for (size_t r = blockIdx.x * (size_t)blockDim.x + threadIdx.x; r < rows;
-       r += (size_t)gridDim.x * blockDim.x) {
+  const int lane = threadIdx.x & 31;
+  const size_t warps = ((size_t)gridDim.x * blockDim.x) >> 5;
+  for (size_t r = ((size_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; r < rows; r += warps) {
     int64_t a = 0, b = 0, c = 0;
-    for (uint32_t e = aoff[r]; e < aoff[r + 1]; e++) a += hbit(h, acol[e]) ? acoef[e] : 0;
-    for (uint32_t e = boff[r]; e < boff[r + 1]; e++) b += hbit(h, bcol[e]) ? bcoef[e] : 0;
-    for (uint32_t e = coff[r]; e < coff[r + 1]; e++) c += hbit(h, ccol[e]) ? ccoef[e] : 0;
-    if (r < n_in) c += bit_c[r];
-    if (r >= rows - 256) c += bit_c[n_in + (r - (rows - 256))];
-    prod[r] = a;
-    prod[rows + r] = b;
-    prod[2 * rows + r] = c;
-    if ((__int128)a * b != (__int128)c) atomicExch(unsat, 1);
+    for (uint32_t e = aoff[r] + lane; e < aoff[r + 1]; e += 32) a += hbit(h, acol[e]) ? acoef[e] : 0;
+    for (uint32_t e = boff[r] + lane; e < boff[r + 1]; e += 32) b += hbit(h, bcol[e]) ? bcoef[e] : 0;
+    for (uint32_t e = coff[r] + lane; e < coff[r + 1]; e += 32) c += hbit(h, ccol[e]) ? ccoef[e] : 0;
+    a = warp_sum64(a);
+    b = warp_sum64(b);
+    c = warp_sum64(c);
+    if (lane == 0) {
+      if (r < n_in) c += bit_c[r];
+      if (r >= rows - 256) c += bit_c[n_in + (r - (rows - 256))];
+      prod[r] = a;
+      prod[rows + r] = b;
+      prod[2 * rows + r] = c;
+      if ((__int128)a * b != (__int128)c) atomicExch(unsat, 1);
+    }
   }
 }
 
@@ -141,7 +157,7 @@ void witness_generate(const WitnessArgs &a, cudaStream_t s) {
   size_t words = (a.h_len + 31) / 32;
   k_hbits<<<grid_for(words * 32), kThreads, 0, s>>>(a.m_off, a.m_pos, a.h_len, a.f, a.h);
   BZ_LAUNCH_CHECK();
-  k_products<<<grid_for(a.rows), kThreads, 0, s>>>(
+  k_products<<<grid_for(a.rows * 32), kThreads, 0, s>>>(
       a.abc_off[0], a.abc_col[0], a.abc_coef[0], a.abc_off[1], a.abc_col[1], a.abc_coef[1],
       a.abc_off[2], a.abc_col[2], a.abc_coef[2], a.h, a.rows, a.n_inputs, a.bit_c, a.prod,
       a.unsat);
