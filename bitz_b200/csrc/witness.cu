@@ -37,51 +37,75 @@ __device__ __forceinline__ void put_bits(uint32_t *f, uint64_t pos, uint64_t v, 
   }
 }
 
-// One thread per compression: the schedule sums (34 bits), each round's e and
+// One warp per compression: the schedule sums (34 bits), each round's e and
 // a sums before truncation (35 bits: the doubled-Ch/Maj quotient), and the
-// eight feed-forward sums (33 bits).
-__global__ void k_sha_hints(const uint32_t *__restrict__ states, const uint32_t *__restrict__ msgs,
-                            const uint64_t *__restrict__ offsets, int nblocks, uint32_t *f) {
-  int blk = blockIdx.x * blockDim.x + threadIdx.x;
-  if (blk >= nblocks) return;
-  uint64_t pos = offsets[blk];
-  uint32_t w[64];
-  for (int i = 0; i < 16; i++) w[i] = msgs[16 * blk + i];
-  for (int i = 16; i < 64; i++) {
-    uint64_t s = (uint64_t)w[i - 16] +
-                 (ror32(w[i - 15], 7) ^ ror32(w[i - 15], 18) ^ (w[i - 15] >> 3)) +
-                 (uint64_t)w[i - 7] + (ror32(w[i - 2], 17) ^ ror32(w[i - 2], 19) ^ (w[i - 2] >> 10));
-    put_bits(f, pos, s, 34);
-    pos += 34;
-    w[i] = (uint32_t)s;
+// eight feed-forward sums (33 bits), in that order from the compression's
+// bit offset. Lane 0 runs the compression and keeps the 184 values in shared
+// memory; the warp's lanes then OR them into f.
+constexpr int kShaWarps = 4;  // compressions per block
+constexpr int kShaVals = 48 + 128 + 8;
+__global__ void __launch_bounds__(32 * kShaWarps) k_sha_hints(const uint32_t *__restrict__ states,
+                                                              const uint32_t *__restrict__ msgs,
+                                                              const uint64_t *__restrict__ offsets,
+                                                              int nblocks, uint32_t *f) {
+  __shared__ uint64_t vals[kShaWarps][kShaVals];
+  const int wib = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int blk = blockIdx.x * kShaWarps + wib;
+  if (blk >= nblocks) return;  // the whole warp
+  uint64_t *v = vals[wib];
+  if (lane == 0) {
+    uint32_t w[64];
+    for (int i = 0; i < 16; i++) w[i] = msgs[16 * blk + i];
+    for (int i = 16; i < 64; i++) {
+      uint64_t s = (uint64_t)w[i - 16] +
+                   (ror32(w[i - 15], 7) ^ ror32(w[i - 15], 18) ^ (w[i - 15] >> 3)) +
+                   (uint64_t)w[i - 7] +
+                   (ror32(w[i - 2], 17) ^ ror32(w[i - 2], 19) ^ (w[i - 2] >> 10));
+      v[i - 16] = s;
+      w[i] = (uint32_t)s;
+    }
+    uint32_t st[8];
+    for (int i = 0; i < 8; i++) st[i] = states[8 * blk + i];
+    uint32_t a = st[0], b = st[1], c = st[2], d = st[3], e = st[4], ff = st[5], g = st[6],
+             h = st[7];
+    for (int i = 0; i < 64; i++) {
+      uint64_t s1 = ror32(e, 6) ^ ror32(e, 11) ^ ror32(e, 25);
+      uint64_t ch = (e & ff) ^ (~e & g);
+      uint64_t s0 = ror32(a, 2) ^ ror32(a, 13) ^ ror32(a, 22);
+      uint64_t mj = (a & b) ^ (a & c) ^ (b & c);
+      uint64_t base = (uint64_t)h + s1 + c_sha_k[i] + w[i] + ch;
+      uint64_t ne = base + d;
+      uint64_t na = base + s0 + mj;
+      v[48 + 2 * i] = ne;
+      v[49 + 2 * i] = na;
+      h = g;
+      g = ff;
+      ff = e;
+      e = (uint32_t)ne;
+      d = c;
+      c = b;
+      b = a;
+      a = (uint32_t)na;
+    }
+    const uint32_t work[8] = {a, b, c, d, e, ff, g, h};
+    for (int i = 0; i < 8; i++) v[176 + i] = (uint64_t)st[i] + work[i];
   }
-  uint32_t st[8];
-  for (int i = 0; i < 8; i++) st[i] = states[8 * blk + i];
-  uint32_t a = st[0], b = st[1], c = st[2], d = st[3], e = st[4], ff = st[5], g = st[6], h = st[7];
-  for (int i = 0; i < 64; i++) {
-    uint64_t s1 = ror32(e, 6) ^ ror32(e, 11) ^ ror32(e, 25);
-    uint64_t ch = (e & ff) ^ (~e & g);
-    uint64_t s0 = ror32(a, 2) ^ ror32(a, 13) ^ ror32(a, 22);
-    uint64_t mj = (a & b) ^ (a & c) ^ (b & c);
-    uint64_t base = (uint64_t)h + s1 + c_sha_k[i] + w[i] + ch;
-    uint64_t ne = base + d;
-    uint64_t na = base + s0 + mj;
-    put_bits(f, pos, ne, 35);
-    put_bits(f, pos + 35, na, 35);
-    pos += 70;
-    h = g;
-    g = ff;
-    ff = e;
-    e = (uint32_t)ne;
-    d = c;
-    c = b;
-    b = a;
-    a = (uint32_t)na;
-  }
-  uint32_t work[8] = {a, b, c, d, e, ff, g, h};
-  for (int i = 0; i < 8; i++) {
-    put_bits(f, pos, (uint64_t)st[i] + work[i], 33);
-    pos += 33;
+  __syncwarp();
+  const uint64_t pos = offsets[blk];
+  for (int k = lane; k < kShaVals; k += 32) {
+    uint64_t off;
+    int width;
+    if (k < 48) {
+      off = 34ull * k;
+      width = 34;
+    } else if (k < 176) {
+      off = 1632 + 35ull * (k - 48);
+      width = 35;
+    } else {
+      off = 1632 + 4480 + 33ull * (k - 176);
+      width = 33;
+    }
+    put_bits(f, pos + off, v[k], width);
   }
 }
 
@@ -152,7 +176,8 @@ __global__ void k_products(const uint32_t *__restrict__ aoff, const uint32_t *__
 }
 
 void witness_generate(const WitnessArgs &a, cudaStream_t s) {
-  k_sha_hints<<<(a.nblocks + 63) / 64, 64, 0, s>>>(a.states, a.msgs, a.offsets, a.nblocks, a.f);
+  k_sha_hints<<<(a.nblocks + kShaWarps - 1) / kShaWarps, 32 * kShaWarps, 0, s>>>(
+      a.states, a.msgs, a.offsets, a.nblocks, a.f);
   BZ_LAUNCH_CHECK();
   size_t words = (a.h_len + 31) / 32;
   k_hbits<<<grid_for(words * 32), kThreads, 0, s>>>(a.m_off, a.m_pos, a.h_len, a.f, a.h);
