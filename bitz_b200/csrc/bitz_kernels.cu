@@ -495,17 +495,19 @@ void merkle_build(const f128 *cw, size_t rows, int k, uint32_t *nodes, cudaStrea
   }
 }
 
-// A small tree in one block: the leaves, then each level of parents after a
-// block barrier (the nodes stay in global memory, which the block's barrier
-// orders), and the root (node 1) posted as four mailbox words.
+// A small tree in one block: the leaves (unless leaves_done: a grid launch
+// hashed them already), then each level of parents after a block barrier (the
+// nodes stay in global memory, which the block's barrier orders), and the
+// root (node 1) posted as four mailbox words.
 constexpr int kMerkleBlockThreads = 512;
 __global__ void __launch_bounds__(kMerkleBlockThreads) k_merkle_block(
-    const f128 *__restrict__ cw, size_t rows, int k, uint32_t *nodes, Publish pub) {
+    const f128 *__restrict__ cw, size_t rows, int k, uint32_t *nodes, Publish pub,
+    int leaves_done) {
   const uint32_t IV[8] = {0x6A09E667, 0xBB67AE85, 0x3C6EF372, 0xA54FF53A,
                           0x510E527F, 0x9B05688C, 0x1F83D9AB, 0x5BE0CD19};
   const int nbytes = 16 << k;
   const int nblk = (nbytes + 63) / 64;
-  for (size_t i = threadIdx.x; i < rows; i += blockDim.x) {
+  for (size_t i = threadIdx.x; i < rows && !leaves_done; i += blockDim.x) {
     const uint32_t *p = reinterpret_cast<const uint32_t *>(cw + (i << k));
     uint32_t cv[8];
     for (int j = 0; j < 8; j++) cv[j] = IV[j];
@@ -539,7 +541,15 @@ __global__ void __launch_bounds__(kMerkleBlockThreads) k_merkle_block(
 bool merkle_build_posted(const f128 *cw, size_t rows, int k, uint32_t *nodes, Publish pub,
                          cudaStream_t s) {
   if (rows > kMerkleBlockMaxRows || !pub.counter) return false;
-  k_merkle_block<<<1, kMerkleBlockThreads, 0, s>>>(cw, rows, k, nodes, pub);
+  // many leaf compressions: the leaves over the whole GPU first, then the
+  // parents and the post in one block
+  const size_t leaf_compressions = rows * (size_t)(((16 << k) + 63) / 64);
+  const int split = leaf_compressions > 2 * (size_t)kMerkleBlockThreads;
+  if (split) {
+    k_merkle_leaves<<<grid_for(rows), kThreads, 0, s>>>(cw, rows, k, nodes);
+    BZ_LAUNCH_CHECK();
+  }
+  k_merkle_block<<<1, kMerkleBlockThreads, 0, s>>>(cw, rows, k, nodes, pub, split);
   BZ_LAUNCH_CHECK();
   return true;
 }

@@ -462,10 +462,17 @@ int ProofSystem::commit(cudaStream_t s) {
   nodes0_->resize(16 * rows);
   const f128 *fpk = reinterpret_cast<const f128 *>(f_->get());
   rs_encode(fpk, log_n, L0.k, L0.log_inv_rate, T.wh.get(), codeword0_->get(), s);
-  merkle_build(codeword0_->get(), rows, L0.k, nodes0_->get(), s);
   f128 *root_h = W.pin_small.get(kPinSmall) + kPinRoot;
-  BZ_CUDA(cudaMemcpyAsync(root_h, nodes0_->get() + 8, 32, cudaMemcpyDeviceToHost, s));
-  BZ_CUDA(cudaStreamSynchronize(s));
+  RoundChannel *lch = lane_->channel();
+  if (rows <= kMerkleBlockMaxRows &&
+      merkle_build_posted(codeword0_->get(), rows, L0.k, nodes0_->get(), lch->arm(), s)) {
+    // a small tree in one launch that posts its root
+    lch->wait(s, reinterpret_cast<uint64_t *>(root_h), 4);
+  } else {
+    merkle_build(codeword0_->get(), rows, L0.k, nodes0_->get(), s);
+    BZ_CUDA(cudaMemcpyAsync(root_h, nodes0_->get() + 8, 32, cudaMemcpyDeviceToHost, s));
+    BZ_CUDA(cudaStreamSynchronize(s));
+  }
   memcpy(root_, root_h, 32);
   const char *dom = circuit_name(kind_);
   ts_.reset(new Transcript((const uint8_t *)"bitz/circuit-e2e/v2", 19, (const uint8_t *)dom,
