@@ -27,21 +27,9 @@ struct Point {
 // repay building it.
 __device__ __forceinline__ void eq_factor_block(const Point &p, int first, int n, f128 *out,
                                                 MulTable &T) {
-  // the first (up to six) levels at once: entry k is the product of its six
-  // factors (1 + z_i, or z_i where bit i of k is set; one past the n-th), a
-  // product tree of depth three instead of six dependent doubling levels
-  const int l0 = n < 6 ? n : 6;
-  for (int k = threadIdx.x; k < (1 << l0); k += blockDim.x) {
-    f128 v[6];
-#pragma unroll
-    for (int i = 0; i < 6; i++) {
-      const f128 z = i < l0 ? p.c[first + i] : mk(0, 0);
-      v[i] = i >= l0 ? mk(1, 0) : ((k >> i) & 1) ? z : gadd(mk(1, 0), z);
-    }
-    out[k] = gmul(gmul(gmul(v[0], v[1]), gmul(v[2], v[3])), gmul(v[4], v[5]));
-  }
+  if (threadIdx.x == 0) out[0] = mk(1, 0);
   __syncthreads();
-  for (int i = l0; i < n; i++) {
+  for (int i = 0; i < n; i++) {
     const f128 z = p.c[first + i];
     const int half = 1 << i;
     const bool tab = half >= 64;  // uniform across the block
