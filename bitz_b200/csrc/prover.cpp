@@ -528,8 +528,7 @@ std::vector<uint8_t> ProofSystem::ligerito(cudaStream_t s, f128 target) {
     t.public_message(b4, 4);
     uint8_t seed[16];
     t.squeeze(seed, 16);
-    uint64_t nonce = 0;
-    while (!pow_valid(seed, nonce, bits)) nonce++;
+    const uint64_t nonce = pow_search(seed, bits);
     t.prover_message(&nonce, 8);
   };
   auto sample_vec = [&](size_t n) {

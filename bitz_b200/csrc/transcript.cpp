@@ -10,31 +10,107 @@
 #include <functional>
 #include <memory>
 #include <mutex>
+#include <stdexcept>
 #include <thread>
 #include <vector>
 
 namespace bz {
 
+static const uint32_t kB3IV[8] = {0x6A09E667, 0xBB67AE85, 0x3C6EF372, 0xA54FF53A,
+                                  0x510E527F, 0x9B05688C, 0x1F83D9AB, 0x5BE0CD19};
+constexpr uint32_t kPowLen = 39;  // 15 + 16 + 8 bytes: one block of one chunk
+constexpr uint32_t kPowFlags = B3_CHUNK_START | B3_CHUNK_END | B3_ROOT;
 
-
-
-bool pow_valid(const uint8_t seed[16], uint64_t nonce, uint32_t bits) {
-  if (bits > 32) return false;
-  if (bits == 0) return nonce == 0;
-  // The message is 15 + 16 + 8 = 39 bytes: one BLAKE3 block of one chunk.
+// The grinding message "bitz-pcs-pow-v1" || seed || nonce (little-endian) as
+// the block's sixteen words (crates/transcript/src/pow.rs:38-50).
+static void pow_words(const uint8_t seed[16], uint64_t nonce, uint32_t m[16]) {
   uint8_t blk[64];
   memset(blk, 0, sizeof blk);
   memcpy(blk, "bitz-pcs-pow-v1", 15);
   memcpy(blk + 15, seed, 16);
   for (int i = 0; i < 8; i++) blk[31 + i] = (uint8_t)(nonce >> (8 * i));
-  static const uint32_t IV[8] = {0x6A09E667, 0xBB67AE85, 0x3C6EF372, 0xA54FF53A,
-                                 0x510E527F, 0x9B05688C, 0x1F83D9AB, 0x5BE0CD19};
-  uint32_t m[16], o[8];
   b3_load_le(blk, m, 16);
-  b3_compress(IV, m, 0, 39, B3_CHUNK_START | B3_CHUNK_END | B3_ROOT, o);
-  uint32_t v = __builtin_bswap32(o[0]);
-  uint32_t lz = v == 0 ? 32 : (uint32_t)__builtin_clz(v);
-  return lz >= bits;
+}
+
+// A hash passes when its first `bits` bits, read big-endian from byte 0, are
+// zero: the output's word 0 has no bit in common with this mask.
+static uint32_t pow_mask(uint32_t bits) { return __builtin_bswap32(~0u << (32 - bits)); }
+
+bool pow_valid(const uint8_t seed[16], uint64_t nonce, uint32_t bits) {
+  if (bits > 32) return false;
+  if (bits == 0) return nonce == 0;
+  uint32_t m[16], o[8];
+  pow_words(seed, nonce, m);
+  b3_compress(kB3IV, m, 0, kPowLen, kPowFlags, o);
+  return (o[0] & pow_mask(bits)) == 0;
+}
+
+// Sixteen nonces base .. base + 15 per step, one per 32-bit lane. With base a
+// multiple of 16 the nonces differ only in their byte 0, the top byte of
+// message word 7; words 8 and 9 (nonce bytes 1-7) are the same in every lane.
+// Returns the smallest passing nonce, the one the one-at-a-time loop finds.
+#define BZ_B3_G16(a, b, c, d, x, y)                                 \
+  do {                                                              \
+    s[a] = _mm512_add_epi32(_mm512_add_epi32(s[a], s[b]), x);       \
+    s[d] = _mm512_ror_epi32(_mm512_xor_si512(s[d], s[a]), 16);      \
+    s[c] = _mm512_add_epi32(s[c], s[d]);                            \
+    s[b] = _mm512_ror_epi32(_mm512_xor_si512(s[b], s[c]), 12);      \
+    s[a] = _mm512_add_epi32(_mm512_add_epi32(s[a], s[b]), y);       \
+    s[d] = _mm512_ror_epi32(_mm512_xor_si512(s[d], s[a]), 8);       \
+    s[c] = _mm512_add_epi32(s[c], s[d]);                            \
+    s[b] = _mm512_ror_epi32(_mm512_xor_si512(s[b], s[c]), 7);       \
+  } while (0)
+
+__attribute__((target("avx512f"))) static uint64_t pow_search16(const uint32_t w[16],
+                                                                 uint32_t mask) {
+  const __m512i lane = _mm512_setr_epi32(0, 1, 2, 3, 4, 5, 6, 7, 8, 9, 10, 11, 12, 13, 14, 15);
+  const __m512i vmask = _mm512_set1_epi32((int)mask);
+  for (uint64_t base = 0;; base += 16) {
+    __m512i m[16];
+    for (int i = 0; i < 16; i++) m[i] = _mm512_set1_epi32((int)w[i]);
+    m[7] = _mm512_or_si512(
+        m[7], _mm512_slli_epi32(_mm512_add_epi32(_mm512_set1_epi32((int)(base & 0xff)), lane), 24));
+    m[8] = _mm512_set1_epi32((int)(uint32_t)(base >> 8));
+    m[9] = _mm512_set1_epi32((int)(uint32_t)(base >> 40));
+    __m512i s[16];
+    for (int i = 0; i < 8; i++) s[i] = _mm512_set1_epi32((int)kB3IV[i]);
+    for (int i = 0; i < 4; i++) s[8 + i] = _mm512_set1_epi32((int)kB3IV[i]);
+    s[12] = _mm512_setzero_si512();
+    s[13] = _mm512_setzero_si512();
+    s[14] = _mm512_set1_epi32((int)kPowLen);
+    s[15] = _mm512_set1_epi32((int)kPowFlags);
+    for (int r = 0; r < 7; r++) {
+      BZ_B3_G16(0, 4, 8, 12, m[0], m[1]);
+      BZ_B3_G16(1, 5, 9, 13, m[2], m[3]);
+      BZ_B3_G16(2, 6, 10, 14, m[4], m[5]);
+      BZ_B3_G16(3, 7, 11, 15, m[6], m[7]);
+      BZ_B3_G16(0, 5, 10, 15, m[8], m[9]);
+      BZ_B3_G16(1, 6, 11, 12, m[10], m[11]);
+      BZ_B3_G16(2, 7, 8, 13, m[12], m[13]);
+      BZ_B3_G16(3, 4, 9, 14, m[14], m[15]);
+      // the message schedule permutation of b3_compress
+      const __m512i t[16] = {m[2], m[6], m[3],  m[10], m[7],  m[0],  m[4],  m[13],
+                             m[1], m[11], m[12], m[5], m[9], m[14], m[15], m[8]};
+      for (int i = 0; i < 16; i++) m[i] = t[i];
+    }
+    const __mmask16 fail = _mm512_test_epi32_mask(_mm512_xor_si512(s[0], s[8]), vmask);
+    if (fail != 0xffff) return base + (uint64_t)__builtin_ctz(~(unsigned)fail & 0xffffu);
+  }
+}
+#undef BZ_B3_G16
+
+uint64_t pow_search(const uint8_t seed[16], uint32_t bits) {
+  if (bits == 0) return 0;
+  if (bits > 32) throw std::invalid_argument("grinding difficulty exceeds 32 bits");
+  static const bool simd = __builtin_cpu_supports("avx512f");
+  if (simd) {
+    uint32_t w[16];
+    pow_words(seed, 0, w);
+    return pow_search16(w, pow_mask(bits));
+  }
+  uint64_t nonce = 0;
+  while (!pow_valid(seed, nonce, bits)) nonce++;
+  return nonce;
 }
 
 void Transcript::grind(const char *label, uint32_t bits) {
@@ -48,8 +124,7 @@ void Transcript::grind(const char *label, uint32_t bits) {
   public_message(b4, 4);
   uint8_t seed[16];
   squeeze(seed, 16);
-  uint64_t nonce = 0;
-  while (!pow_valid(seed, nonce, bits)) nonce++;
+  const uint64_t nonce = pow_search(seed, bits);
   uint8_t n8[8];
   for (int i = 0; i < 8; i++) n8[i] = (uint8_t)(nonce >> (8 * i));
   prover_message(n8, 8);

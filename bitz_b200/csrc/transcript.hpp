@@ -145,6 +145,8 @@ class Transcript {
 
 // crates/transcript/src/pow.rs:38-50
 bool pow_valid(const uint8_t seed[16], uint64_t nonce, uint32_t bits);
+// The smallest nonce that passes (0 for no grinding); at most 32 bits.
+uint64_t pow_search(const uint8_t seed[16], uint32_t bits);
 
 // crates/common/src/security.rs:25-31
 inline uint32_t grinding_bits(uint32_t security_bits, uint64_t coefficient) {

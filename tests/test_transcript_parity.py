@@ -33,6 +33,21 @@ def test_random_event_sequences_agree(seed):
     assert np.array_equal(p.verifier_message_f128(), o.verifier_message_f128())
 
 
+def test_grinding_nonces_agree_at_every_difficulty():
+    # The library searches sixteen nonces per step; the oracle tries them one
+    # at a time. Both must send the smallest passing nonce, wherever it falls
+    # within a step of sixteen (difficulties 1-16, several seeds each).
+    for bits in range(1, 17):
+        for s in range(4 if bits <= 12 else 1):
+            session = b"grind-%d-%d" % (bits, s)
+            p = bz.build_prover(session, b"pow")
+            o = of.Transcript(session, b"pow")
+            p.grind(b"bitz/pcs/sumcheck/v1", bits)
+            o.grind(b"bitz/pcs/sumcheck/v1", bits)
+            assert p.narg() == o.narg(), (bits, s)
+            assert np.array_equal(p.verifier_message_f128(), o.verifier_message_f128())
+
+
 def test_prime_sampling_agrees_and_is_prime():
     import ctypes
     p = bz.build_prover(b"s", b"prime")
