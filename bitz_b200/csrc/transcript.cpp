@@ -3,6 +3,8 @@
 
 #include <immintrin.h>
 
+#include <stdlib.h>
+
 #include <algorithm>
 #include <atomic>
 #include <condition_variable>
@@ -99,10 +101,20 @@ __attribute__((target("avx512f"))) static uint64_t pow_search16(const uint32_t w
 }
 #undef BZ_B3_G16
 
+// The AVX-512 paths (grinding, the prime's strong rounds) run where the host
+// has the instructions, unless BITZ_HOST_SIMD=0 selects the scalar ones.
+static bool host_simd() {
+  static const bool on = [] {
+    const char *v = getenv("BITZ_HOST_SIMD");
+    return !(v && v[0] == '0');
+  }();
+  return on;
+}
+
 uint64_t pow_search(const uint8_t seed[16], uint32_t bits) {
   if (bits == 0) return 0;
   if (bits > 32) throw std::invalid_argument("grinding difficulty exceeds 32 bits");
-  static const bool simd = __builtin_cpu_supports("avx512f");
+  static const bool simd = host_simd() && __builtin_cpu_supports("avx512f");
   if (simd) {
     uint32_t w[16];
     pow_words(seed, 0, w);
@@ -177,6 +189,154 @@ static bool strong_round(const FpCtx &c, u128 q, u128 base) {
   return false;
 }
 
+// The same rounds for many bases of one modulus on AVX-512 IFMA (52-bit
+// multiply-add): Montgomery arithmetic in radix 2^52 with three limbs and
+// R = 2^156, after the IFMA multiplication of Gueron and Krasnov
+// ("Accelerating big integer arithmetic using Intel IFMA extensions", 2016).
+// As 4q < R, products of values below 2q stay below 2q without a final
+// subtraction, so a value is 1 (or -1) exactly when it equals one of that
+// residue's two forms below 2q. Every base follows the same square-and-
+// multiply schedule (the exponent is the modulus's), eight per vector.
+namespace {
+struct MrSimd {
+  uint64_t q[3], qinv;        // modulus limbs; -q^-1 mod 2^52
+  uint64_t one[3], one_q[3];  // R mod q, and that plus q
+  uint64_t neg[3], neg_q[3];  // q - (R mod q), and that plus q
+  uint64_t r2[3];             // R^2 mod q
+  u128 e;                     // (q - 1) >> shift
+  int shift, top;             // top: the highest set bit of e
+};
+
+struct V3 {
+  __m512i l[3];
+};
+}  // namespace
+
+static void limbs52(u128 v, uint64_t o[3]) {
+  const uint64_t m = (1ull << 52) - 1;
+  o[0] = (uint64_t)v & m;
+  o[1] = (uint64_t)(v >> 52) & m;
+  o[2] = (uint64_t)(v >> 104);
+}
+
+static MrSimd mr_simd_setup(u128 q) {
+  MrSimd s;
+  limbs52(q, s.q);
+  uint64_t inv = 1;
+  for (int i = 0; i < 7; i++) inv *= 2 - (uint64_t)q * inv;  // Newton: q * inv = 1 mod 2^64
+  s.qinv = (0 - inv) & ((1ull << 52) - 1);
+  u128 x = 1 % q;
+  for (int i = 0; i < 156; i++) {
+    x <<= 1;
+    if (x >= q) x -= q;
+  }
+  const u128 rm = x;
+  for (int i = 0; i < 156; i++) {
+    x <<= 1;
+    if (x >= q) x -= q;
+  }
+  limbs52(x, s.r2);
+  limbs52(rm, s.one);
+  limbs52(rm + q, s.one_q);
+  limbs52(q - rm, s.neg);
+  limbs52(q - rm + q, s.neg_q);
+  const u128 qm1 = q - 1;
+  s.shift = 0;
+  while (((qm1 >> s.shift) & 1) == 0) s.shift++;
+  s.e = qm1 >> s.shift;
+  s.top = 127;
+  while (s.top > 0 && !((s.e >> s.top) & 1)) s.top--;
+  return s;
+}
+
+#define BZ_IFMA __attribute__((target("avx512f,avx512ifma")))
+
+// a b R^-1 mod q, below 2q for a, b below 2q; limbs below 2^52 in and out.
+BZ_IFMA static inline V3 mont52(const V3 &a, const V3 &b, const __m512i q[3], __m512i qinv) {
+  const __m512i z = _mm512_setzero_si512(), m52 = _mm512_set1_epi64((1ll << 52) - 1);
+  __m512i t0 = z, t1 = z, t2 = z, t3 = z;
+  for (int i = 0; i < 3; i++) {
+    const __m512i bi = b.l[i];
+    t0 = _mm512_madd52lo_epu64(t0, a.l[0], bi);
+    t1 = _mm512_madd52hi_epu64(t1, a.l[0], bi);
+    t1 = _mm512_madd52lo_epu64(t1, a.l[1], bi);
+    t2 = _mm512_madd52hi_epu64(t2, a.l[1], bi);
+    t2 = _mm512_madd52lo_epu64(t2, a.l[2], bi);
+    t3 = _mm512_madd52hi_epu64(t3, a.l[2], bi);
+    // m = t0 (-q^-1) mod 2^52 makes t0 + m q0 a multiple of 2^52
+    const __m512i m = _mm512_madd52lo_epu64(z, t0, qinv);
+    t0 = _mm512_madd52lo_epu64(t0, q[0], m);
+    t1 = _mm512_madd52hi_epu64(t1, q[0], m);
+    t1 = _mm512_madd52lo_epu64(t1, q[1], m);
+    t2 = _mm512_madd52hi_epu64(t2, q[1], m);
+    t2 = _mm512_madd52lo_epu64(t2, q[2], m);
+    t3 = _mm512_madd52hi_epu64(t3, q[2], m);
+    t0 = _mm512_add_epi64(t1, _mm512_srli_epi64(t0, 52));
+    t1 = t2;
+    t2 = t3;
+    t3 = z;
+  }
+  V3 r;
+  r.l[0] = _mm512_and_si512(t0, m52);
+  t1 = _mm512_add_epi64(t1, _mm512_srli_epi64(t0, 52));
+  r.l[1] = _mm512_and_si512(t1, m52);
+  r.l[2] = _mm512_add_epi64(t2, _mm512_srli_epi64(t1, 52));
+  return r;
+}
+
+BZ_IFMA static inline __mmask8 eq52(const V3 &a, const uint64_t c[3]) {
+  return _mm512_cmpeq_epi64_mask(a.l[0], _mm512_set1_epi64((long long)c[0])) &
+         _mm512_cmpeq_epi64_mask(a.l[1], _mm512_set1_epi64((long long)c[1])) &
+         _mm512_cmpeq_epi64_mask(a.l[2], _mm512_set1_epi64((long long)c[2]));
+}
+
+// pass[i] = strong_round(q, bases[i]) for i < n, bases below q. Two vectors
+// of eight bases go through the schedule side by side, so each product's
+// dependent chain overlaps the other's.
+BZ_IFMA static void strong_rounds_ifma(u128 qv, const u128 *bases, int n, char *pass) {
+  const MrSimd s = mr_simd_setup(qv);
+  __m512i q[3];
+  for (int i = 0; i < 3; i++) q[i] = _mm512_set1_epi64((long long)s.q[i]);
+  const __m512i qinv = _mm512_set1_epi64((long long)s.qinv);
+  V3 r2;
+  for (int i = 0; i < 3; i++) r2.l[i] = _mm512_set1_epi64((long long)s.r2[i]);
+  for (int at = 0; at < n; at += 16) {
+    alignas(64) uint64_t bl[2][3][8];
+    for (int k = 0; k < 16; k++) {
+      uint64_t t[3];
+      limbs52(at + k < n ? bases[at + k] : 2, t);
+      for (int i = 0; i < 3; i++) bl[k >> 3][i][k & 7] = t[i];
+    }
+    V3 b0, b1;
+    for (int i = 0; i < 3; i++) {
+      b0.l[i] = _mm512_load_si512(bl[0][i]);
+      b1.l[i] = _mm512_load_si512(bl[1][i]);
+    }
+    b0 = mont52(b0, r2, q, qinv);  // to Montgomery form
+    b1 = mont52(b1, r2, q, qinv);
+    V3 w0 = b0, w1 = b1;  // the top bit of e is set
+    for (int i = s.top - 1; i >= 0; i--) {
+      w0 = mont52(w0, w0, q, qinv);
+      w1 = mont52(w1, w1, q, qinv);
+      if ((s.e >> i) & 1) {
+        w0 = mont52(w0, b0, q, qinv);
+        w1 = mont52(w1, b1, q, qinv);
+      }
+    }
+    __mmask8 ok0 = eq52(w0, s.one) | eq52(w0, s.one_q) | eq52(w0, s.neg) | eq52(w0, s.neg_q);
+    __mmask8 ok1 = eq52(w1, s.one) | eq52(w1, s.one_q) | eq52(w1, s.neg) | eq52(w1, s.neg_q);
+    for (int r = 1; r < s.shift; r++) {
+      w0 = mont52(w0, w0, q, qinv);
+      w1 = mont52(w1, w1, q, qinv);
+      ok0 |= eq52(w0, s.neg) | eq52(w0, s.neg_q);
+      ok1 |= eq52(w1, s.neg) | eq52(w1, s.neg_q);
+    }
+    const unsigned ok = (unsigned)ok0 | ((unsigned)ok1 << 8);
+    for (int k = 0; k < 16 && at + k < n; k++) pass[at + k] = (char)((ok >> k) & 1);
+  }
+}
+#undef BZ_IFMA
+
 // A few host threads for independent work items of one call (the
 // Miller-Rabin rounds of a candidate). The calling thread works on its own
 // job too, so a call finishes even when every pool thread is busy with
@@ -249,7 +409,8 @@ class HostPool {
 // and stopping at the first failure. The draws depend on the outcomes, so
 // they follow the reference exactly: once a candidate passes its first round
 // (almost surely a prime), the sponge state is saved, the other 79 bases are
-// drawn in order and their rounds run in parallel; if some round j failed,
+// drawn in order and their rounds run together (sixteen bases at a time on
+// AVX-512 IFMA, else spread over the host pool); if some round j failed,
 // the state goes back and exactly the bases up to j are drawn again, as the
 // sequential loop would have.
 u128 Transcript::prime(uint32_t bits) {
@@ -292,11 +453,16 @@ u128 Transcript::prime(uint32_t bits) {
         memcpy(st_saved, st_, sizeof st_);
         const int absorb_saved = absorb_pos_, squeeze_saved = squeeze_pos_;
         std::vector<u128> base(kRounds);
-        for (int r = 1; r < kRounds; r++) base[r] = draw();
+        for (int r = 1; r < kRounds; r++) base[r] = 2 + draw();
         std::vector<char> pass(kRounds, 1);
-        HostPool::get().run(kRounds - 1, [&](int i) {
-          pass[i + 1] = strong_round(ctx, cand, 2 + base[i + 1]) ? 1 : 0;
-        });
+        static const bool ifma = host_simd() && __builtin_cpu_supports("avx512f") &&
+                                 __builtin_cpu_supports("avx512ifma");
+        if (ifma)
+          strong_rounds_ifma(cand, base.data() + 1, kRounds - 1, pass.data() + 1);
+        else
+          HostPool::get().run(kRounds - 1, [&](int i) {
+            pass[i + 1] = strong_round(ctx, cand, base[i + 1]) ? 1 : 0;
+          });
         int fail = 0;
         for (int r = 1; r < kRounds && !fail; r++)
           if (!pass[r]) fail = r;

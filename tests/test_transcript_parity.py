@@ -1,6 +1,10 @@
 """The product's host transcript (libbitz_b200.so) against the oracle's, byte for byte.
 
 Runs on CPU: the transcript is host code (Fiat-Shamir stays on the host)."""
+import os
+import subprocess
+import sys
+
 import numpy as np
 import pytest
 
@@ -63,9 +67,53 @@ def test_prime_sampling_agrees_and_is_prime():
             assert pow(base, q - 1, q) == 1
 
 
+def _oracle_prime(o, bits):
+    import ctypes
+    buf = ctypes.create_string_buffer(16)
+    of.lib().o_ts_prime_le(ctypes.c_void_p(o.h), bits, buf)
+    return int.from_bytes(buf.raw, "little")
+
+
+# Sessions (empty instance) in which a composite candidate passes its first
+# strong round and fails a later one: the library runs the remaining rounds
+# together, so it must put the sponge back and redraw exactly the bases the
+# oracle's round-at-a-time loop draws.
+@pytest.mark.parametrize("session,bits", [
+    (b"rb-14-2554", 14), (b"rb-14-3623", 14), (b"rb-16-261", 16),
+    (b"rb-16-518", 16), (b"rb-18-331", 18), (b"rb-18-902", 18)])
+def test_prime_sampling_after_a_round_zero_liar(session, bits):
+    p = bz.build_prover(session, b"")
+    o = of.Transcript(session, b"")
+    assert p.squeeze_prime(bits) == _oracle_prime(o, bits)
+    assert np.array_equal(p.verifier_message_f128(), o.verifier_message_f128())
+
+
+def test_prime_sampling_agrees_over_many_sessions():
+    for i in range(150):
+        session = b"many-%d" % i
+        bits = (121, 64, 40)[i % 3]
+        p = bz.build_prover(session, b"prime")
+        o = of.Transcript(session, b"prime")
+        assert p.squeeze_prime(bits) == _oracle_prime(o, bits), (i, bits)
+        assert np.array_equal(p.verifier_message_f128(), o.verifier_message_f128())
+
+
 def test_hints_bypass_the_sponge():
     a = bz.build_prover(b"s", b"i")
     b = bz.build_prover(b"s", b"i")
     a.hint(b"\xaa" * 5)
     assert np.array_equal(a.verifier_message_f128(), b.verifier_message_f128())
     assert a.hints() == b"\xaa" * 5 and a.narg() == b""
+
+
+@pytest.mark.skipif(os.environ.get("BITZ_HOST_SIMD") == "0", reason="already the scalar paths")
+def test_scalar_host_paths_agree_too():
+    # BITZ_HOST_SIMD=0 selects the one-nonce-at-a-time grind and the
+    # thread-pool strong rounds (the paths of hosts without AVX-512); the
+    # grinding and prime tests above rerun on them in a fresh process.
+    env = dict(os.environ, BITZ_HOST_SIMD="0")
+    r = subprocess.run(
+        [sys.executable, "-m", "pytest", "-q", "-p", "no:cacheprovider", __file__,
+         "-k", "grinding or prime"],
+        env=env, capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0, r.stdout[-2000:] + r.stderr[-2000:]
