@@ -557,16 +557,29 @@ bool merkle_build_posted(const f128 *cw, size_t rows, int k, uint32_t *nodes, Pu
 // ----------------------------------------------------- Ligerito query glue
 
 // basis[j] += sum_q s_q prod_{t in j} w[q][t]: block q builds its tensor table
-// in shared memory by doubling and XORs it into the basis.
-__global__ void k_query_basis(const f128 *__restrict__ w, const f128 *__restrict__ scale, int l,
+// in shared memory by doubling and XORs it into the basis. The factors are
+// the subspace polynomials at the queried row: w[q][t] = Wh_t(x_q) = the sum
+// of Wh_t(X^s) over the set bits s >= t of idx[q] (wh is that table, t-major
+// with kMaxRsDim entries per t), formed by the block's first threads.
+__global__ void k_query_basis(const uint64_t *__restrict__ idx, const f128 *__restrict__ wh,
+                              const f128 *__restrict__ scale, int l,
                               unsigned long long *basis) {
   extern __shared__ f128 tab[];
-  int q = blockIdx.x;
+  __shared__ f128 w[kMaxRsDim];
+  const int q = blockIdx.x;
+  if (threadIdx.x < l) {
+    const int t = threadIdx.x;
+    f128 v = mk(0, 0);
+    // row indices stay below 2^kMaxRsDim; the mask keeps every read in wh
+    for (uint64_t bits = (idx[q] >> t) & ((1ull << (kMaxRsDim - t)) - 1); bits; bits &= bits - 1)
+      v = gadd(v, ld(wh + t * kMaxRsDim + t + __ffsll((long long)bits) - 1));
+    w[t] = v;
+  }
   if (threadIdx.x == 0) tab[0] = scale[q];
   __syncthreads();
   for (int t = 0; t < l; t++) {
     int h = 1 << t;
-    f128 wt = w[q * kMaxRsDim + t];
+    const f128 wt = w[t];
     for (int j = threadIdx.x; j < h; j += blockDim.x) tab[h + j] = gmul(tab[j], wt);
     __syncthreads();
   }
@@ -577,12 +590,14 @@ __global__ void k_query_basis(const f128 *__restrict__ w, const f128 *__restrict
   }
 }
 
-void query_basis(const f128 *w, const f128 *scale, int nq, int l, f128 *basis, cudaStream_t s) {
+void query_basis(const uint64_t *idx, const f128 *wh, const f128 *scale, int nq, int l,
+                 f128 *basis, cudaStream_t s) {
+  if (l > kMaxRsDim || l > kThreads) throw CudaError("query basis dimension out of range");
   size_t smem = sizeof(f128) << l;
-  if (smem > 48 * 1024)
+  if (smem > 48 * 1024 - sizeof(f128) * kMaxRsDim)
     BZ_CUDA(cudaFuncSetAttribute(k_query_basis, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)smem));
-  k_query_basis<<<nq, kThreads, smem, s>>>(w, scale, l, (unsigned long long *)basis);
+  k_query_basis<<<nq, kThreads, smem, s>>>(idx, wh, scale, l, (unsigned long long *)basis);
   BZ_LAUNCH_CHECK();
 }
 

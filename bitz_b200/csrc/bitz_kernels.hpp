@@ -40,7 +40,10 @@ void merkle_build(const f128 *cw, size_t rows, int k, uint32_t *nodes, cudaStrea
 constexpr size_t kMerkleBlockMaxRows = 4096;
 bool merkle_build_posted(const f128 *cw, size_t rows, int k, uint32_t *nodes, Publish pub,
                          cudaStream_t s);
-void query_basis(const f128 *w, const f128 *scale, int nq, int l, f128 *basis, cudaStream_t s);
+// basis += sum_q scale[q] * tensor(Wh_t(x_q), t < l), x_q = idx[q]; wh is the
+// kMaxRsDim x kMaxRsDim subspace table (Wh_t(X^s) at t * kMaxRsDim + s).
+void query_basis(const uint64_t *idx, const f128 *wh, const f128 *scale, int nq, int l,
+                 f128 *basis, cudaStream_t s);
 // Per query (idx[q] < rows): the codeword row and its Merkle siblings, packed
 // as width + 2 * depth 16-byte units.
 void gather_openings(const f128 *cw, const uint32_t *nodes, size_t rows, int width, int depth,

@@ -239,7 +239,7 @@ struct Workspace {
   DeviceBuffer<fp> cols_fp;
   DeviceBuffer<u128> exps, folds;
   DeviceBuffer<f128> images, u1, u2, weights, w0, ones, eq, eqs, suffix, basis, eq_ood, lf, lb,
-      lf2, lb2, qw, qs, level_cw, bw;
+      lf2, lb2, qs, level_cw, bw;
   DeviceBuffer<uint32_t> b3, level_nodes;
   DeviceBuffer<unsigned long long> acc;
   fp *host_fp = nullptr;
@@ -699,28 +699,16 @@ std::vector<uint8_t> ProofSystem::ligerito(cudaStream_t s, f128 target) {
     f128 mu = t.challenge_f128();
     std::vector<f128> beta((size_t)1 << av);
     eq_table_host(alpha.data(), av, beta.data());
-    // glue: basis += sum_q s_q X(x_q) with X_j(x) = prod_{t in j} Wh_t(x)
-    const size_t nwq = (size_t)L.queries * kMaxRsDim;
-    f128 *wq = W.pin_qw.get(nwq + L.queries), *sq = wq + nwq;
+    // glue: basis += sum_q s_q X(x_q) with X_j(x) = prod_{t in j} Wh_t(x);
+    // the kernel forms Wh_t(x_q) from the uploaded row indices
+    f128 *sq = W.pin_qw.get(L.queries);
     for (int q = 0; q < L.queries; q++) {
       sq[q] = gmul(mu, beta[q]);
       claim = gadd(claim, gmul(sq[q], vals[q]));
-      // Wh_t(x_q) = sum over the set bits s >= t of idx of Wh_t(X^s)
-      for (int tt = 0; tt < kMaxRsDim; tt++) {
-        f128 w = mk(0, 0);
-        if (tt < l)
-          for (uint64_t bits = idx[q] >> tt; bits; bits &= bits - 1) {
-            int sb = tt + __builtin_ctzll(bits);
-            w = gadd(w, T.wh_host[tt * kMaxRsDim + sb]);
-          }
-        wq[(size_t)q * kMaxRsDim + tt] = w;
-      }
     }
-    W.qw.resize(nwq);
     W.qs.resize(L.queries);
-    BZ_CUDA(cudaMemcpyAsync(W.qw.get(), wq, nwq * 16, cudaMemcpyHostToDevice, s));
     BZ_CUDA(cudaMemcpyAsync(W.qs.get(), sq, (size_t)L.queries * 16, cudaMemcpyHostToDevice, s));
-    query_basis(W.qw.get(), W.qs.get(), L.queries, l, b, s);
+    query_basis(W.qidx.get(), T.wh.get(), W.qs.get(), L.queries, l, b, s);
     ph.mark("lig queries+glue");
     if (!last) {
       cw = next_cw[flip].get();

@@ -12,6 +12,7 @@
 #include <stdint.h>
 #include <string.h>
 
+#include <algorithm>
 #include <string>
 #include <vector>
 
@@ -58,15 +59,21 @@ class Transcript {
     hints_.insert(hints_.end(), p, p + len);
   }
 
+  // Byte i of the rate is byte i % 8 (little-endian) of lane i / 8, which on
+  // a little-endian host is where it lies in memory: spans are copied whole.
   void squeeze(uint8_t *out, size_t n) {
-    for (size_t i = 0; i < n; i++) {
+    static_assert(__BYTE_ORDER__ == __ORDER_LITTLE_ENDIAN__, "lanes read as memory bytes");
+    while (n > 0) {
       if (squeeze_pos_ == RATE) {
         keccak_f1600(st_);
         squeeze_pos_ = 0;
         absorb_pos_ = 0;
       }
-      out[i] = (uint8_t)(st_[squeeze_pos_ / 8] >> (8 * (squeeze_pos_ % 8)));
-      squeeze_pos_++;
+      const size_t take = std::min(n, (size_t)(RATE - squeeze_pos_));
+      memcpy(out, reinterpret_cast<const uint8_t *>(st_) + squeeze_pos_, take);
+      squeeze_pos_ += (int)take;
+      out += take;
+      n -= take;
     }
   }
 
