@@ -50,6 +50,7 @@ SIGNATURES = [
       ctypes.POINTER(ctypes.c_double)]),
     ("bitz_free", None, [_vp]),
     ("bitz_launch_count", ctypes.c_ulonglong, []),
+    ("bitz_resident_rounds", ctypes.c_int, []),
     ("bitz_system_witness", ctypes.c_int,
      [_vp, _vp, ctypes.c_size_t, _vp, ctypes.c_size_t, _vp, ctypes.c_size_t]),
     ("bitz_circuit_layout", ctypes.c_int,

@@ -122,6 +122,8 @@ void bitz_free(void *p) { free(p); }
 
 unsigned long long bitz_launch_count(void) { return launch_counter(); }
 
+int bitz_resident_rounds(void) { return resident_rounds_enabled() ? 1 : 0; }
+
 int bitz_system_witness(bitz_system *sys, uint32_t *f_words, size_t f_cap, uint32_t *h_words,
                         size_t h_cap, int64_t *products, size_t prod_cap) {
   if (!sys) return capi_fail(BZ_ERR_ARGUMENT, "null argument");

@@ -75,6 +75,17 @@ void RoundChannel::clear_down() {
   for (int k = 0; k < 2 * kMailboxWords; k++) s[k] = 0;
 }
 
+bool resident_rounds_enabled() {
+  static const bool on = [] {
+    const char *e = getenv("BITZ_RESIDENT_ROUNDS");
+    if (e && e[0] == '0') return false;
+    if (e && e[0] == '1') return true;
+    const char *inj = getenv("CUDA_INJECTION64_PATH");
+    return !(inj && inj[0]);
+  }();
+  return on;
+}
+
 // ------------------------------------------------------------ DeviceGate
 
 static thread_local int resident_depth = 0;

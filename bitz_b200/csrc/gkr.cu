@@ -662,13 +662,8 @@ f128 gkr_prove(int s, const f128 *zeta, uint32_t grind_bits, Transcript &ts, Gkr
   KernelProbe &probe = KernelProbe::get();
   RoundChannel *ch = sc.channel;
   bool tail = false;  // a tail kernel of this layer is resident and waiting
-  // BITZ_RESIDENT_ROUNDS=0 runs every round as its own launch (same results):
-  // a kernel profiler that serialises launches and holds the host thread at
-  // each one cannot run a kernel that waits for the host.
-  static const bool resident = [] {
-    const char *e = getenv("BITZ_RESIDENT_ROUNDS");
-    return !(e && e[0] == '0');
-  }();
+  // without resident rounds every round is its own launch (same results)
+  const bool resident = resident_rounds_enabled();
   // BITZ_ROUND_TRACE=1 prints the host time between consecutive round results
   static const bool trace = getenv("BITZ_ROUND_TRACE") != nullptr;
   auto t_prev = std::chrono::steady_clock::now();

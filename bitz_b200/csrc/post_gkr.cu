@@ -441,10 +441,7 @@ int post_gkr_prove(const PostGkrArgs &a, Transcript &ts, PostGkrScratch &sc, cud
   size_t len = n1;
   RoundChannel *ch = sc.channel;
   bool tail = false;  // pg_tail is resident and runs the remaining rounds
-  static const bool resident = [] {
-    const char *e = getenv("BITZ_RESIDENT_ROUNDS");
-    return !(e && e[0] == '0');
-  }();
+  const bool resident = resident_rounds_enabled();
   // Queued mode: the rounds above the tail are launched now behind the first
   // fold, then the tail. Loop iteration k folds at r_k (point_out[1 + k]),
   // which the host posts as downbox publication d0 + k; the kernel before

@@ -558,12 +558,8 @@ std::vector<uint8_t> ProofSystem::ligerito(cudaStream_t s, f128 target) {
     const PcsLevel &L = cfg.levels[i];
     std::vector<f128> rs;
     BZ_CUDA(cudaMemsetAsync(acc, 0, 8 * sizeof(unsigned long long) * (L.k + 1), s));
-    // BITZ_RESIDENT_ROUNDS=0 keeps every kernel that waits for the host off,
-    // as for the sumchecks (a kernel profiler cannot run one)
-    static const bool resident = [] {
-      const char *e = getenv("BITZ_RESIDENT_ROUNDS");
-      return !(e && e[0] == '0');
-    }();
+    // kernels that wait for the host follow the sumchecks' mode
+    const bool resident = resident_rounds_enabled();
     if (resident && lane_->resident_middle() && pg_mid_fits_folds(n, L.k)) {
       // the level's folds in one resident kernel: fold r takes its challenge
       // from the downbox and posts the next message itself

@@ -662,10 +662,7 @@ void spartan_prove(const SpartanArgs &a, Transcript &ts, SpartanScratch &sc, cud
   size_t len = R;
   fp r = fp_zero();
   RoundChannel *ch = sc.channel;
-  static const bool resident = [] {
-    const char *e = getenv("BITZ_RESIDENT_ROUNDS");
-    return !(e && e[0] == '0');
-  }();
+  const bool resident = resident_rounds_enabled();
   bool tail = false;  // a resident tail kernel runs the remaining rounds
   // no other thread's device allocation while a tail kernel waits for this one
   ResidentScope gate(ch && resident);

@@ -2,6 +2,8 @@
 import ctypes
 import os
 import re
+import subprocess
+import sys
 
 import bitz_b200
 from bitz_b200 import _lib
@@ -38,3 +40,27 @@ def test_errors_are_reported_not_raised():
     rc = lib.bitz_post_gkr_prove(None, 7, None, 0, None, None, 100, None, None, None)
     assert rc == 1
     assert b"null" in lib.bitz_last_error()
+
+
+def _resident_mode(env_updates):
+    env = {k: v for k, v in os.environ.items()
+           if k not in ("BITZ_RESIDENT_ROUNDS", "CUDA_INJECTION64_PATH")}
+    env.update(env_updates)
+    code = ("import ctypes, sys; lib = ctypes.CDLL(sys.argv[1]); "
+            "print(lib.bitz_resident_rounds())")
+    out = subprocess.run([sys.executable, "-c", code, _lib.LIB_PATH], env=env,
+                         capture_output=True, text=True, check=True)
+    return int(out.stdout.strip())
+
+
+def test_resident_rounds_follow_the_environment():
+    """Kernels that wait for the host are off under an injected CUDA tool
+    (a kernel profiler holds the host at each launch) unless forced on."""
+    assert _resident_mode({}) == 1
+    assert _resident_mode({"CUDA_INJECTION64_PATH": "/opt/tool/libinject.so"}) == 0
+    assert _resident_mode({"CUDA_INJECTION64_PATH": ""}) == 1
+    assert _resident_mode({"BITZ_RESIDENT_ROUNDS": "0"}) == 0
+    assert _resident_mode({"BITZ_RESIDENT_ROUNDS": "1",
+                           "CUDA_INJECTION64_PATH": "/opt/tool/libinject.so"}) == 1
+    assert _resident_mode({"BITZ_RESIDENT_ROUNDS": "0",
+                           "CUDA_INJECTION64_PATH": "/opt/tool/libinject.so"}) == 0
