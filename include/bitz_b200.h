@@ -70,16 +70,18 @@ int bitz_post_gkr_prove_dev(const uint64_t *rows_dev, int log_rows, const uint64
 
 /* The post-GKR sumcheck as bitz_post_gkr_prove_dev, allocating nothing.
  * No counterpart in the reference. For callers that cannot allocate device
- * memory: code running inside a CUDA graph capture (where cudaMalloc is not
- * allowed), processes whose device memory belongs to another allocator or to
- * a fixed budget set aside at start-up, and embedders that forbid allocation
- * on the request path. Inputs are device pointers, outputs host pointers;
+ * memory: processes whose device memory belongs to another allocator or to a
+ * fixed budget set aside at start-up, and embedders that forbid allocation on
+ * the request path. Inputs are device pointers, outputs host pointers;
  * stream may be NULL (the default stream). Its scratch is a fixed array in
  * the library's device memory (32 MiB on every GPU that loads the library,
  * held until the process exits), so log_rows + log_cols must be at most 20:
  * larger claims return BZ_ERR_SCRATCH. Every call shares that array: calls
- * that overlap on the GPU race, so serialise them. The first call on a
- * device looks up the array's address; make it before any stream capture. */
+ * that overlap on the GPU race, so serialise them. Each round copies its
+ * message to the host and synchronises the stream (the host transcript draws
+ * the next challenge), so the call cannot run while a stream is being
+ * captured. The first call on a device (and the first after the device's
+ * context was reset) looks up the array's address. */
 int bitz_post_gkr_prove_noalloc(const uint64_t *rows_dev, int log_rows, const uint64_t *cols_dev,
                                 int log_cols, const uint64_t target[2], const uint64_t *packed_dev,
                                 uint32_t security_bits, bitz_transcript *t, void *stream,
@@ -134,6 +136,13 @@ void bitz_free(void *p);
 /* Diagnostic (no reference counterpart): kernel launches issued by this
  * library since the process started. */
 unsigned long long bitz_launch_count(void);
+/* Diagnostic (no reference counterpart): 1 when kernels that wait for the
+ * host thread (resident and queued sumcheck rounds) are in use, 0 when every
+ * round is its own launch. BITZ_RESIDENT_ROUNDS=0/1 forces the mode; unset,
+ * it is off when a CUDA injection tool (a kernel profiler or sanitizer) is
+ * attached, since such a tool holds the host at every launch. Proof bytes are
+ * the same in both modes. Needs no GPU. */
+int bitz_resident_rounds(void);
 /* Diagnostic (no reference counterpart): the last proof's packed witness f,
  * packed h = M (1 || f) and the exact products (A h, B h, C h per row). */
 int bitz_system_witness(bitz_system *sys, uint32_t *f_words, size_t f_cap, uint32_t *h_words,

@@ -33,6 +33,9 @@ _SIGS = [
      [ctypes.POINTER(ctypes.c_uint32), ctypes.POINTER(ctypes.c_uint32), ctypes.c_size_t, _u64p,
       ctypes.c_int, _u64p, _u64p]),
     ("o_set_clmul_mode", None, [ctypes.c_int]),
+    ("o_blake3", None, [ctypes.c_char_p, ctypes.c_size_t, ctypes.c_char_p]),
+    ("o_blake3_derive_key", None,
+     [ctypes.c_char_p, ctypes.c_char_p, ctypes.c_size_t, ctypes.c_size_t, ctypes.c_char_p]),
 ]
 
 _lib = None

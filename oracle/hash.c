@@ -294,3 +294,14 @@ void o_blake3(const uint8_t *in, size_t len, uint8_t out[32]) {
   o_blake3_update(&h, in, len);
   o_blake3_final(&h, out);
 }
+
+/* Derive-key mode over `in`, fed in pieces of `piece` bytes (0: in one
+ * update), so the streaming state is exercised at every split. */
+void o_blake3_derive_key(const char *context, const uint8_t *in, size_t len, size_t piece,
+                         uint8_t out[32]) {
+  o_blake3_state h;
+  o_blake3_init_derive_key(&h, context);
+  if (!piece) piece = len ? len : 1;
+  for (size_t i = 0; i < len; i += piece) o_blake3_update(&h, in + i, len - i < piece ? len - i : piece);
+  o_blake3_final(&h, out);
+}

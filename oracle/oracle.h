@@ -89,6 +89,8 @@ void o_blake3_init_derive_key(o_blake3_state *h, const char *context);
 void o_blake3_update(o_blake3_state *h, const uint8_t *in, size_t len);
 void o_blake3_final(const o_blake3_state *h, uint8_t out[32]);
 void o_blake3(const uint8_t *in, size_t len, uint8_t out[32]);
+void o_blake3_derive_key(const char *context, const uint8_t *in, size_t len, size_t piece,
+                         uint8_t out[32]);
 
 /* -------------------------------------------------------------- transcript
  * crates/transcript/src/{domain,prover,pow,challenge}.rs over a Keccak duplex

@@ -50,7 +50,9 @@ def aes_block(key, block):
 
 
 def main():
-    ref = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+    if len(sys.argv) != 2:
+        sys.exit("usage: make_ghash_fixture.py <path to the reference tree>")
+    ref = sys.argv[1]
     path = os.path.join(ref, "crates/field/tests/vectors/gcm_encrypt_128.rsp")
     cases = parse(open(path).read())
     assert len(cases) == 525, len(cases)

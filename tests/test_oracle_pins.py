@@ -3,7 +3,9 @@
 - GF(2^128): the NIST CAVP GCM vectors the reference ships
   (crates/field/tests/ghash_vectors.rs), via tests/golden/ghash_nist.json.
 - SHA-256 / SHA3-256 (Keccak-f): Python hashlib; FIPS 180-4 "abc".
-- BLAKE3: the published digests of "" and "abc".
+- BLAKE3: the published digests of "" and "abc"; hash and derive-key mode
+  over 0 bytes to 100 chunks from the BLAKE3 team's implementation, via
+  tests/golden/blake3_vectors.json.
 - The narg layout of the reference's golden transcript (crates/transcript/tests/golden.rs:14).
 """
 import ctypes
@@ -92,6 +94,43 @@ def test_blake3_published_digests():
     assert buf.raw.hex() == "af1349b9f5f9a1a6a0404dea36dcc9499bcb25c9adc112b7cc9a93cae41f3262"
     of.lib().o_blake3(b"abc", 3, buf)
     assert buf.raw.hex() == "6437b3ac38465133ffb63b75273a8db548c558465d79db03fd359c6cd5bd9d85"
+
+
+def _blake3_vectors():
+    import json
+    path = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "blake3_vectors.json")
+    return json.load(open(path))
+
+
+def _blake3_input(n):
+    return bytes(i % 251 for i in range(n))
+
+
+def test_blake3_tree_mode_known_answers():
+    """Hash mode from 0 bytes to 100 chunks: every chunk boundary and parent
+    merge of the chunk tree (fixture: tests/golden/make_blake3_fixture.py)."""
+    vec = _blake3_vectors()
+    buf = ctypes.create_string_buffer(32)
+    for case in vec["cases"]:
+        x = _blake3_input(case["len"])
+        of.lib().o_blake3(x, len(x), buf)
+        assert buf.raw.hex() == case["hash"], case["len"]
+
+
+def test_blake3_derive_key_known_answers():
+    """Derive-key mode (the weight digest's, crates/pcs/src/opening.rs:354-365)
+    for the path's context and the test-vector context, fed whole and in
+    uneven pieces."""
+    vec = _blake3_vectors()
+    buf = ctypes.create_string_buffer(32)
+    for case in vec["cases"]:
+        x = _blake3_input(case["len"])
+        for ctx in vec["contexts"]:
+            for piece in (0, 1, 63, 1000, 4096):
+                if piece == 1 and case["len"] > 8192:
+                    continue
+                of.lib().o_blake3_derive_key(ctx.encode(), x, len(x), piece, buf)
+                assert buf.raw.hex() == case["derive_key"][ctx], (case["len"], ctx, piece)
 
 
 def test_golden_transcript_narg_layout():
