@@ -5,7 +5,9 @@
  * public messages absorbed only, hints written beside the sponge. The sponge
  * is a Keccak-f[1600] duplex with a 136-byte rate standing in for spongefish
  * 0.7.4's std sponge, whose source is not in the reference tree: its exact
- * byte framing is parity unpinned. */
+ * byte framing is parity unpinned. The narg and hint bytes of the reference's
+ * golden transcript (crates/transcript/tests/golden.rs:14-15) are reproduced;
+ * its two challenges (:16-17) are not. */
 #include <stdlib.h>
 #include <string.h>
 

@@ -133,15 +133,39 @@ def test_blake3_derive_key_known_answers():
                 assert buf.raw.hex() == case["derive_key"][ctx], (case["len"], ctx, piece)
 
 
-def test_golden_transcript_narg_layout():
-    """crates/transcript/tests/golden.rs:7-38: the narg string is the F128 message
-    (16 B LE, lo then hi) then the Fq message (16 B LE canonical); the hint stays out.
-    The challenges C1/C2 depend on spongefish's byte framing, which is not in the
-    reference tree: they are parity unpinned."""
-    t = of.Transcript(b"golden-session", b"golden-instance")
+GOLDEN_C1 = "1d1bcda36aa1541c3752f7b23fedef81"
+GOLDEN_C2 = "e80729d4aa76e8e4d28dd085143eb3d5"
+
+
+def _golden_events(t):
+    """The event sequence of crates/transcript/tests/golden.rs:22-30 (the hint
+    goes to the hint stream, not the sponge); returns (c1, c2) as bytes."""
     msg = (0x0123456789ABCDEF).to_bytes(8, "little") + (0xFEDCBA9876543210).to_bytes(8, "little")
     t.prover_message(msg)
-    t.verifier_message_f128()
+    c1 = t.verifier_message_f128()
     t.prover_message((12345).to_bytes(16, "little"))
-    t.verifier_message_f128()
+    c2 = t.verifier_message_f128()
+    as_bytes = lambda c: int(c[0]).to_bytes(8, "little") + int(c[1]).to_bytes(8, "little")
+    return as_bytes(c1), as_bytes(c2)
+
+
+def test_golden_transcript_narg_layout():
+    """crates/transcript/tests/golden.rs:7-38: the narg string is the F128 message
+    (16 B LE, lo then hi) then the Fq message (16 B LE canonical); the hint stays out."""
+    t = of.Transcript(b"golden-session", b"golden-instance")
+    _golden_events(t)
     assert t.narg().hex() == "efcdab89674523011032547698badcfe39300000000000000000000000000000"
+
+
+@pytest.mark.xfail(strict=True, reason=(
+    "golden challenges NOT reproduced: spongefish 0.7.4 (its DomainSeparator, protocol_id, "
+    "session/instance absorption and duplex rules) is not in the reference tree, and no "
+    "candidate framing searched reproduces C1"))
+def test_golden_transcript_challenges():
+    """crates/transcript/tests/golden.rs:16-17 pins the two squeezed challenges.
+    The sponge here is a Keccak-f[1600] duplex (rate 136) framed from the
+    reference's own description; this test states the pin and records that it
+    is not met."""
+    c1, c2 = _golden_events(of.Transcript(b"golden-session", b"golden-instance"))
+    assert c1.hex() == GOLDEN_C1
+    assert c2.hex() == GOLDEN_C2

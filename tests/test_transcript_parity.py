@@ -118,3 +118,23 @@ def test_scalar_host_paths_agree_too():
          "-k", "grinding or prime"],
         env=env, capture_output=True, text=True, timeout=600)
     assert r.returncode == 0, r.stdout[-2000:] + r.stderr[-2000:]
+
+
+def test_golden_event_sequence_agrees():
+    """The reference's golden event sequence (crates/transcript/tests/golden.rs:22-30)
+    gives the same narg, hints and challenges through the product's transcript
+    as through the oracle's (whose golden-challenge pin is recorded as not met
+    in test_oracle_pins.py)."""
+    msg = (0x0123456789ABCDEF).to_bytes(8, "little") + (0xFEDCBA9876543210).to_bytes(8, "little")
+    p = bz.build_prover(b"golden-session", b"golden-instance")
+    o = of.Transcript(b"golden-session", b"golden-instance")
+    for t in (p, o):
+        t.prover_message(msg)
+    assert np.array_equal(p.verifier_message_f128(), o.verifier_message_f128())
+    p.hint(b"\xaa" * 5)
+    for t in (p, o):
+        t.prover_message((12345).to_bytes(16, "little"))
+    assert np.array_equal(p.verifier_message_f128(), o.verifier_message_f128())
+    assert p.narg() == o.narg()
+    assert p.narg().hex() == "efcdab89674523011032547698badcfe39300000000000000000000000000000"
+    assert p.hints().hex() == "aaaaaaaaaa"
