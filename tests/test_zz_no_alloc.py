@@ -1,8 +1,9 @@
 """The allocation-free post-GKR entry point against the allocating one.
 
 bitz_post_gkr_prove_noalloc serves callers that cannot allocate device memory
-(graph capture, a fixed memory budget owned elsewhere): it runs the same
-sumcheck on a fixed device array inside the library. It must give the same
+(a fixed memory budget owned by another allocator, a request path that must not
+allocate): it runs the same sumcheck on a fixed device array inside the
+library. It must give the same
 point, value and transcript bytes as bitz_post_gkr_prove, on consecutive calls
 that reuse the same array. This file is collected last on purpose.
 """
@@ -68,3 +69,40 @@ def test_noalloc_rejects_claims_beyond_its_scratch():
     rc, _, _ = _noalloc(rows, cols, packed, target, 100, bz.build_prover(b"s", b"i"))
     assert rc == 7  # BZ_ERR_SCRATCH
     assert b"at most 20" in _lib.load().bitz_last_error()
+
+
+def test_noalloc_takes_no_device_memory():
+    """After a warm-up call, a second call leaves the device's free memory as
+    it was: nothing is allocated on the request path."""
+    import torch
+    rows, cols, packed, target = _claim(11, 14, 3)
+    d_rows = torch.from_numpy(rows.view(np.int64)).cuda()
+    d_cols = torch.from_numpy(cols.view(np.int64)).cuda()
+    d_packed = torch.from_numpy(packed.view(np.int64)).cuda()
+    lib = _lib.load()
+    tgt = np.ascontiguousarray(target, dtype=np.uint64)
+    results = []
+
+    def call():
+        ts = bz.build_prover(b"no-alloc", b"memory")
+        point = np.zeros((17, 2), dtype=np.uint64)
+        value = np.zeros(2, dtype=np.uint64)
+        rc = lib.bitz_post_gkr_prove_noalloc(
+            ctypes.c_void_p(d_rows.data_ptr()), 14, ctypes.c_void_p(d_cols.data_ptr()), 3,
+            tgt.ctypes.data_as(_u64p), ctypes.c_void_p(d_packed.data_ptr()), 100, ts.handle,
+            None, point.ctypes.data_as(_u64p), value.ctypes.data_as(_u64p))
+        assert rc == 0, lib.bitz_last_error()
+        results.append((point.copy(), value.copy(), ts.narg()))
+
+    torch.cuda.synchronize()
+    call()  # warm-up: loads the kernels and sets up the array's address
+    torch.cuda.synchronize()
+    torch.cuda.empty_cache()
+    free_before, _ = torch.cuda.mem_get_info()
+    call()
+    torch.cuda.synchronize()
+    free_after, _ = torch.cuda.mem_get_info()
+    assert free_after == free_before
+    assert np.array_equal(results[0][0], results[1][0])
+    assert np.array_equal(results[0][1], results[1][1])
+    assert results[0][2] == results[1][2]
