@@ -19,8 +19,9 @@ import numpy as np
 from . import _lib
 
 __all__ = ["BitzError", "ProverState", "build_prover", "post_gkr_prove", "gkr_prove",
-           "gkr_outputs", "device_count", "CircuitProofSystem", "batch_prove", "ProveServer",
-           "probe_kernel", "probe_read", "l2_flush"]
+           "gkr_outputs", "device_count", "CircuitProofSystem", "Witness", "CommittedWitness",
+           "wire_decode", "batch_prove", "ProveServer", "probe_kernel", "probe_read", "probe_kernels", "gf_peak",
+           "l2_flush"]
 
 _ERRORS = {
     1: "ArgumentError", 2: "ClaimDoesNotHold", 3: "Unsatisfied", 4: "Configuration",
@@ -60,6 +61,14 @@ def set_device(device: int):
 
 def launch_count() -> int:
     return int(_lib.load().bitz_launch_count())
+
+
+def round_wait_stats():
+    """(seconds the host has waited for round results on the default lane,
+    number of waits) since the process started."""
+    out = (ctypes.c_ulonglong * 2)()
+    _check(_lib.load().bitz_round_wait_stats(out))
+    return out[0] * 1e-9, int(out[1])
 
 
 class ProverState:
@@ -187,12 +196,24 @@ class CircuitProofSystem:
                 "prime_bits", "pcs_security", "claim_log_cols", "compressions"]
         return dict(zip(keys, (int(x) for x in out)))
 
-    def prove(self, restage: bool = True):
-        """witness + commit + prove; returns (proof bytes, times in ms).
+    def prove(self, witness=None, commitment=None, restage: bool = True):
+        """Returns (proof bytes, times in ms).
 
-        restage=False reuses the statement staged on the device at creation."""
+        Without arguments: witness + commit + prove in one call (restage=False
+        reuses the statement staged on the device at creation). With a
+        Witness and its CommittedWitness (from ``witness`` and ``commit``):
+        the prove stage alone, consuming both (end_to_end.rs:260); the times
+        are then empty."""
         p = ctypes.POINTER(ctypes.c_uint8)()
         n = ctypes.c_size_t(0)
+        if witness is not None or commitment is not None:
+            if witness is None or commitment is None:
+                raise BitzError(1, "prove takes both the witness and its commitment")
+            wh, ch = witness._take(), commitment._take()
+            _check(self._lib.bitz_prove(self._h, wh, ch, ctypes.byref(p), ctypes.byref(n)))
+            data = ctypes.string_at(p, n.value)
+            self._lib.bitz_free(p)
+            return data, {}
         times = (ctypes.c_double * 4)()
         _check(self._lib.bitz_system_prove_ex(self._h, int(restage), ctypes.byref(p),
                                               ctypes.byref(n), times))
@@ -201,13 +222,81 @@ class CircuitProofSystem:
         return data, {"witness_ms": times[0], "commit_ms": times[1], "prove_ms": times[2],
                       "device_ms": times[3]}
 
-    def witness(self, f_words: int, h_words: int, rows: int):
+    def witness(self, inputs):
+        """CircuitProofSystem::witness (end_to_end.rs:215): the witness of
+        ``inputs`` (0/1 per input bit), kept on the device."""
+        inp = np.ascontiguousarray(inputs, dtype=np.uint8)
+        h = ctypes.c_void_p()
+        _check(self._lib.bitz_witness(self._h, inp.ctypes.data, inp.size, ctypes.byref(h)))
+        return Witness(self._lib, h)
+
+    def commit(self, witness):
+        """CircuitProofSystem::commit (end_to_end.rs:248): commits the witness."""
+        h = ctypes.c_void_p()
+        _check(self._lib.bitz_commit(self._h, witness._handle(), ctypes.byref(h)))
+        return CommittedWitness(self._lib, h)
+
+    def verify(self, proof: bytes):
+        """CircuitProofSystem::verify (end_to_end.rs:339-377) by this library's
+        verifier; raises BitzError (MalformedProof or VerifyError, naming the
+        failed check) unless the proof is accepted."""
+        buf = (ctypes.c_uint8 * max(len(proof), 1)).from_buffer_copy(proof or b"\0")
+        _check(self._lib.bitz_verify(self._h, buf, len(proof)))
+
+    def witness_parts(self, f_words: int, h_words: int, rows: int):
         f = np.zeros(f_words, dtype=np.uint32)
         h = np.zeros(h_words, dtype=np.uint32)
         pr = np.zeros(3 * rows, dtype=np.int64)
         _check(self._lib.bitz_system_witness(self._h, f.ctypes.data, f.size, h.ctypes.data, h.size,
                                              pr.ctypes.data, pr.size))
         return f, h, pr
+
+
+class _StagedHandle:
+    """A witness or commitment held on the device between the staged calls."""
+
+    _free = None
+
+    def __init__(self, lib, h):
+        self._lib = lib
+        self._h = h
+
+    def _handle(self):
+        if not self._h:
+            raise BitzError(1, "the handle was already consumed")
+        return self._h
+
+    def _take(self):
+        h = self._handle()
+        self._h = None
+        return h
+
+    def __del__(self):
+        if getattr(self, "_h", None):
+            getattr(self._lib, self._free)(self._h)
+            self._h = None
+
+
+class Witness(_StagedHandle):
+    """CircuitProofSystem::witness's result (end_to_end.rs:215-243)."""
+    _free = "bitz_witness_free"
+
+
+class CommittedWitness(_StagedHandle):
+    """CircuitProofSystem::commit's result (end_to_end.rs:248-255)."""
+    _free = "bitz_committed_witness_free"
+
+
+def wire_decode(data: bytes):
+    """WireProof::from_bytes (crates/host/src/wire_proof.rs:109-140): returns
+    (narg bytes, hint bytes); raises BitzError (MalformedProof) naming the
+    reference's decoding error."""
+    out = np.zeros(4, dtype=np.uint64)
+    buf = (ctypes.c_uint8 * max(len(data), 1)).from_buffer_copy(data or b"\0")
+    _check(_lib.load().bitz_wire_decode(buf, len(data),
+                                        out.ctypes.data_as(ctypes.POINTER(ctypes.c_uint64))))
+    a, n, b, h = (int(x) for x in out)
+    return data[a:a + n], data[b:b + h]
 
 
 def gkr_outputs(row_images, columns):
@@ -297,16 +386,39 @@ class ProveServer:
             pass
 
 
-def probe_kernel(name):
-    """Times every launch of kernel ``name`` with CUDA events (None: off)."""
-    _check(_lib.load().bitz_probe_kernel(name.encode() if name else None))
+def probe_kernel(spec):
+    """Times every launch of the probed kernels with CUDA events: None turns
+    the probe off, "*" probes every instrumented kernel, else a
+    comma-separated list of names. While on, every round is its own launch."""
+    _check(_lib.load().bitz_probe_kernel(spec.encode() if spec else None))
 
 
-def probe_read():
-    """(total ms, total algorithmic bytes, launches) of the probed kernel."""
-    ms, b, n = ctypes.c_double(0), ctypes.c_double(0), ctypes.c_ulonglong(0)
-    _check(_lib.load().bitz_probe_read(ctypes.byref(ms), ctypes.byref(b), ctypes.byref(n)))
-    return ms.value, b.value, n.value
+def probe_read(kernel):
+    """One probed kernel's totals: ms, algorithmic bytes, GF(2^128) products
+    (gmuls reduced, wides unreduced, tables by the round challenge through its
+    window table) and launches."""
+    out = (ctypes.c_double * 5)()
+    n = ctypes.c_ulonglong(0)
+    _check(_lib.load().bitz_probe_read(kernel.encode(), out, ctypes.byref(n)))
+    return {"ms": out[0], "bytes": out[1], "gmuls": out[2], "wides": out[3], "tables": out[4],
+            "launches": n.value}
+
+
+def probe_kernels():
+    """Names of the probed kernels that launched since the probe was enabled."""
+    lib = _lib.load()
+    n = lib.bitz_probe_kernels(None, 0)
+    buf = ctypes.create_string_buffer(n + 1)
+    lib.bitz_probe_kernels(buf, n + 1)
+    return [x for x in buf.value.decode().split(",") if x]
+
+
+def gf_peak(kind: int) -> float:
+    """Measured GF(2^128) products per second on this GPU: kind 0 reduced, 1
+    unreduced (wide), 2 through a window table."""
+    v = ctypes.c_double(0)
+    _check(_lib.load().bitz_diag_gf_peak(kind, ctypes.byref(v)))
+    return v.value
 
 
 def l2_flush():

@@ -49,8 +49,18 @@ SIGNATURES = [
      [_vp, ctypes.c_int, ctypes.POINTER(_u8p), ctypes.POINTER(ctypes.c_size_t),
       ctypes.POINTER(ctypes.c_double)]),
     ("bitz_free", None, [_vp]),
+    ("bitz_witness", ctypes.c_int, [_vp, _vp, ctypes.c_size_t, ctypes.POINTER(_vp)]),
+    ("bitz_commit", ctypes.c_int, [_vp, _vp, ctypes.POINTER(_vp)]),
+    ("bitz_prove", ctypes.c_int,
+     [_vp, _vp, _vp, ctypes.POINTER(_u8p), ctypes.POINTER(ctypes.c_size_t)]),
+    ("bitz_witness_free", None, [_vp]),
+    ("bitz_verify", ctypes.c_int, [_vp, _vp, ctypes.c_size_t]),
+    ("bitz_wire_decode", ctypes.c_int, [_vp, ctypes.c_size_t, _u64p]),
+    ("bitz_blake3", ctypes.c_int, [ctypes.c_char_p, ctypes.c_char_p, ctypes.c_size_t, _u8p]),
+    ("bitz_committed_witness_free", None, [_vp]),
     ("bitz_launch_count", ctypes.c_ulonglong, []),
     ("bitz_resident_rounds", ctypes.c_int, []),
+    ("bitz_round_wait_stats", ctypes.c_int, [ctypes.POINTER(ctypes.c_ulonglong)]),
     ("bitz_system_witness", ctypes.c_int,
      [_vp, _vp, ctypes.c_size_t, _vp, ctypes.c_size_t, _vp, ctypes.c_size_t]),
     ("bitz_circuit_layout", ctypes.c_int,
@@ -69,9 +79,10 @@ SIGNATURES = [
     ("bitz_server_stop", ctypes.c_int, [_vp]),
     ("bitz_probe_kernel", ctypes.c_int, [ctypes.c_char_p]),
     ("bitz_probe_read", ctypes.c_int,
-     [ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double),
-      ctypes.POINTER(ctypes.c_ulonglong)]),
+     [ctypes.c_char_p, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_ulonglong)]),
+    ("bitz_probe_kernels", ctypes.c_size_t, [ctypes.c_char_p, ctypes.c_size_t]),
     ("bitz_l2_flush", ctypes.c_int, []),
+    ("bitz_diag_gf_peak", ctypes.c_int, [ctypes.c_int, ctypes.POINTER(ctypes.c_double)]),
     ("bitz_diag_round_trip", ctypes.c_int,
      [ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_double)]),
 ]

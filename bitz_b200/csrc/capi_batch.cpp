@@ -34,6 +34,7 @@ int capi_fail(int code, const std::string &msg);
 int check_statement(int circuit_kind, const uint8_t *input_bits, size_t n_inputs,
                     const uint8_t *output_bits, uint32_t security_bits);
 double diag_round_trip(int mode, int rounds);
+double diag_gf_peak(int kind, int blocks_per_sm);
 
 namespace {
 
@@ -96,6 +97,20 @@ uint8_t *copy_out(const std::vector<uint8_t> &p) {
 }
 
 }  // namespace
+
+// One lane from the pool for a caller that holds it across calls (the staged
+// witness/commit/prove calls), and its return.
+std::unique_ptr<Context> take_lane(int device) {
+  auto v = LanePool::get().take(device, 1);
+  return std::move(v[0]);
+}
+
+void give_lane(int device, std::unique_ptr<Context> lane) {
+  std::vector<std::unique_ptr<Context>> v;
+  v.push_back(std::move(lane));
+  LanePool::get().give(device, v);
+}
+
 }  // namespace bz
 
 using namespace bz;
@@ -389,13 +404,30 @@ int bitz_probe_kernel(const char *name) {
   }
 }
 
-int bitz_probe_read(double *ms_total, double *bytes_total, unsigned long long *launches) {
+int bitz_probe_read(const char *kernel, double out[5], unsigned long long *launches) {
+  if (!kernel || !out) return capi_fail(BZ_ERR_ARGUMENT, "null argument");
   try {
     KernelProbe::get().collect();
-    KernelProbe::get().read(ms_total, bytes_total, launches);
+    KernelProbe::get().read(kernel, out, launches);
     return BZ_OK;
   } catch (const std::exception &e) {
     return capi_fail(BZ_ERR_CUDA, e.what());
+  }
+}
+
+size_t bitz_probe_kernels(char *out, size_t cap) {
+  try {
+    KernelProbe::get().collect();
+    const std::string n = KernelProbe::get().names();
+    if (out && cap) {
+      const size_t k = std::min(cap - 1, n.size());
+      memcpy(out, n.data(), k);
+      out[k] = 0;
+    }
+    return n.size();
+  } catch (const std::exception &e) {
+    capi_fail(BZ_ERR_CUDA, e.what());
+    return 0;
   }
 }
 
@@ -404,6 +436,16 @@ int bitz_diag_round_trip(int mode, int rounds, double *us_per_round) {
     return capi_fail(BZ_ERR_ARGUMENT, "bad argument");
   try {
     *us_per_round = diag_round_trip(mode, rounds);
+    return BZ_OK;
+  } catch (const std::exception &e) {
+    return capi_fail(BZ_ERR_CUDA, e.what());
+  }
+}
+
+int bitz_diag_gf_peak(int kind, double *products_per_s) {
+  if (!products_per_s || kind < 0 || kind > 2) return capi_fail(BZ_ERR_ARGUMENT, "bad argument");
+  try {
+    *products_per_s = diag_gf_peak(kind, 4);
     return BZ_OK;
   } catch (const std::exception &e) {
     return capi_fail(BZ_ERR_CUDA, e.what());

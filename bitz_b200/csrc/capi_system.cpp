@@ -98,7 +98,8 @@ int bitz_system_prove_ex(bitz_system *sys, int restage, uint8_t **proof, size_t 
   try {
     std::vector<uint8_t> p;
     StageTimes t;
-    int rc = sys->ps->prove(p, &t, restage != 0);
+    LaneLease lease;  // the default lane unless a staged proof holds it
+    int rc = sys->ps->prove(p, &t, restage != 0, lease.lane());
     if (rc) return capi_fail(rc, sys->ps->error);
     *proof = (uint8_t *)malloc(p.size());
     if (!*proof) return capi_fail(BZ_ERR_INTERNAL, "out of host memory");
@@ -123,6 +124,18 @@ void bitz_free(void *p) { free(p); }
 unsigned long long bitz_launch_count(void) { return launch_counter(); }
 
 int bitz_resident_rounds(void) { return resident_rounds_enabled() ? 1 : 0; }
+
+int bitz_round_wait_stats(unsigned long long out[2]) {
+  if (!out) return capi_fail(BZ_ERR_ARGUMENT, "null argument");
+  try {
+    RoundChannel *ch = Context::get().channel();
+    out[0] = ch->wait_ns;
+    out[1] = ch->waits;
+    return BZ_OK;
+  } catch (const std::exception &e) {
+    return capi_fail(BZ_ERR_CUDA, e.what());
+  }
+}
 
 int bitz_system_witness(bitz_system *sys, uint32_t *f_words, size_t f_cap, uint32_t *h_words,
                         size_t h_cap, int64_t *products, size_t prod_cap) {

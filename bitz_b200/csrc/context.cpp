@@ -83,7 +83,8 @@ bool resident_rounds_enabled() {
     const char *inj = getenv("CUDA_INJECTION64_PATH");
     return !(inj && inj[0]);
   }();
-  return on;
+  // probed launches are timed one by one, each its own round
+  return on && !KernelProbe::get().active();
 }
 
 // ------------------------------------------------------------ DeviceGate
@@ -208,18 +209,35 @@ KernelProbe &KernelProbe::get() {
   return *p;
 }
 
-void KernelProbe::enable(const char *name) {
+void KernelProbe::enable(const char *spec) {
   std::lock_guard<std::mutex> lk(mu_);
-  target_ = name ? name : "";
-  active_ = !target_.empty();
-  ms_ = bytes_ = 0;
-  launches_ = 0;
+  const std::string sp = spec ? spec : "";
+  targets_.clear();
+  size_t at = 0;
+  while (at <= sp.size() && !sp.empty()) {
+    size_t comma = sp.find(',', at);
+    if (comma == std::string::npos) comma = sp.size();
+    if (comma > at) targets_.push_back(sp.substr(at, comma - at));
+    at = comma + 1;
+  }
+  all_ = sp == "*";
+  active_ = !targets_.empty();
+  totals_.clear();
   used_ = 0;
-  pending_bytes_.clear();
+  pending_.clear();
   if (active_ && ev_.empty()) {
     ev_.resize(2 * 4096);
     for (auto &e : ev_) BZ_CUDA(cudaEventCreate(&e));
   }
+}
+
+bool KernelProbe::on(const char *name) const {
+  if (!active_) return false;
+  if (all_) return true;
+  std::lock_guard<std::mutex> lk(mu_);
+  for (const auto &t : targets_)
+    if (t == name) return true;
+  return false;
 }
 
 void KernelProbe::before(cudaStream_t s) {
@@ -228,10 +246,11 @@ void KernelProbe::before(cudaStream_t s) {
   BZ_CUDA(cudaEventRecord(ev_[2 * used_], s));
 }
 
-void KernelProbe::after(cudaStream_t s, double bytes) {
+void KernelProbe::after(cudaStream_t s, const char *name, double bytes, double gmuls,
+                        double wides, double tables) {
   std::lock_guard<std::mutex> lk(mu_);
   BZ_CUDA(cudaEventRecord(ev_[2 * used_ + 1], s));
-  pending_bytes_.push_back(bytes);
+  pending_.push_back(Pending{name, {bytes, gmuls, wides, tables}});
   used_++;
 }
 
@@ -245,19 +264,32 @@ void KernelProbe::collect_locked_full() {
     BZ_CUDA(cudaEventSynchronize(ev_[2 * i + 1]));
     float ms = 0;
     BZ_CUDA(cudaEventElapsedTime(&ms, ev_[2 * i], ev_[2 * i + 1]));
-    ms_ += ms;
-    bytes_ += pending_bytes_[i];
-    launches_++;
+    Totals &t = totals_[pending_[i].name];
+    t.v[0] += ms;
+    for (int k = 0; k < 4; k++) t.v[1 + k] += pending_[i].work[k];
+    t.launches++;
   }
   used_ = 0;
-  pending_bytes_.clear();
+  pending_.clear();
 }
 
-void KernelProbe::read(double *ms, double *bytes, unsigned long long *launches) {
+void KernelProbe::read(const char *name, double out[5], unsigned long long *launches) {
   std::lock_guard<std::mutex> lk(mu_);
-  if (ms) *ms = ms_;
-  if (bytes) *bytes = bytes_;
-  if (launches) *launches = launches_;
+  Totals t;
+  auto it = totals_.find(name ? name : "");
+  if (it != totals_.end()) t = it->second;
+  for (int k = 0; k < 5; k++) out[k] = t.v[k];
+  if (launches) *launches = t.launches;
+}
+
+std::string KernelProbe::names() {
+  std::lock_guard<std::mutex> lk(mu_);
+  std::string out;
+  for (const auto &kv : totals_) {
+    if (!out.empty()) out += ",";
+    out += kv.first;
+  }
+  return out;
 }
 
 }  // namespace bz

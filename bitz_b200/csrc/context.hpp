@@ -3,6 +3,7 @@
 #pragma once
 #include <cuda_runtime.h>
 
+#include <map>
 #include <memory>
 #include <mutex>
 #include <string>
@@ -161,30 +162,68 @@ class Context {
   DeviceBuffer<unsigned int> counter_;
 };
 
-// Optional CUDA-event timing of every launch of one named kernel, with the
-// algorithmic bytes each launch moves (a measurement aid; off by default).
-// Events are recorded on the launching stream; totals are collected once the
-// stream has synchronised.
+// A lane held for one proof: the process's default lane when no other proof
+// holds it, else one from the process's lane pool (given back when the lease
+// ends). Defined with the C ABI (capi_stages.cpp).
+class LaneLease {
+ public:
+  LaneLease();
+  ~LaneLease();
+  LaneLease(const LaneLease &) = delete;
+  LaneLease &operator=(const LaneLease &) = delete;
+  Context *lane() const { return lane_; }
+
+ private:
+  Context *lane_ = nullptr;
+  std::unique_ptr<Context> pool_;
+  int device_ = 0;
+  bool default_ = false;
+};
+
+// Optional CUDA-event timing of every launch of the probed kernels, with the
+// algorithmic bytes each launch moves and the GF(2^128) products it computes
+// (a measurement aid; off by default). Events are recorded on the launching
+// stream; totals are collected once the stream has synchronised. While the
+// probe is on, every sumcheck round runs as its own launch (as under a kernel
+// profiler), so each probed launch is timed alone.
 class KernelProbe {
  public:
   static KernelProbe &get();
-  void enable(const char *name);  // null or "" turns the probe off
-  bool on(const char *name) const { return active_ && target_ == name; }
+  // "" or null: off; "*": every probed launch site; else a comma-separated
+  // list of kernel names. Enabling resets the totals.
+  void enable(const char *spec);
+  bool active() const { return active_; }
+  bool on(const char *name) const;
   void before(cudaStream_t s);
-  void after(cudaStream_t s, double bytes);
+  // GF(2^128) products of the launch: `gmuls` reduced general products,
+  // `wides` unreduced ones (reduced once per sum), `tables` products by one
+  // fixed factor (the round's challenge) through its window table
+  void after(cudaStream_t s, const char *name, double bytes, double gmuls = 0, double wides = 0,
+             double tables = 0);
   void collect();  // adds the finished launches' times to the totals
-  void read(double *ms, double *bytes, unsigned long long *launches);
+  // Totals of one kernel (zeros if it never ran).
+  // out: ms, bytes, gmuls, wides, tables
+  void read(const char *name, double out[5], unsigned long long *launches);
+  // Names of the kernels with at least one collected launch, comma-separated.
+  std::string names();
 
  private:
+  struct Totals {
+    double v[5] = {0, 0, 0, 0, 0};  // ms, bytes, gmuls, wides, tables
+    unsigned long long launches = 0;
+  };
+  struct Pending {
+    std::string name;
+    double work[4];  // bytes, gmuls, wides, tables
+  };
   void collect_locked_full();
-  std::mutex mu_;
-  bool active_ = false;
-  std::string target_;
+  mutable std::mutex mu_;
+  bool active_ = false, all_ = false;
+  std::vector<std::string> targets_;
   std::vector<cudaEvent_t> ev_;
-  std::vector<double> pending_bytes_;
+  std::vector<Pending> pending_;
   size_t used_ = 0;
-  double ms_ = 0, bytes_ = 0;
-  unsigned long long launches_ = 0;
+  std::map<std::string, Totals> totals_;
 };
 
 }  // namespace bz

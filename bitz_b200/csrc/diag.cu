@@ -62,4 +62,74 @@ double diag_round_trip(int mode, int rounds) {
   return us / rounds;
 }
 
+// The GPU's GF(2^128) product throughput, the ceiling of the integer-bound
+// kernels: every thread runs kChains independent chains of `iters` products
+// of one kind (0 reduced general products, 1 unreduced ones folded into an
+// accumulator, 2 products by one factor through its window table in shared
+// memory). The chains' values are XORed into `sink` so none is dead code.
+// The time is that of one launch of blocks_per_sm waves of blocks per SM.
+constexpr int kPeakChains = 4;
+
+template <int kKind>
+__global__ void __launch_bounds__(kThreads) k_gf_peak(int iters, f128 y, f128 *sink) {
+  __shared__ MulTable T;
+  if (kKind == 2) mul_table_build(T, y);
+  f128 x[kPeakChains];
+  for (int k = 0; k < kPeakChains; k++)
+    x[k] = mk(0x9e3779b97f4a7c15ull * (blockIdx.x * blockDim.x + threadIdx.x + 1) + k,
+              0xc2b2ae3d27d4eb4full ^ (uint64_t)k);
+  wide acc = wzero();
+  for (int i = 0; i < iters; i++)
+#pragma unroll
+    for (int k = 0; k < kPeakChains; k++) {
+      if (kKind == 0) {
+        x[k] = gmul(x[k], y);
+      } else if (kKind == 1) {
+        const wide w = gmul_wide(x[k], y);
+        wacc(acc, w);
+        x[k] = mk(w.w0 ^ w.w2, w.w1 ^ w.w3);  // the next operand depends on the product
+      } else {
+        x[k] = mul_table(T, x[k]);
+      }
+    }
+  f128 r = greduce(acc);
+  for (int k = 0; k < kPeakChains; k++) r = gadd(r, x[k]);
+  if (gis_zero(r)) st(sink, r);  // practically never; keeps the chains live
+}
+
+template <int kKind>
+static float time_gf_peak(int blocks, int iters, f128 y, f128 *sink, cudaStream_t s) {
+  cudaEvent_t e0, e1;
+  BZ_CUDA(cudaEventCreate(&e0));
+  BZ_CUDA(cudaEventCreate(&e1));
+  k_gf_peak<kKind><<<blocks, kThreads, 0, s>>>(16, y, sink);  // warm-up
+  BZ_LAUNCH_CHECK();
+  BZ_CUDA(cudaEventRecord(e0, s));
+  k_gf_peak<kKind><<<blocks, kThreads, 0, s>>>(iters, y, sink);
+  BZ_LAUNCH_CHECK();
+  BZ_CUDA(cudaEventRecord(e1, s));
+  BZ_CUDA(cudaEventSynchronize(e1));
+  float ms = 0;
+  BZ_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  return ms;
+}
+
+// Products per second of `kind` over a grid of `blocks_per_sm` blocks per SM.
+double diag_gf_peak(int kind, int blocks_per_sm) {
+  Context &lane = Context::get();
+  cudaStream_t s = lane.stream();
+  int dev = 0, sms = 0;
+  BZ_CUDA(cudaGetDevice(&dev));
+  BZ_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+  DeviceBuffer<f128> sink(1);
+  const int blocks = sms * blocks_per_sm, iters = kind == 2 ? 4096 : 1024;
+  const f128 y = mk(0x0123456789abcdefull, 0xfedcba9876543210ull);
+  const float ms = kind == 0   ? time_gf_peak<0>(blocks, iters, y, sink.get(), s)
+                   : kind == 1 ? time_gf_peak<1>(blocks, iters, y, sink.get(), s)
+                               : time_gf_peak<2>(blocks, iters, y, sink.get(), s);
+  return (double)blocks * kThreads * kPeakChains * iters / (ms * 1e-3);
+}
+
 }  // namespace bz

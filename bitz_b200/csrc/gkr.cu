@@ -604,6 +604,11 @@ static f128 eq_factor(f128 r, f128 z) { return gadd(gadd(mk(1, 0), r), z); }
 
 // One bind round of hh elements per half: by tiles up to kMidMaxH, one
 // element per thread above (issue bound there).
+// Elements below h whose packed column holds bits of h (the rest are padding).
+static double live_threads(size_t h, size_t colmask, size_t live) {
+  return h > colmask ? (double)(h / (colmask + 1)) * (double)live : (double)std::min(h, live);
+}
+
 static void launch_bind(f128 *c, size_t n_half, size_t hh, f128 r, f128 *eq, int at_one,
                         unsigned long long *acc, const Publish &pub, const RoundLink &lk,
                         size_t colmask, size_t live, cudaStream_t st) {
@@ -694,7 +699,7 @@ f128 gkr_prove(int s, const f128 *zeta, uint32_t grind_bits, Transcript &ts, Gkr
     // sums after binding r_i, which the host posts as downbox publication
     // d0 + (n - 1 - i). The kernel probe times kernels alone, so it runs
     // every round as its own launch.
-    const bool queued = ch && resident && !probe.on("gkr_bind_sums");
+    const bool queued = ch && resident;
     int i_tail = n - 1;
     while (i_tail > 0 && ((size_t)1 << (i_tail - 1)) > (size_t)kTailH) i_tail--;
     const Publish top = arm(sc);
@@ -713,10 +718,19 @@ f128 gkr_prove(int s, const f128 *zeta, uint32_t grind_bits, Transcript &ts, Gkr
     RoundLink top_link = none;
     if (queued && n - 1 > i_tail) top_link = RoundLink{nullptr, link_for(n - 1), ch->down_dev, d0};
     if (queued) tail = true;  // from here a kernel of the lane may wait for this thread
+    const bool probe_top = probe.on("gkr_top_sums");
+    if (probe_top) probe.before(st_);
     gkr_top_sums<<<grid_for(h), kThreads, 0, st_>>>(c, n_half, h, lo, a, hi, sc.eq,
                                                     gis_zero(point[n - 1]), sc.acc, top, top_link,
                                                     colmask, live);
     BZ_LAUNCH_CHECK();
+    if (probe_top) {
+      // each thread forms e = lo * hi and writes it; a live one also reads its
+      // four child entries and multiplies e by two of them and the results by two more
+      const double nl = live_threads(h, colmask, live);
+      probe.after(st_, "gkr_top_sums", 16.0 * (double)h + 64.0 * nl, (double)h + 2.0 * nl,
+                  2.0 * nl);
+    }
     if (queued) {
       int i = n - 1;
       for (; i > i_tail && !in_mid(i); i--) {
@@ -759,17 +773,19 @@ f128 gkr_prove(int s, const f128 *zeta, uint32_t grind_bits, Transcript &ts, Gkr
         ch->arm();
       } else if (i > 0) {
         size_t hh = (size_t)1 << (i - 1);
-        // the probe times gkr_bind_sums itself: the launches above kMidMaxH
-        const bool probed = probe.on("gkr_bind_sums") && hh > kMidMaxH;
+        const char *name = hh <= kMidMaxH ? "gkr_round" : "gkr_bind_sums";
+        const bool probed = probe.on(name);
         if (probed) probe.before(st_);
         launch_bind(c, n_half, hh, r, sc.eq, gis_zero(point[i - 1]), acc + 4, arm(sc), none,
                     colmask, live, st_);
-        // reads 8 child and 2 eq entries per thread, writes 4 and 1
         if (probed) {
-          // live threads move 15 entries, padded ones the eq table's 3
-          double nl = hh > colmask ? (double)(hh / (colmask + 1)) * (double)live
-                                   : (double)std::min(hh, live);
-          probe.after(st_, 240.0 * nl + 48.0 * ((double)hh - nl));
+          // a live element reads 8 child and 2 eq entries and writes 4 and 1
+          // (240 B), binds four entries by r through r's window table and
+          // makes four general products (two by e, two wide); a padded one
+          // moves the eq table's 3 entries (48 B)
+          const double nl = live_threads(hh, colmask, live);
+          probe.after(st_, name, 240.0 * nl + 48.0 * ((double)hh - nl), 2.0 * nl, 2.0 * nl,
+                      4.0 * nl);
         }
       } else {
         gkr_final_bind<<<1, 32, 0, st_>>>(c, n_half, r, sc.pair, arm(sc));

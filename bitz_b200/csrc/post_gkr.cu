@@ -11,6 +11,7 @@
 // coefficients are XOR sums of weights with no multiplication
 // (lib.rs:189-239).
 #include "device.cuh"
+#include "context.hpp"
 #include "post_gkr.hpp"
 
 namespace bz {
@@ -177,13 +178,26 @@ void quad_sums(const f128 *w, const f128 *v, size_t n, unsigned long long *acc, 
   BZ_LAUNCH_CHECK();
 }
 
+// pg_round's algorithmic work for `nout` folded entries: each reads two
+// entries of W and of V and writes one of each (96 B), binds both by r through
+// r's window table, and each pair of them adds two wide products to the sums.
+static void probe_pg_round(KernelProbe &probe, bool on, cudaStream_t s, size_t nout, int emit) {
+  if (on)
+    probe.after(s, "pg_round", 96.0 * (double)nout, 0.0,
+                emit ? (double)(nout & ~(size_t)1) : 0.0, 2.0 * (double)nout);
+}
+
 void quad_fold(const f128 *w, const f128 *v, f128 r, f128 *w2, f128 *v2, size_t n, int emit,
                unsigned long long *acc, Publish pub, cudaStream_t s) {
   size_t nout = n / 2;
+  KernelProbe &probe = KernelProbe::get();
+  const bool probed = probe.on("pg_round");
+  if (probed) probe.before(s);
   pg_round<<<grid_for((nout + 1) / 2), kThreads, 0, s>>>(w, v, r, w2, v2, nout, emit && nout >= 2,
                                                          acc, pub,
                                                          RoundLink{nullptr, nullptr, nullptr, 0});
   BZ_LAUNCH_CHECK();
+  probe_pg_round(probe, probed, s, nout, emit && nout >= 2);
 }
 
 // h' = p(rho) with a1 = h + a2 (lib.rs:320-323).
@@ -537,11 +551,15 @@ int post_gkr_prove(const PostGkrArgs &a, Transcript &ts, PostGkrScratch &sc, cud
     }
     size_t nout = len / 2;
     int emit = nout >= 2;
+    KernelProbe &probe = KernelProbe::get();
+    const bool probed = probe.on("pg_round");
+    if (probed) probe.before(s);
     pg_round<<<grid_for((nout + 1) / 2), kThreads, 0, s>>>(w, v, rr, w2, v2, nout, emit,
                                                            acc + 8 * (k + 2),
                                                            emit ? arm(sc) : Publish{nullptr, nullptr, 0},
                                                            RoundLink{nullptr, nullptr, nullptr, 0});
     BZ_LAUNCH_CHECK();
+    probe_pg_round(probe, probed, s, nout, emit);
     f128 *t = w;
     w = w2;
     w2 = t;

@@ -16,6 +16,7 @@
 #include "post_gkr.hpp"
 #include "status.hpp"
 #include "witness.hpp"
+#include "prover_internal.hpp"
 
 namespace bz {
 
@@ -92,17 +93,6 @@ bool pcs_config(int m, int sec, PcsConfig &cfg) {
 
 namespace {
 
-void put_u64(std::vector<uint8_t> &b, uint64_t v) {
-  for (int i = 0; i < 8; i++) b.push_back((uint8_t)(v >> (8 * i)));
-}
-void put_u128(std::vector<uint8_t> &b, u128 v) {
-  for (int i = 0; i < 16; i++) b.push_back((uint8_t)(v >> (8 * i)));
-}
-int ceil_log2(size_t n) {
-  int l = 0;
-  while (((size_t)1 << l) < n) l++;
-  return l;
-}
 double ms_since(std::chrono::steady_clock::time_point t) {
   return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t).count();
 }
@@ -199,13 +189,7 @@ std::shared_ptr<DeviceSetup> device_setup(int kind, size_t n_inputs, cudaStream_
   return d;
 }
 
-// Process-wide tables: the generator's comb and the additive-FFT subspace
-// table, built once.
-struct Tables {
-  f128 generator;
-  DeviceBuffer<f128> comb, wh;
-  std::vector<f128> wh_host;
-};
+}  // namespace
 
 Tables &tables(cudaStream_t s) {
   static Tables *t = nullptr;
@@ -225,64 +209,8 @@ Tables &tables(cudaStream_t s) {
   return *t;
 }
 
-}  // namespace
-
-// Slots of Workspace::pin_small, the page-locked home of the small
-// device-to-host reads (16-byte units).
-constexpr size_t kPinFlag = 0, kPinRoot = 1, kPinLevelRoot = 3, kPinW0 = 5, kPinOne = 6,
-                 kPinClaims = 8, kPinSmall = 8 + 128;
-
-// Per-lane device workspace, grown on demand.
-struct Workspace {
-  DeviceBuffer<int> flag;
-  DeviceBuffer<fp> sp_t, sp_d, sp_eqs, sp_part, sp_sums, sp_tab;
-  DeviceBuffer<fp> cols_fp;
-  DeviceBuffer<u128> exps, folds;
-  DeviceBuffer<f128> images, u1, u2, weights, w0, ones, eq, eqs, suffix, basis, eq_ood, lf, lb,
-      lf2, lb2, qs, level_cw, bw;
-  DeviceBuffer<uint32_t> b3, level_nodes;
-  DeviceBuffer<unsigned long long> acc;
-  fp *host_fp = nullptr;
-  uint64_t *host_acc = nullptr;
-  // the claim's canonical column weights and the column folds, copied back
-  // while the host absorbs earlier messages
-  DeviceBuffer<fp> cols_canon;
-  PinnedBuffer<u128> host_cols, host_folds;
-  // Ligerito: the next levels' codewords and trees, the query indices and the
-  // gathered openings, with their host copies
-  DeviceBuffer<f128> lig_cw[2], openings;
-  DeviceBuffer<uint32_t> lig_nodes[2];
-  DeviceBuffer<uint64_t> qidx;
-  PinnedBuffer<uint64_t> pin_idx;
-  PinnedBuffer<f128> pin_open, pin_f, pin_b, pin_qw, pin_small;
-  // the proof's own state: the staged statement, the witness, the level-0
-  // codeword and tree
-  DeviceBuffer<uint32_t> states, msgs, fin, f, h, bit_rows, nodes0;
-  DeviceBuffer<uint64_t> offsets;
-  DeviceBuffer<int64_t> prod;
-  DeviceBuffer<uint8_t> bit_c;
-  DeviceBuffer<f128> codeword0;
-  DeviceBuffer<f128> mt_dense;  // the rows' eq table for the M^T gather
-  uint64_t staged_serial = 0;  // the system whose statement these hold
-  cudaEvent_t ev_cols = nullptr, ev_folds = nullptr;
-  Workspace() {
-    AllocScope gate;
-    BZ_CUDA(cudaMallocHost(&host_fp, 8 * sizeof(fp)));
-    BZ_CUDA(cudaMallocHost(&host_acc, 512 * sizeof(uint64_t)));
-    BZ_CUDA(cudaEventCreateWithFlags(&ev_cols, cudaEventDisableTiming));
-    BZ_CUDA(cudaEventCreateWithFlags(&ev_folds, cudaEventDisableTiming));
-  }
-  ~Workspace() {
-    AllocScope gate(false);
-    if (host_fp) cudaFreeHost(host_fp);
-    if (host_acc) cudaFreeHost(host_acc);
-    if (ev_cols) cudaEventDestroy(ev_cols);
-    if (ev_folds) cudaEventDestroy(ev_folds);
-  }
-};
-
 // The lane's workspace, created on its first proof.
-static Workspace &workspace(Context &lane) {
+Workspace &workspace(Context &lane) {
   if (!lane.workspace) lane.workspace = std::make_shared<Workspace>();
   return *lane.workspace;
 }
@@ -1055,15 +983,89 @@ int ProofSystem::prove_after_commit(cudaStream_t s, std::vector<uint8_t> &proof)
   return BZ_OK;
 }
 
-int ProofSystem::prove(std::vector<uint8_t> &proof, StageTimes *times, bool restage,
-                       Context *lane) {
+void ProofSystem::bind_lane(Context *lane) {
   lane_ = lane ? lane : &Context::get();
-  cudaStream_t s = lane_->stream();
-  auto t0 = std::chrono::steady_clock::now();
   Workspace &W = workspace(*lane_);
   states_ = &W.states, msgs_ = &W.msgs, fin_ = &W.fin, offsets_ = &W.offsets;
   f_ = &W.f, h_ = &W.h, prod_ = &W.prod, bit_c_ = &W.bit_c, d_bit_rows_ = &W.bit_rows;
   codeword0_ = &W.codeword0, nodes0_ = &W.nodes0;
+}
+
+int ProofSystem::split_witness(const uint8_t *inputs, size_t n_inputs, Context *lane) {
+  if (split_) {
+    error = "this system already holds a witness: prove or drop it first";
+    return BZ_ERR_ARGUMENT;
+  }
+  if (n_inputs != inputs_.size()) {  // end_to_end.rs:216-218
+    error = "wrong witness input length";
+    return BZ_ERR_ARGUMENT;
+  }
+  for (size_t i = 0; i < n_inputs; i++)
+    if (inputs[i] > 1) {
+      error = "input bits must be 0 or 1";
+      return BZ_ERR_ARGUMENT;
+    }
+  bind_lane(lane);
+  cudaStream_t s = lane_->stream();
+  // the witness is computed from these inputs; the bit constraints keep the
+  // statement's expected values, so other inputs leave it unsatisfied
+  std::vector<uint8_t> in(inputs, inputs + n_inputs);
+  std::vector<uint32_t> states, msgs, fin;
+  std::vector<uint8_t> bitc_unused;
+  prepare_statement(kind_, *dev_->host, in, outputs_, states, msgs, fin, bitc_unused);
+  states_->upload(states.data(), states.size(), s);
+  msgs_->upload(msgs.data(), msgs.size(), s);
+  offsets_->upload(dev_->host->block_f_offset.data(), dev_->host->block_f_offset.size(), s);
+  if (!fin.empty()) fin_->upload(fin.data(), fin.size(), s);
+  bit_c_->upload(bitc_h_.data(), bitc_h_.size(), s);
+  workspace(*lane_).staged_serial = 0;  // not this statement's staging: restage next time
+  BZ_CUDA(cudaEventRecord(ev_start_, s));
+  int rc = witness(s);
+  if (rc) return rc;
+  split_ = 1;
+  return BZ_OK;
+}
+
+int ProofSystem::split_commit() {
+  if (split_ != 1) {
+    error = split_ ? "the witness is already committed" : "no witness to commit";
+    return BZ_ERR_ARGUMENT;
+  }
+  int rc = commit(lane_->stream());
+  if (rc) return rc;
+  split_ = 2;
+  return BZ_OK;
+}
+
+int ProofSystem::split_prove(std::vector<uint8_t> &proof) {
+  if (split_ != 2) {
+    error = split_ ? "the witness is not committed" : "no committed witness to prove";
+    return BZ_ERR_ARGUMENT;
+  }
+  split_ = 0;
+  cudaStream_t s = lane_->stream();
+  int rc = prove_after_commit(s, proof);
+  BZ_CUDA(cudaEventRecord(ev_stop_, s));
+  BZ_CUDA(cudaEventSynchronize(ev_stop_));
+  KernelProbe::get().collect();
+  return rc;
+}
+
+void ProofSystem::split_drop() {
+  split_ = 0;
+  ts_.reset();
+}
+
+int ProofSystem::prove(std::vector<uint8_t> &proof, StageTimes *times, bool restage,
+                       Context *lane) {
+  if (split_) {
+    error = "this system holds a witness of the staged calls: prove or drop it first";
+    return BZ_ERR_ARGUMENT;
+  }
+  bind_lane(lane);
+  cudaStream_t s = lane_->stream();
+  auto t0 = std::chrono::steady_clock::now();
+  Workspace &W = workspace(*lane_);
   BZ_CUDA(cudaEventRecord(ev_start_, s));
   if (restage || W.staged_serial != serial_) {
     stage_statement(s);

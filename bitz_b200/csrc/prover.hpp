@@ -42,6 +42,15 @@ struct DeviceSetup {
   uint32_t col0_nnz = 0;
 };
 
+// The two streams of a proof's bitzPCS wire container.
+struct WireView {
+  const uint8_t *narg = nullptr, *hints = nullptr;
+  size_t narg_len = 0, hints_len = 0;
+};
+// WireProof::from_bytes (crates/host/src/wire_proof.rs:109-140): strict;
+// BZ_ERR_MALFORMED with the reference's error variant named in err.
+int wire_decode(const uint8_t *bytes, size_t len, WireView &out, std::string &err);
+
 struct StageTimes {
   double witness_ms = 0, commit_ms = 0, prove_ms = 0;
   double device_ms = 0;  // CUDA-event span on the prover's stream, first to last launch
@@ -71,9 +80,31 @@ class ProofSystem {
   int prove(std::vector<uint8_t> &proof, StageTimes *times, bool restage = true,
             Context *lane = nullptr);
 
+  // The reference's stages as separate calls (CircuitProofSystem::witness,
+  // commit and prove, end_to_end.rs:215-336), on one lane from the witness to
+  // the proof: the witness stays in the lane's device buffers and the
+  // commitment (codeword, Merkle tree, transcript) with it. A system holds at
+  // most one such proof at a time, and prove() refuses while it does.
+  // split_witness takes the witness's input bits (one byte each; the same
+  // count as the statement's, else BZ_ERR_ARGUMENT) and returns
+  // BZ_ERR_UNSATISFIED when they do not satisfy the statement.
+  int split_witness(const uint8_t *inputs, size_t n_inputs, Context *lane);
+  int split_commit();
+  // Runs the prove stage and ends the split proof (also on failure).
+  int split_prove(std::vector<uint8_t> &proof);
+  // Ends a split proof at any stage without proving.
+  void split_drop();
+  int split_stage() const { return split_; }  // 0 none, 1 witnessed, 2 committed
+
   const CircuitSetup &setup() const { return *dev_->host; }
   int security() const { return security_; }
   std::string error;
+
+  // CircuitProofSystem::verify (end_to_end.rs:339-377) on proof bytes (root
+  // || Spartan section || wire container), on `lane` (the default lane when
+  // null): BZ_OK when every check passes, BZ_ERR_MALFORMED when the bytes do
+  // not parse, BZ_ERR_VERIFY naming the failed check otherwise.
+  int verify(const uint8_t *proof, size_t proof_len, Context *lane = nullptr);
 
   // Witness-stage products for inspection (valid after prove()).
   void download_witness(std::vector<uint32_t> &f, std::vector<uint32_t> &h,
@@ -86,7 +117,9 @@ class ProofSystem {
   int prove_after_commit(cudaStream_t s, std::vector<uint8_t> &proof);
   std::vector<uint8_t> ligerito(cudaStream_t s, f128 target);
 
+  void bind_lane(Context *lane);
   Context *lane_ = nullptr;  // the lane of the proof in progress
+  int split_ = 0;            // stage of a split proof (split_stage)
   int kind_, security_;
   std::vector<uint8_t> inputs_, outputs_;
   std::shared_ptr<DeviceSetup> dev_;

@@ -8,6 +8,7 @@
 // fold/round fusion, sumcheck.rs:963-1026), then one single-block launch adds
 // the per-block partial sums; 48 (outer) or 32 (inner) bytes go to the host.
 #include "device.cuh"
+#include "context.hpp"
 #include "spartan.hpp"
 
 #include <chrono>
@@ -469,11 +470,15 @@ __global__ void __launch_bounds__(kThreads) sp_inner_tail(const fp *D, const fp 
 static fp host_partial_sum(const fp *d_partial, int nblocks, int N, fp *d_out, fp *h_out,
                            const FpCtx &c, cudaStream_t s, RoundChannel *ch) {
   Publish pub = ch ? ch->arm() : Publish{nullptr, nullptr, 0};
+  KernelProbe &probe = KernelProbe::get();
+  const bool probed = probe.on("k_fp_finalize");
+  if (probed) probe.before(s);
   if (N == 3)
     k_fp_finalize<3><<<1, kThreads, 0, s>>>(d_partial, nblocks, c, d_out, pub);
   else
     k_fp_finalize<2><<<1, kThreads, 0, s>>>(d_partial, nblocks, c, d_out, pub);
   BZ_LAUNCH_CHECK();
+  if (probed) probe.after(s, "k_fp_finalize", 16.0 * N * (nblocks + 1));
   if (ch) {
     ch->wait(s, reinterpret_cast<uint64_t *>(h_out), 2 * N);
   } else {
@@ -764,10 +769,15 @@ void spartan_prove(const SpartanArgs &a, Transcript &ts, SpartanScratch &sc, cud
     } else {
       size_t npairs = fold ? (len / 2 + 1) / 2 : len / 2;
       int g = grid_for(npairs);
+      KernelProbe &probe = KernelProbe::get();
+      const bool probed = probe.on("k_outer_round");
+      if (probed) probe.before(s);
       k_outer_round<<<g, kThreads, 0, s>>>(E, A, B, C, E2, A2, B2, C2, len, fold, 1, r, c,
                                            sc.partial, Publish{nullptr, nullptr, 0},
                                            RoundLink{nullptr, nullptr, nullptr, 0});
       BZ_LAUNCH_CHECK();
+      // four tables of 16-byte residues: read whole, written folded to half
+      if (probed) probe.after(s, "k_outer_round", 16.0 * 4 * (double)len * (fold ? 1.5 : 1.0));
       host_partial_sum(sc.partial, g, 3, sc.sums, sc.host, c, s, sc.channel);
       if (fold) {
         std::swap(E, E2);
@@ -919,10 +929,20 @@ void spartan_prove(const SpartanArgs &a, Transcript &ts, SpartanScratch &sc, cud
     } else {
       size_t npairs = fold ? (len / 2 + 1) / 2 : len / 2;
       int g = grid_for(npairs);
+      KernelProbe &probe = KernelProbe::get();
+      const bool probed = probe.on("k_inner_round");
+      if (probed) probe.before(s);
       k_inner_round<<<g, kThreads, 0, s>>>(D, W, a.hbits, w_bits, D2, W2, len, fold, 1, r, c,
                                            sc.partial, Publish{nullptr, nullptr, 0},
                                            RoundLink{nullptr, nullptr, nullptr, 0});
       BZ_LAUNCH_CHECK();
+      // D (16-byte residues) and W (16-byte residues, or bits while w_bits is
+      // set): read whole, written folded to half
+      if (probed) {
+        const double wbytes = w_bits ? (double)len / 8.0 : 16.0 * (double)len;
+        probe.after(s, "k_inner_round",
+                    16.0 * (double)len + wbytes + (fold ? 16.0 * (double)len : 0.0));
+      }
       host_partial_sum(sc.partial, g, 2, sc.sums, sc.host, c, s, sc.channel);
       if (fold) {
         std::swap(D, D2);
@@ -961,6 +981,52 @@ void spartan_prove(const SpartanArgs &a, Transcript &ts, SpartanScratch &sc, cud
   out.d_at_ry = dw[0];
   out.final_claim = claim;
   out.ok = fp_mul(dw[0], dw[1], c).lo == claim.lo && fp_mul(dw[0], dw[1], c).hi == claim.hi;
+}
+
+// Per-block partial sums of D[y] * E[y] over n entries (mod q).
+__global__ void k_fp_dot(const fp *__restrict__ D, const fp *__restrict__ E, size_t n, FpCtx c,
+                         fp *partial) {
+  fp acc[1] = {fp_zero()};
+  for (size_t y = blockIdx.x * (size_t)blockDim.x + threadIdx.x; y < n;
+       y += (size_t)gridDim.x * blockDim.x)
+    acc[0] = fp_add(acc[0], fp_mul(D[y], E[y], c), c);
+  block_fp_sum<1>(acc, c, partial);
+}
+
+fp spartan_matrix_eval(const SpartanArgs &a, const fp *rx, fp rho, const fp *ry,
+                       SpartanScratch &sc, cudaStream_t s) {
+  const FpCtx &c = a.ctx;
+  const int nr = a.num_row_vars, nc = a.num_col_vars;
+  const size_t Cn = (size_t)1 << nc;
+  const fp rho2 = fp_mul(rho, rho, c);
+  // the prover's bind at (r_x, rho): D(y) for every column y
+  fp *eq = sc.t[0];
+  fp_eq_table(rx, nr, c, eq, sc.eq_scratch, s);
+  k_bind_table<<<(a.ntab + 127) / 128, 128, 0, s>>>(a.tab_vals, a.tab_which, a.ntab, rho, rho2, c,
+                                                     sc.tab);
+  BZ_LAUNCH_CHECK();
+  fp *D = sc.d[0], *EY = sc.d[1];
+  k_bind<<<grid_for(Cn), kThreads, 0, s>>>(a.csc_off, a.csc_row, a.csc_idx, sc.tab, eq, a.cols, Cn,
+                                           c, D);
+  BZ_LAUNCH_CHECK();
+  {
+    int g = grid_for(std::max<size_t>(a.col0_nnz, (size_t)a.n_bit_rows));
+    k_bind_col0<<<g, kThreads, 0, s>>>(a.csc_row, a.csc_idx, sc.tab, eq, a.col0_nnz, a.bit_rows,
+                                       a.n_bit_rows, rho2, c, sc.partial);
+    BZ_LAUNCH_CHECK();
+    k_bind_col0_finish<<<1, kThreads, 0, s>>>(sc.partial, g, c, D);
+    BZ_LAUNCH_CHECK();
+  }
+  // then sum_y D(y) eq(r_y, y)
+  fp_eq_table(ry, nc, c, EY, sc.eq_scratch, s);
+  const int g = grid_for(Cn);
+  k_fp_dot<<<g, kThreads, 0, s>>>(D, EY, Cn, c, sc.partial);
+  BZ_LAUNCH_CHECK();
+  k_fp_finalize<1><<<1, kThreads, 0, s>>>(sc.partial, g, c, sc.sums, Publish{nullptr, nullptr, 0});
+  BZ_LAUNCH_CHECK();
+  BZ_CUDA(cudaMemcpyAsync(sc.host, sc.sums, sizeof(fp), cudaMemcpyDeviceToHost, s));
+  BZ_CUDA(cudaStreamSynchronize(s));
+  return sc.host[0];
 }
 
 FpCtx make_fp_ctx(u128 q) {

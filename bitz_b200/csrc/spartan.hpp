@@ -62,5 +62,12 @@ void fp_eq_table(const fp *point, int n, const FpCtx &c, fp *out, fp *scratch, c
 
 void spartan_prove(const SpartanArgs &a, Transcript &ts, SpartanScratch &sc, cudaStream_t s,
                    SpartanOut &out);
+// The verifier's matrix evaluation: sum over the entries of A + rho B +
+// rho^2 C (with the statement's bit constants in C) of eq(r_x, row) eq(r_y,
+// col) times the entry, on the device through the prover's bind (the dense
+// D(y) over the columns) and a dot product with eq(r_y). Montgomery in and
+// out; uses sc.t[0], sc.d[0..1], eq_scratch, partial, sums, tab and host.
+fp spartan_matrix_eval(const SpartanArgs &a, const fp *rx, fp rho, const fp *ry,
+                       SpartanScratch &sc, cudaStream_t s);
 
 }  // namespace bz

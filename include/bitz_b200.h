@@ -133,6 +133,49 @@ int bitz_system_prove(bitz_system *sys, uint8_t **proof, size_t *proof_len, doub
 int bitz_system_prove_ex(bitz_system *sys, int restage, uint8_t **proof, size_t *proof_len,
                          double times_ms[4]);
 void bitz_free(void *p);
+
+/* The same proof as three calls, as the reference's API has it:
+ * CircuitProofSystem::witness (end_to_end.rs:215-243), commit (:248-255) and
+ * prove, which consumes both (:260-336). The witness and its commitment stay
+ * in device memory between the calls, on a prover lane held from bitz_witness
+ * until bitz_prove (the process's default lane when free, else a pooled one).
+ * A system holds at most one staged proof at a time (BZ_ERR_ARGUMENT
+ * otherwise), and bitz_system_prove on it waits for none: it refuses while
+ * one is staged. Handles must be used on the thread's current device and
+ * freed (or consumed) before their system. */
+typedef struct bitz_witness_handle bitz_witness_handle;
+typedef struct bitz_committed_witness bitz_committed_witness;
+/* input_bits: the witness inputs, one byte (0/1) per bit, as many as the
+ * statement's ("wrong witness input length" otherwise, Error::Input);
+ * BZ_ERR_UNSATISFIED when they do not satisfy the statement. */
+int bitz_witness(bitz_system *sys, const uint8_t *input_bits, size_t n_inputs,
+                 bitz_witness_handle **out);
+int bitz_commit(bitz_system *sys, const bitz_witness_handle *wit, bitz_committed_witness **out);
+/* Consumes wit and com on every return. The proof bytes are those of
+ * bitz_system_prove for the same statement, freed with bitz_free. */
+int bitz_prove(bitz_system *sys, bitz_witness_handle *wit, bitz_committed_witness *com,
+               uint8_t **proof, size_t *proof_len);
+/* CircuitProofSystem::verify (end_to_end.rs:339-377) on proof bytes as
+ * bitz_system_prove returns them, replayed by this library's own verifier
+ * (the bulk steps on the device). BZ_OK: accepted. BZ_ERR_MALFORMED: the
+ * bytes do not parse (the wire container's errors,
+ * crates/host/src/wire_proof.rs:40-60, named in bitz_last_error).
+ * BZ_ERR_VERIFY: a check failed (named in bitz_last_error). Hostile bytes
+ * never crash it. */
+int bitz_verify(bitz_system *sys, const uint8_t *proof, size_t proof_len);
+/* WireProof::from_bytes (crates/host/src/wire_proof.rs:109-140): strict
+ * decoding of a bitzPCS container (header, then exactly the declared narg and
+ * hint bytes). out: narg offset, narg length, hint offset, hint length.
+ * Needs no GPU. */
+int bitz_wire_decode(const uint8_t *bytes, size_t len, uint64_t out[4]);
+/* Diagnostic (the reference hashes with the blake3 crate, Cargo.lock:239):
+ * this library's host BLAKE3, the one its transcript grinding, Merkle checks
+ * and weight digest use; derive-key mode when derive_key_context is non-null
+ * (crates/pcs/src/opening.rs:354-365), else hash mode. Needs no GPU. */
+int bitz_blake3(const char *derive_key_context, const uint8_t *in, size_t len, uint8_t out[32]);
+/* Drop a staged proof without proving; freeing either handle ends it. */
+void bitz_witness_free(bitz_witness_handle *wit);
+void bitz_committed_witness_free(bitz_committed_witness *com);
 /* Diagnostic (no reference counterpart): kernel launches issued by this
  * library since the process started. */
 unsigned long long bitz_launch_count(void);
@@ -143,6 +186,12 @@ unsigned long long bitz_launch_count(void);
  * attached, since such a tool holds the host at every launch. Proof bytes are
  * the same in both modes. Needs no GPU. */
 int bitz_resident_rounds(void);
+/* Diagnostic (no reference counterpart): on the default lane since the
+ * process started, out[0] the nanoseconds the host spent waiting for round
+ * results (device work and the PCIe round trip) and out[1] the number of
+ * such waits. The rest of a proof's host time is the host's own transcript
+ * work. */
+int bitz_round_wait_stats(unsigned long long out[2]);
 /* Diagnostic (no reference counterpart): the last proof's packed witness f,
  * packed h = M (1 || f) and the exact products (A h, B h, C h per row). */
 int bitz_system_witness(bitz_system *sys, uint32_t *f_words, size_t f_cap, uint32_t *h_words,
@@ -212,17 +261,34 @@ int bitz_server_stop(bitz_server *srv);
 
 /* --------------------------------------------------------- measurement aids
  * No reference counterpart. */
-/* Times every launch of the named kernel with CUDA events on its stream and
- * counts the algorithmic bytes each launch moves; NULL or "" turns it off
- * (and enabling resets the totals). Currently probed: "gkr_bind_sums". */
-int bitz_probe_kernel(const char *name);
-int bitz_probe_read(double *ms_total, double *bytes_total, unsigned long long *launches);
+/* Times every launch of the probed kernels with CUDA events on their stream
+ * and counts each launch's algorithmic work. spec: NULL or "" turns the
+ * probe off, "*" probes every instrumented launch site, else a comma-separated
+ * list of kernel names; enabling resets the totals. While the probe is on,
+ * every sumcheck round is its own launch (as under a kernel profiler).
+ * Instrumented: gkr_top_sums, gkr_round, gkr_bind_sums, pg_round,
+ * k_outer_round, k_inner_round, k_fp_finalize. */
+int bitz_probe_kernel(const char *spec);
+/* One kernel's totals since the probe was enabled: out[0] milliseconds,
+ * out[1] algorithmic bytes, and its GF(2^128) products: out[2] reduced
+ * general products, out[3] unreduced (wide) general products, out[4] products
+ * by the round's challenge through its window table (none are counted for the
+ * prime-field kernels); *launches the launch count. */
+int bitz_probe_read(const char *kernel, double out[5], unsigned long long *launches);
+/* The probed kernels that launched, comma-separated, into out (truncated to
+ * cap - 1 characters); returns the full length. */
+size_t bitz_probe_kernels(char *out, size_t cap);
 /* Overwrites a 256 MiB device buffer and waits, evicting the L2 cache. */
 int bitz_l2_flush(void);
 /* Mean microseconds per host<->device round on the default lane: mode 0
  * launches one kernel per round that posts to the mailbox; mode 1 runs one
  * resident kernel that waits (bounded) for each host word and posts it back. */
 int bitz_diag_round_trip(int mode, int rounds, double *us_per_round);
+/* The GPU's GF(2^128) product throughput (products per second over every SM,
+ * four independent chains per thread): kind 0 reduced general products, 1
+ * unreduced ones, 2 products by one factor through its window table in
+ * shared memory. The ceiling that the integer-bound kernels are held to. */
+int bitz_diag_gf_peak(int kind, double *products_per_s);
 
 #ifdef __cplusplus
 }

@@ -42,13 +42,44 @@ def test_proof_bytes_match_oracle(kind, blocks, security):
     assert first_difference(gproof, oproof) is None, (len(gproof), len(oproof))
 
 
-def test_witness_matches_oracle():
-    inp, out, _ = ci.instance("sha256-chain", 2, 3)
+# Every single-proof workload at its full size: the benchmark statement
+# (sha256-chain n=64, seed 1), the large one (n=1024, seed 2, 128-bit
+# profile: unique decoding, four PCS levels, m_f = 23), block-aligned k=32
+# and the 2 KiB message.
+FULL_SIZE = [("sha256-chain", 64, 1, 100), ("sha256-block-aligned", 32, 3, 100),
+             ("sha256-2kb", 32, 4, 128), ("sha256-chain", 1024, 2, 128)]
+
+
+@pytest.mark.parametrize("kind,blocks,seed,security", FULL_SIZE)
+def test_full_size_proof_bytes_match_oracle(kind, blocks, seed, security):
+    inp, out, _ = ci.instance(kind, blocks, seed)
+    rc, oproof, _ = of.prove(ci.KINDS[kind], inp, out, security)
+    assert rc == 0
+    gproof, _ = bz.CircuitProofSystem(kind, inp, out, security).prove()
+    assert first_difference(gproof, oproof) is None, (len(gproof), len(oproof),
+                                                      first_difference(gproof, oproof))
+
+
+def test_batch_mix_proofs_match_oracle():
+    """Eight statements of the batched workload (block-aligned, uneven k),
+    proved together on four lanes, each equal to the oracle's proof."""
+    mix = ci.batch_mix(3, 256, 32)[:8]
+    systems = [bz.CircuitProofSystem(kind, inp, out, 100) for kind, inp, out in mix]
+    proofs, _ = bz.batch_prove(systems, 4)
+    for (kind, inp, out), proof in zip(mix, proofs):
+        rc, oproof, _ = of.prove(ci.KINDS[kind], inp, out, 100)
+        assert rc == 0
+        assert first_difference(proof, oproof) is None, (kind, len(inp) // 512)
+
+
+@pytest.mark.parametrize("blocks,seed", [(2, 3), (64, 1)])
+def test_witness_matches_oracle(blocks, seed):
+    inp, out, _ = ci.instance("sha256-chain", blocks, seed)
     oc = of.Circuit(1, inp, out)
     ps = bz.CircuitProofSystem("sha256-chain", inp, out, 100)
     ps.prove()
     s = ps.stats()
-    f, h, prod = ps.witness((s["padded_committed_bits"]) // 32, (1 << (s["claim_log_cols"] + 7)) // 32,
+    f, h, prod = ps.witness_parts((s["padded_committed_bits"]) // 32, (1 << (s["claim_log_cols"] + 7)) // 32,
                             s["constraints"])
     fb = np.unpackbits(f.view(np.uint8), bitorder="little")
     hb = np.unpackbits(h.view(np.uint8), bitorder="little")

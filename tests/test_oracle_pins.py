@@ -169,3 +169,18 @@ def test_golden_transcript_challenges():
     c1, c2 = _golden_events(of.Transcript(b"golden-session", b"golden-instance"))
     assert c1.hex() == GOLDEN_C1
     assert c2.hex() == GOLDEN_C2
+
+def test_product_host_blake3_known_answers():
+    """The product library's host BLAKE3 (grinding, Merkle checks, the weight
+    digest's root) against the same known answers, both modes."""
+    from bitz_b200 import _lib
+    lib = _lib.load()
+    vec = _blake3_vectors()
+    out = (ctypes.c_uint8 * 32)()
+    for case in vec["cases"]:
+        x = _blake3_input(case["len"])
+        assert lib.bitz_blake3(None, x, len(x), out) == 0
+        assert bytes(out).hex() == case["hash"], case["len"]
+        for ctx in vec["contexts"]:
+            assert lib.bitz_blake3(ctx.encode(), x, len(x), out) == 0
+            assert bytes(out).hex() == case["derive_key"][ctx], (case["len"], ctx)
