@@ -7,14 +7,21 @@ times the same three stages). Setup (constraint synthesis, matrix digest) is
 done once per statement and excluded, as in the reference's benchmark. The L2
 cache is flushed before every timed proof.
 
-Beside it, the batched workload: 256 independent sha256-block-aligned proofs
-with message lengths uniform over 0..32 blocks (SplitMix64 seed 3), proved on
-concurrent prover lanes, against the same 256 proved one after another.
+Beside it, in the same JSON line:
+- ``batched``: 256 independent sha256-block-aligned proofs with message lengths
+  uniform over 0..32 blocks (SplitMix64 seed 3), proved on concurrent prover
+  lanes, against the same 256 proved one after another by the plain
+  single-proof call;
+- ``large``: sha256-chain n=1024 at PCS security 128 (seed 2);
+- ``serving``: an open-loop Poisson stream of requests (half sha256-2kb, half
+  block-aligned with log-uniform 1..512 blocks, seed 4) into the prove server,
+  the arrival rate swept upward, against the same stream proved one request
+  after another;
+- ``roofline``: the kernel with the largest share of a proof's device time,
+  every launch timed with CUDA events, held to the measured HBM bandwidth and
+  the measured GF(2^128) product throughput of the GPU.
 
-``--serve`` instead runs the serving workload: an open-loop Poisson stream of
-requests (half sha256-2kb, half block-aligned with log-uniform 1..512 blocks,
-seed 4) into the prove server, sweeping the arrival rate, and prints one JSON
-line per rate with p50/p99 latency and blocks/s.
+``--serve`` runs the serving sweep alone, one JSON line per rate.
 
 Multi-GPU: one process per GPU (torchrun), each proving its own statements,
 no collective on the data path ("replicas"): value = all proofs' blocks / the
@@ -38,9 +45,7 @@ sys.path.insert(0, ROOT)
 
 MEASURED_PEAKS = os.path.join(ROOT, "MEASURED_PEAKS.json")
 FALLBACK_HBM_GBS = 6650.0
-PROBED_KERNEL = "gkr_bind_sums"
-# per-launch DRAM traffic of the probed kernel, from the ncu capture summarised here
-TRAFFIC_SUMMARY = os.path.join(ROOT, "profiles", "gkr_bind_sums_sha256-chain-n64.md")
+PROFILES = os.path.join(ROOT, "profiles")
 
 
 def parse():
@@ -58,6 +63,10 @@ def parse():
     p.add_argument("--no-batch", action="store_true")
     p.add_argument("--serve", action="store_true")
     p.add_argument("--serve-requests", type=int, default=96)
+    p.add_argument("--serving-requests", type=int, default=32,
+                   help="requests in the default line's serving sweep")
+    p.add_argument("--no-large", action="store_true")
+    p.add_argument("--no-serving", action="store_true")
     return p.parse_args()
 
 
@@ -160,16 +169,79 @@ def peaks():
         return {"hbm_gbs": FALLBACK_HBM_GBS}, "fallback"
 
 
-def profile_figure(key):
-    """A figure of the probed kernel's ncu summary (e.g. DRAM bytes per
-    launch), or None."""
+def profile_figure(kernel, key):
+    """A figure (e.g. DRAM bytes per launch) from the committed ncu summary of
+    ``kernel`` on this workload, or None: the lines ``key: value`` of
+    profiles/<kernel>_sha256-chain-n64.md."""
+    path = os.path.join(PROFILES, f"{kernel}_sha256-chain-n64.md")
     try:
-        for line in open(TRAFFIC_SUMMARY):
+        for line in open(path):
             if line.startswith(key + ":"):
                 return float(line.split(":", 1)[1])
     except OSError:
         pass
     return None
+
+
+def roofline(bz, ps, steps, hbm_gbs, pk_kind):
+    """Times every launch of the instrumented kernels with CUDA events over
+    ``steps`` proofs (every round its own launch, as under a kernel profiler),
+    picks the kernel with the largest share of the proofs' device time, and
+    holds it to its roofline: its algorithmic bytes at the measured HBM
+    bandwidth and its GF(2^128) products at the GPU's measured product
+    throughput (bitz_diag_gf_peak), whichever takes longer."""
+    peaks = {k: bz.gf_peak(i) for i, k in enumerate(("gmuls", "wides", "tables"))}
+    bz.probe_kernel("*")
+    spans = []
+    for _ in range(steps):
+        bz.l2_flush()
+        _, t = ps.prove(restage=False)
+        spans.append(t["device_ms"])
+    table = {k: bz.probe_read(k) for k in bz.probe_kernels()}
+    bz.probe_kernel(None)
+    span_ms = sum(spans)
+    rows = []
+    for name, t in table.items():
+        if not t["launches"]:
+            continue
+        secs = t["ms"] / 1e3
+        t_hbm = t["bytes"] / (hbm_gbs * 1e9)
+        t_int = sum(t[k] / peaks[k] for k in peaks)
+        bound = "hbm" if t_hbm >= t_int else "integer"
+        rows.append({"kernel": name, "launches": t["launches"] // steps,
+                     "us_per_proof": 1e3 * t["ms"] / steps,
+                     "avg_launch_us": 1e3 * t["ms"] / t["launches"],
+                     "share_of_device_time": t["ms"] / span_ms, "bound": bound,
+                     "frac": max(t_hbm, t_int) / secs if secs > 0 else None,
+                     "bytes_per_launch": t["bytes"] / t["launches"],
+                     "products_per_launch": sum(t[k] for k in peaks) / t["launches"]})
+    rows.sort(key=lambda r: -r["share_of_device_time"])
+    top = rows[0]
+    t = table[top["kernel"]]
+    secs = t["ms"] / 1e3
+    prods = sum(t[k] for k in peaks)
+    if top["bound"] == "hbm":
+        achieved, peak, unit = t["bytes"] / secs / 1e9, hbm_gbs, "GB/s"
+        peak_source = f"hbm_gbs, {pk_kind}"
+    else:
+        # the ceiling of this kernel's product mix at the measured throughputs
+        t_int = sum(t[k] / peaks[k] for k in peaks)
+        achieved, peak, unit = prods / secs / 1e9, prods / t_int / 1e9, "Gproducts/s"
+        peak_source = ("measured GF(2^128) product throughput of this GPU (bitz_diag_gf_peak: "
+                       + ", ".join(f"{k} {v / 1e9:.1f} G/s" for k, v in peaks.items())
+                       + "), weighted by the kernel's product mix")
+    traffic = profile_figure(top["kernel"], "traffic_bytes_per_launch")
+    return {"kernel": top["kernel"], "bound": top["bound"], "achieved": achieved, "peak": peak,
+            "unit": unit, "frac": achieved / peak, "peak_source": peak_source,
+            "traffic": traffic,
+            "traffic_source": (f"ncu dram__bytes_read.sum + dram__bytes_write.sum per launch, "
+                               f"profiles/{top['kernel']}_sha256-chain-n64.md") if traffic else None,
+            "algorithmic_bytes_per_launch": top["bytes_per_launch"],
+            "products_per_launch": top["products_per_launch"],
+            "launches_per_proof": top["launches"], "avg_launch_us": top["avg_launch_us"],
+            "share_of_device_time": top["share_of_device_time"],
+            "mode": "every sumcheck round its own launch (as under ncu), events per launch",
+            "kernels": rows[:8]}
 
 
 def pct(xs, q):
@@ -236,8 +308,10 @@ def reference_arm(args):
 
 
 def batched(args, bz):
-    """256 sha256-block-aligned proofs, k ~ U{0..32} (seed 3): sequential on
-    one lane against concurrent on ``args.lanes`` lanes."""
+    """256 sha256-block-aligned proofs, k ~ U{0..32} (seed 3), concurrent on
+    ``args.lanes`` lanes, against the same 256 proved one after another by the
+    plain single-proof call on the default lane (CircuitProofSystem.prove) and
+    on one pool lane."""
     from bitz_b200 import statements
     mix = statements.batch_mix(3, 256, 32)
     systems = [bz.CircuitProofSystem(kind, inp, out, args.security) for kind, inp, out in mix]
@@ -246,34 +320,73 @@ def batched(args, bz):
     largest = sorted(range(len(mix)), key=lambda i: -mix[i][1].size)[:args.lanes]
     bz.batch_prove([systems[i] for i in largest], args.lanes)
     bz.batch_prove([systems[largest[0]]], 1)
+    systems[largest[0]].prove()
     bz.batch_prove(systems, args.lanes)
     res = {}
-    for name, lanes in (("sequential", 1), ("batched", args.lanes)):
+    # the plain path: one proof after another through the single-proof call
+    bz.l2_flush()
+    plain, lat = [], []
+    t0 = time.perf_counter()
+    for ps in systems:
+        t = time.perf_counter()
+        plain.append(ps.prove()[0])
+        lat.append(1e3 * (time.perf_counter() - t))
+    res["plain"] = (blocks / (time.perf_counter() - t0), lat, plain)
+    for name, lanes in (("pool_lane", 1), ("batched", args.lanes)):
         bz.l2_flush()
         t0 = time.perf_counter()
         proofs, lat = bz.batch_prove(systems, lanes)
         wall = time.perf_counter() - t0
         res[name] = (blocks / wall, lat, proofs)
-    same = res["sequential"][2] == res["batched"][2]
+    same = res["plain"][2] == res["batched"][2] == res["pool_lane"][2]
     return {"workload": "256 x sha256-block-aligned, k ~ U{0..32} blocks (SplitMix64 seed 3), "
                         f"pcs-security-bits {args.security}",
             "blocks": blocks, "lanes": args.lanes,
             "value": res["batched"][0], "unit": "blocks/s",
-            "sequential_value": res["sequential"][0],
-            "speedup_vs_sequential": res["batched"][0] / res["sequential"][0],
+            "sequential_plain_value": res["plain"][0],
+            "speedup_vs_sequential_plain": res["batched"][0] / res["plain"][0],
+            "sequential_pool_lane_value": res["pool_lane"][0],
             "latency_ms": {"p50": pct(res["batched"][1], 0.5), "p99": pct(res["batched"][1], 0.99)},
-            "sequential_latency_ms": {"p50": pct(res["sequential"][1], 0.5),
-                                      "p99": pct(res["sequential"][1], 0.99)},
-            "proofs_identical_to_sequential": same}
+            "sequential_plain_latency_ms": {"p50": pct(res["plain"][1], 0.5),
+                                            "p99": pct(res["plain"][1], 0.99)},
+            "proofs_identical_to_alone": same}
 
 
-def serve(args):
-    """Open-loop Poisson arrivals into the prove server, rate swept upward
-    until p99 latency exceeds 10x the single-proof latency."""
-    import bitz_b200 as bz
+def large(args, bz, steps=5, warmup=2):
+    """sha256-chain n=1024 (64 KiB, SplitMix64 seed 2) at PCS security 128 (unique
+    decoding, no OOD): one proof per step, device time by CUDA events on the
+    prover's stream, L2 flushed before each."""
     from bitz_b200 import statements
-    bz.set_device(dist_env()[2])
-    mix = statements.serve_mix(4, args.serve_requests, 512)
+    inp, out, _ = statements.instance("sha256-chain", 1024, 2)
+    ps = bz.CircuitProofSystem("sha256-chain", inp, out, 128)
+    for _ in range(warmup):
+        ps.prove(restage=False)
+    spans, e2e = [], []
+    for _ in range(steps):
+        bz.l2_flush()
+        _, t = ps.prove(restage=False)
+        spans.append(t["device_ms"])
+    for _ in range(steps):
+        bz.l2_flush()
+        t0 = time.perf_counter()
+        ps.prove(restage=True)
+        e2e.append(1e3 * (time.perf_counter() - t0))
+    return {"workload": "sha256-chain n=1024 pcs-security-bits 128 (seed 2)", "blocks": 1024,
+            "steps": steps, "value": 1024 * steps / (sum(spans) / 1e3), "unit": "blocks/s",
+            "latency_ms": {"p50": statistics.median(spans), "p99": pct(spans, 0.99)},
+            "e2e": {"value": 1024 * steps / (sum(e2e) / 1e3), "unit": "blocks/s",
+                    "latency_ms": {"p50": statistics.median(e2e), "p99": pct(e2e, 0.99)}}}
+
+
+def serve_sweep(args, bz, requests, max_rates, emit=False):
+    """Open-loop Poisson arrivals into the prove server, the rate swept upward
+    by 1.5x until p99 latency exceeds 10x the single-request p99 (or after
+    ``max_rates`` rates). Returns the sweep and the plain arm: the same stream
+    proved one request after another through the single-proof call
+    (statement preparation included, as a served request's latency includes
+    it)."""
+    from bitz_b200 import statements
+    mix = statements.serve_mix(4, requests, 512)
     blocks = [statements.blocks_proven(k, i.size) for k, i, _ in mix]
     # circuit shapes are built once per (circuit, size) and cached, as the
     # reference's benchmark excludes setup: build every shape of the stream
@@ -281,19 +394,19 @@ def serve(args):
     shapes = {}
     for kind, inp, out in mix:
         shapes.setdefault((kind, inp.size), (kind, inp, out))
-    prove_only, alone = [], []
     for kind, inp, out in shapes.values():
-        ps = bz.CircuitProofSystem(kind, inp, out, args.security)
-        ps.prove()
+        bz.CircuitProofSystem(kind, inp, out, args.security).prove()
     setup_s = time.perf_counter() - t0
-    # proof bytes and prove-only latency of the first requests, alone
-    for kind, inp, out in mix[:16]:
-        ps = bz.CircuitProofSystem(kind, inp, out, args.security)
+    # the plain arm: each request prepared and proved alone, one after another
+    alone, plain_lat = [], []
+    t0 = time.perf_counter()
+    for kind, inp, out in mix:
         t = time.perf_counter()
-        p, _ = ps.prove()
-        prove_only.append(1000 * (time.perf_counter() - t))
-        alone.append(p)
+        alone.append(bz.CircuitProofSystem(kind, inp, out, args.security).prove()[0])
+        plain_lat.append(1e3 * (time.perf_counter() - t))
+    plain_bps = sum(blocks) / (time.perf_counter() - t0)
     rng = random.Random(4)
+    sweep = []
     with bz.ProveServer(lanes=args.lanes, hbm_budget=96 << 30, security_bits=args.security) as srv:
         # warm-up: every lane's scratch grows to the largest shape of the stream
         big = max(mix, key=lambda m: m[1].size)
@@ -301,8 +414,8 @@ def serve(args):
         for t in warm:
             while srv.poll(t, 50) is None:
                 pass
-        # single-request latency: each of the first requests alone on an idle
-        # server, submit to proof bytes (statement preparation included)
+        # single-request latency: each request alone on an idle server, submit
+        # to proof bytes (statement preparation included)
         alone_served = []
         for kind, inp, out in mix:
             t = srv.submit(kind, inp, out)
@@ -314,7 +427,7 @@ def serve(args):
         # sweep is the p99 of the requests served one at a time
         single = pct(alone_served, 0.99)
         rate = 1000.0 / statistics.mean(alone_served)  # one request at a time
-        while True:
+        for _ in range(max_rates):
             gaps = [rng.expovariate(rate) for _ in mix]
             tickets, t0 = [], time.perf_counter()
             due = t0
@@ -323,7 +436,7 @@ def serve(args):
                 while time.perf_counter() < due:
                     time.sleep(min(0.0005, max(0.0, due - time.perf_counter())))
                 tickets.append(srv.submit(kind, inp, out))
-            lat, got = [], {}
+            got = {}
             while len(got) < len(tickets):
                 for t in tickets:
                     if t not in got:
@@ -332,23 +445,44 @@ def serve(args):
                             got[t] = r
             wall = time.perf_counter() - t0
             lat = [got[t][1] for t in tickets]
-            same = all(got[t][0] == a for t, a in zip(tickets[:16], alone))
+            same = all(got[t][0] == a for t, a in zip(tickets, alone))
             p99 = pct(lat, 0.99)
-            print(json.dumps({"metric": "SHA-256 blocks proven/sec (serving)", "rate_rps": rate,
-                              "value": sum(blocks) / wall, "unit": "blocks/s",
-                              "latency_ms": {"p50": pct(lat, 0.5), "p99": p99},
-                              "single_request_latency_ms": {
-                                  "p50": pct(alone_served, 0.5), "p99": single},
-                              "prove_only_latency_ms": statistics.median(prove_only),
-                              "lanes": args.lanes,
-                              "requests": len(mix), "peak_in_flight": srv.stats()["peak_in_flight"],
-                              "shapes_prebuilt": len(shapes), "setup_s": setup_s,
-                              "proofs_identical_to_alone": same,
-                              "workload": "Poisson arrivals; 50% sha256-2kb, 50% sha256-block-aligned "
-                                          "k = floor(2^U(0,9)) in 1..512 (seed 4)"}), flush=True)
+            point = {"rate_rps": rate, "value": sum(blocks) / wall, "unit": "blocks/s",
+                     "latency_ms": {"p50": pct(lat, 0.5), "p99": p99},
+                     "peak_in_flight": srv.stats()["peak_in_flight"],
+                     "proofs_identical_to_alone": same}
+            sweep.append(point)
+            if emit:
+                print(json.dumps(dict(point, metric="SHA-256 blocks proven/sec (serving)",
+                                      single_request_latency_ms={"p50": pct(alone_served, 0.5),
+                                                                 "p99": single},
+                                      lanes=args.lanes, requests=len(mix))), flush=True)
             if p99 > 10 * single or rate > 2000:
                 break
             rate *= 1.5
+    below = [pt for pt in sweep if pt["latency_ms"]["p99"] <= 10 * single]
+    best = max(below or sweep[:1], key=lambda pt: pt["value"])
+    return {"workload": "Poisson arrivals; 50% sha256-2kb, 50% sha256-block-aligned "
+                        "k = floor(2^U(0,9)) in 1..512 (seed 4)",
+            "requests": len(mix), "blocks": sum(blocks), "lanes": args.lanes,
+            "rate_rps": best["rate_rps"], "value": best["value"], "unit": "blocks/s",
+            "latency_ms": best["latency_ms"],
+            "single_request_latency_ms": {"p50": pct(alone_served, 0.5), "p99": single},
+            "plain_sequential_value": plain_bps,
+            "speedup_vs_plain_sequential": best["value"] / plain_bps,
+            "plain_latency_ms": {"p50": pct(plain_lat, 0.5), "p99": pct(plain_lat, 0.99)},
+            "proofs_identical_to_alone": all(pt["proofs_identical_to_alone"] for pt in sweep),
+            "rates_swept": len(sweep), "shapes_prebuilt": len(shapes), "setup_s": setup_s,
+            "note": "the point reported is the highest-throughput rate whose p99 stays within "
+                    "10x the single-request p99"}
+
+
+def serve(args):
+    """``--serve``: the full serving sweep, one JSON line per rate, then the summary."""
+    import bitz_b200 as bz
+    bz.set_device(dist_env()[2])
+    summary = serve_sweep(args, bz, args.serve_requests, 30, emit=True)
+    print(json.dumps(dict(summary, metric="SHA-256 blocks proven/sec (serving)")))
 
 
 def ours(args):
@@ -368,25 +502,16 @@ def ours(args):
     # flushed before every proof, each proof timed by CUDA events on its stream
     dist.barrier()
     launches0 = bz.launch_count()
+    wait0 = bz.round_wait_stats()
     with Clocks(local) as clk:
-        spans = []
+        spans, host_ms = [], []
         for _ in range(args.steps):
             bz.l2_flush()
             proof, times = ps.prove(restage=False)
             spans.append(times["device_ms"])
+            host_ms.append(times["witness_ms"] + times["commit_ms"] + times["prove_ms"])
     launches = bz.launch_count() - launches0
-    dist.barrier()
-    # the probed kernel timed alone, in a pass of its own: with the probe on,
-    # its rounds run as separate launches instead of queued behind one another
-    # (a queued round kernel's last block also waits for the next challenge)
-    bz.probe_kernel(PROBED_KERNEL)
-    probe_spans = []
-    for _ in range(min(args.steps, 3)):
-        bz.l2_flush()
-        _, ptimes = ps.prove(restage=False)
-        probe_spans.append(ptimes["device_ms"])
-    probe_ms, probe_bytes, probe_launches = bz.probe_read()
-    bz.probe_kernel(None)
+    wait1 = bz.round_wait_stats()
     dist.barrier()
     dev_total_ms = dist.max(sum(spans))
     # end to end through the C ABI: the statement copied from host memory and
@@ -405,14 +530,17 @@ def ours(args):
     stats = ps.stats()
     h2d = 4 * (8 + 16) * stats["compressions"] + 8 * stats["compressions"] + (inputs.size + 7) // 8 \
         + inputs.size + 256
-    batch = None
+    pk, pk_kind = peaks()
+    roof = roofline(bz, ps, 3, pk["hbm_gbs"], pk_kind)
+    batch = big = serving = None
     if world == 1 and not args.no_batch:
         batch = batched(args, bz)
+    if world == 1 and not args.no_large:
+        big = large(args, bz)
+    if world == 1 and not args.no_serving:
+        serving = serve_sweep(args, bz, args.serving_requests, 6)
     line = None
     if rank == 0:
-        pk, pk_kind = peaks()
-        achieved = probe_bytes / (probe_ms / 1000.0) / 1e9 if probe_ms > 0 else None
-        per_launch = profile_figure("traffic_bytes_per_launch")
         line = {
             "metric": "SHA-256 blocks proven/sec", "value": value, "unit": "blocks/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": statistics.mean(spans),
@@ -427,23 +555,24 @@ def ours(args):
             "e2e": {"value": e2e, "unit": "blocks/s", "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": len(proof)},
             "gpu_launches": launches,
-            "roofline": {"kernel": PROBED_KERNEL, "bound": "hbm", "achieved": achieved,
-                         "peak": pk["hbm_gbs"], "peak_source": f"hbm_gbs, {pk_kind}", "unit": "GB/s",
-                         "frac": achieved / pk["hbm_gbs"] if achieved else None,
-                         "traffic": per_launch,
-                         "algorithmic_bytes_per_launch": probe_bytes / probe_launches if probe_launches else None,
-                         "launches": probe_launches,
-                         "avg_launch_us": 1000 * probe_ms / probe_launches if probe_launches else None,
-                         "share_of_device_time": probe_ms / sum(probe_spans) if probe_spans else None,
-                         "integer_issue_active_ncu": profile_figure("issue_active_largest_launch"),
-                         "note": "integer-issue bound (GF(2^128) products), not HBM bound: "
-                                 "see profiles/gkr_bind_sums_sha256-chain-n64.md"},
+            "round_split": {
+                "rounds_per_proof": (wait1[1] - wait0[1]) / args.steps,
+                "host_waiting_ms_per_proof": 1e3 * (wait1[0] - wait0[0]) / args.steps,
+                "host_ms_per_proof": statistics.mean(host_ms),
+                "note": "host_waiting: the prover's host thread waiting for round results "
+                        "(device work plus the PCIe round trip); the rest of host_ms is the host's "
+                        "own transcript work (Keccak absorbs, challenges, grinding)"},
+            "roofline": roof,
             "clocks": clk.summary(),
             "proof_bytes": len(proof),
             "peaks": pk_kind,
         }
         if batch:
             line["batched"] = batch
+        if big:
+            line["large"] = big
+        if serving:
+            line["serving"] = serving
         if world == 1 and not args.no_cpu_baseline:
             line["cpu_baseline"] = cpu_baseline(args, inputs, outputs, blocks)
         print(json.dumps(line))
