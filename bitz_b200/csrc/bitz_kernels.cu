@@ -13,6 +13,7 @@
 #include "bitz_kernels.hpp"
 #include "device.cuh"
 #include "hash.cuh"
+#include "context.hpp"
 
 namespace bz {
 
@@ -622,6 +623,32 @@ void gather_openings(const f128 *cw, const uint32_t *nodes, size_t rows, int wid
                      const uint64_t *idx, int nq, f128 *out, cudaStream_t s) {
   k_gather_openings<<<nq, 64, 0, s>>>(cw, nodes, rows, width, depth, idx, out);
   BZ_LAUNCH_CHECK();
+}
+
+// Every kernel of this file, loaded when the process's first lane on a device
+// is made (lane_bootstrap, context.cpp).
+void preload_pcs_kernels() {
+  load_kernels({(const void *)k_fold_columns,
+                (const void *)k_comb_pow,
+                (const void *)k_mt_transpose,
+                (const void *)k_mt_col0,
+                (const void *)k_mt_dense,
+                (const void *)k_mt_gather,
+                (const void *)k_b3_chunks,
+                (const void *)k_b3_parents,
+                (const void *)k_b3_top,
+                (const void *)k_ring_claims,
+                (const void *)k_packed_basis,
+                (const void *)k_dot,
+                (const void *)k_axpy,
+                (const void *)k_rs_spread,
+                (const void *)k_rs_level,
+                (const void *)k_rs_encode_block,
+                (const void *)k_merkle_leaves,
+                (const void *)k_merkle_parents,
+                (const void *)k_merkle_block,
+                (const void *)k_query_basis,
+                (const void *)k_gather_openings});
 }
 
 }  // namespace bz

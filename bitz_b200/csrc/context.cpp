@@ -3,6 +3,8 @@
 #include <immintrin.h>
 
 #include <atomic>
+#include <mutex>
+#include <set>
 #include <chrono>
 #include <thread>
 
@@ -75,16 +77,58 @@ void RoundChannel::clear_down() {
   for (int k = 0; k < 2 * kMailboxWords; k++) s[k] = 0;
 }
 
+// The probe's verdict, set when the process's first lane is made: -1 not
+// yet probed, 0 the host cannot reach a running kernel, 1 it can.
+static std::atomic<int> g_host_reaches_kernel{-1};
+
 bool resident_rounds_enabled() {
-  static const bool on = [] {
+  static const int forced = [] {
     const char *e = getenv("BITZ_RESIDENT_ROUNDS");
-    if (e && e[0] == '0') return false;
-    if (e && e[0] == '1') return true;
+    if (e && e[0] == '0') return 0;
+    if (e && e[0] == '1') return 1;
     const char *inj = getenv("CUDA_INJECTION64_PATH");
-    return !(inj && inj[0]);
+    return (inj && inj[0]) ? 0 : -1;
   }();
+  const bool on = forced >= 0 ? forced == 1 : g_host_reaches_kernel.load() != 0;
   // probed launches are timed one by one, each its own round
   return on && !KernelProbe::get().active();
+}
+
+void load_kernels(std::initializer_list<const void *> kernels) {
+  cudaFuncAttributes a;
+  for (const void *k : kernels) BZ_CUDA(cudaFuncGetAttributes(&a, k));
+}
+
+void preload_pcs_kernels();
+void preload_eq_kernels();
+void preload_gkr_kernels();
+void preload_post_gkr_kernels();
+void preload_spartan_kernels();
+void preload_witness_kernels();
+void preload_diag_kernels();
+bool host_reaches_running_kernel(Context &lane);
+
+// Once per device, when its first lane is made: every kernel of the library
+// is loaded; and once per process, whether this host can reach a running
+// kernel is probed on that lane (a tool that holds the host at every launch
+// cannot run the kernels that wait for the host).
+static void lane_bootstrap(Context &lane) {
+  static std::mutex mu;
+  static std::set<int> loaded;
+  std::lock_guard<std::mutex> lk(mu);
+  int dev = 0;
+  BZ_CUDA(cudaGetDevice(&dev));
+  if (loaded.insert(dev).second) {
+    preload_pcs_kernels();
+    preload_eq_kernels();
+    preload_gkr_kernels();
+    preload_post_gkr_kernels();
+    preload_spartan_kernels();
+    preload_witness_kernels();
+    preload_diag_kernels();
+  }
+  if (g_host_reaches_kernel.load() < 0)
+    g_host_reaches_kernel.store(host_reaches_running_kernel(lane) ? 1 : 0);
 }
 
 // ------------------------------------------------------------ DeviceGate
@@ -172,6 +216,7 @@ Context::Context() {
   pg_.channel = &channel_;
   pg_.ctl = gk_ctl_.get();
   gk_.channel = &channel_;
+  lane_bootstrap(*this);
 }
 
 Context::~Context() {

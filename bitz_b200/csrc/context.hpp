@@ -3,6 +3,7 @@
 #pragma once
 #include <cuda_runtime.h>
 
+#include <initializer_list>
 #include <map>
 #include <memory>
 #include <mutex>
@@ -161,6 +162,11 @@ class Context {
   RoundChannel channel_;
   DeviceBuffer<unsigned int> counter_;
 };
+
+// Loads kernels now (cudaFuncGetAttributes), so no kernel is loaded on its
+// first launch while a kernel that waits for a host thread is in flight: a
+// load may wait for the running kernels to finish.
+void load_kernels(std::initializer_list<const void *> kernels);
 
 // A lane held for one proof: the process's default lane when no other proof
 // holds it, else one from the process's lane pool (given back when the lease

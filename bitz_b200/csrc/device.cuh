@@ -258,13 +258,14 @@ struct RoundLink {
 constexpr unsigned long long kRoundWaitNs = 2000000000ull;  // 2 s per challenge
 
 // Whether kernels that wait for their lane's host thread may run (resident
-// tails, queued rounds, the resident middle rounds). Resolved once per
-// process: BITZ_RESIDENT_ROUNDS=0 turns them off and =1 on; unset, they are
-// on unless a CUDA injection tool is attached (Nsight Compute and
-// compute-sanitizer set CUDA_INJECTION64_PATH). Such a tool serialises
-// launches and holds the host thread at each one, so a kernel that waits for
-// the host would sit out its time limit. The proof bytes are the same either
-// way.
+// tails, queued rounds, the resident middle rounds). BITZ_RESIDENT_ROUNDS=0
+// turns them off and =1 on. Otherwise they are off when a CUDA injection tool
+// announces itself (CUDA_INJECTION64_PATH), or when the process's first lane
+// found that its host thread cannot reach a running kernel (a kernel that
+// waits up to 100 ms for one word from the host got none): a kernel profiler
+// holds the host at every launch until the kernel has finished, so a kernel
+// that waits for the host would sit out its time limit. The proof bytes are
+// the same either way.
 bool resident_rounds_enabled();
 
 // Kernels that wait for their lane's host thread, and calls that wait for the

@@ -23,6 +23,36 @@ __global__ void k_ping_pong(Mailbox *mb, unsigned long long seq0, const Mailbox 
   }
 }
 
+// One thread waits up to limit_ns for the host's word (downbox publication
+// dseq) and posts it back plus one as publication seq, or zero when the word
+// never came while the kernel ran.
+__global__ void k_host_echo(Mailbox *mb, unsigned long long seq, const Mailbox *down,
+                            unsigned long long dseq, unsigned long long limit_ns) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  unsigned long long v = 0;
+  const bool got = mailbox_wait_device(down, dseq, 1, &v, limit_ns);
+  mailbox_post(mb, seq, 0, got ? v + 1 : 0);
+}
+
+// Whether this host thread can talk to a kernel while the kernel runs: false
+// under a tool that holds the host at every launch until the kernel has
+// finished (a kernel profiler), where every kernel that waits for the host
+// would sit out its time limit. Costs one round trip, 100 ms at most.
+bool host_reaches_running_kernel(Context &lane) {
+  cudaStream_t s = lane.stream();
+  RoundChannel *ch = lane.channel();
+  const uint64_t word = 0x5eedull;
+  const Publish p = ch->arm();
+  k_host_echo<<<1, 32, 0, s>>>(p.mailbox, p.seq, ch->down_dev, ch->down_next + 1, 100000000ull);
+  BZ_LAUNCH_CHECK();
+  ch->send(&word, 1);
+  uint64_t out = 0;
+  ch->wait(s, &out, 1);
+  BZ_CUDA(cudaStreamSynchronize(s));
+  ch->clear_down();
+  return out == word + 1;
+}
+
 // Mean microseconds per round over `rounds` rounds: mode 0 launches one
 // kernel per round, mode 1 runs one resident kernel that waits for the host.
 double diag_round_trip(int mode, int rounds) {
@@ -130,6 +160,17 @@ double diag_gf_peak(int kind, int blocks_per_sm) {
                    : kind == 1 ? time_gf_peak<1>(blocks, iters, y, sink.get(), s)
                                : time_gf_peak<2>(blocks, iters, y, sink.get(), s);
   return (double)blocks * kThreads * kPeakChains * iters / (ms * 1e-3);
+}
+
+// Every kernel of this file, loaded when the process's first lane on a device
+// is made (lane_bootstrap, context.cpp).
+void preload_diag_kernels() {
+  load_kernels({(const void *)k_post_once,
+                (const void *)k_ping_pong,
+                (const void *)k_host_echo,
+                (const void *)k_gf_peak<0>,
+                (const void *)k_gf_peak<1>,
+                (const void *)k_gf_peak<2>});
 }
 
 }  // namespace bz

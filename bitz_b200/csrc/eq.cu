@@ -1,5 +1,7 @@
 #include "eq.cuh"
 
+#include "context.hpp"
+
 namespace bz {
 
 // Both factor tables in one launch: block 0 the low a coordinates, block 1
@@ -33,6 +35,13 @@ void eq_table_device(const f128 *point, int n, f128 *out, f128 *scratch, cudaStr
   size_t total = (size_t)1 << n;
   eq_expand_kernel<<<grid_for(total), kThreads, 0, s>>>(lo, a, hi, out, total);
   BZ_LAUNCH_CHECK();
+}
+
+// Every kernel of this file, loaded when the process's first lane on a device
+// is made (lane_bootstrap, context.cpp).
+void preload_eq_kernels() {
+  load_kernels({(const void *)eq_factors_kernel,
+                (const void *)eq_expand_kernel});
 }
 
 }  // namespace bz

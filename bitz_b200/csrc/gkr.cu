@@ -815,4 +815,18 @@ f128 gkr_prove(int s, const f128 *zeta, uint32_t grind_bits, Transcript &ts, Gkr
   return claim;
 }
 
+// Every kernel of this file, loaded when the process's first lane on a device
+// is made (lane_bootstrap, context.cpp).
+void preload_gkr_kernels() {
+  load_kernels({(const void *)gkr_leaves,
+                (const void *)gkr_parent,
+                (const void *)gkr_layer_setup,
+                (const void *)gkr_top_sums,
+                (const void *)gkr_bind_sums,
+                (const void *)gkr_round,
+                (const void *)gkr_mid,
+                (const void *)gkr_final_bind,
+                (const void *)gkr_tail});
+}
+
 }  // namespace bz

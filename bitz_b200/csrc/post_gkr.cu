@@ -593,4 +593,15 @@ int post_gkr_prove(const PostGkrArgs &a, Transcript &ts, PostGkrScratch &sc, cud
   return geq(gmul(fin[0], fin[1]), claim) ? BZ_OK : BZ_ERR_INTERNAL;
 }
 
+// Every kernel of this file, loaded when the process's first lane on a device
+// is made (lane_bootstrap, context.cpp).
+void preload_post_gkr_kernels() {
+  load_kernels({(const void *)pg_first_message,
+                (const void *)pg_first_fold,
+                (const void *)pg_round,
+                (const void *)pg_sums,
+                (const void *)pg_tail,
+                (const void *)pg_mid});
+}
+
 }  // namespace bz

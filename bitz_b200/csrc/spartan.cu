@@ -1068,4 +1068,27 @@ void fp_canonical_device(const fp *in, size_t n, const FpCtx &c, fp *out, cudaSt
 
 fp fp_to_mont(u128 v, const FpCtx &c) { return fp_mul(fp{(uint64_t)v, (uint64_t)(v >> 64)}, c.r2, c); }
 
+// Every kernel of this file, loaded when the process's first lane on a device
+// is made (lane_bootstrap, context.cpp).
+void preload_spartan_kernels() {
+  load_kernels({(const void *)k_fp_eq_factor,
+                (const void *)k_fp_eq_expand,
+                (const void *)k_products_to_fp,
+                (const void *)k_outer_round,
+                (const void *)k_inner_round,
+                (const void *)k_fp_finalize<1>,
+                (const void *)k_fp_finalize<2>,
+                (const void *)k_fp_finalize<3>,
+                (const void *)k_bind_table,
+                (const void *)k_bind,
+                (const void *)k_bind_col0,
+                (const void *)k_bind_col0_finish,
+                (const void *)sp_outer_tail,
+                (const void *)sp_inner_tail,
+                (const void *)sp_mid<4, 3>,
+                (const void *)sp_mid<2, 2>,
+                (const void *)k_fp_dot,
+                (const void *)k_fp_canonical});
+}
+
 }  // namespace bz

@@ -8,6 +8,7 @@
 // commitment and the BitZ table read (end_to_end.rs:499-507).
 #include "device.cuh"
 #include "witness.hpp"
+#include "context.hpp"
 
 namespace bz {
 
@@ -187,6 +188,14 @@ void witness_generate(const WitnessArgs &a, cudaStream_t s) {
       a.abc_off[2], a.abc_col[2], a.abc_coef[2], a.h, a.rows, a.n_inputs, a.bit_c, a.prod,
       a.unsat);
   BZ_LAUNCH_CHECK();
+}
+
+// Every kernel of this file, loaded when the process's first lane on a device
+// is made (lane_bootstrap, context.cpp).
+void preload_witness_kernels() {
+  load_kernels({(const void *)k_sha_hints,
+                (const void *)k_hbits,
+                (const void *)k_products});
 }
 
 }  // namespace bz

@@ -182,9 +182,11 @@ unsigned long long bitz_launch_count(void);
 /* Diagnostic (no reference counterpart): 1 when kernels that wait for the
  * host thread (resident and queued sumcheck rounds) are in use, 0 when every
  * round is its own launch. BITZ_RESIDENT_ROUNDS=0/1 forces the mode; unset,
- * it is off when a CUDA injection tool (a kernel profiler or sanitizer) is
- * attached, since such a tool holds the host at every launch. Proof bytes are
- * the same in both modes. Needs no GPU. */
+ * it is off when a CUDA injection tool announces itself
+ * (CUDA_INJECTION64_PATH) or when the first prover lane found that the host
+ * cannot reach a running kernel (a kernel profiler holds the host at every
+ * launch). Proof bytes are the same in both modes. Needs no GPU (before the
+ * first lane exists it reports the environment's answer). */
 int bitz_resident_rounds(void);
 /* Diagnostic (no reference counterpart): on the default lane since the
  * process started, out[0] the nanoseconds the host spent waiting for round
