@@ -82,6 +82,8 @@ SIGNATURES = [
      [ctypes.c_char_p, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_ulonglong)]),
     ("bitz_probe_kernels", ctypes.c_size_t, [ctypes.c_char_p, ctypes.c_size_t]),
     ("bitz_l2_flush", ctypes.c_int, []),
+    ("bitz_diag_fibers", ctypes.c_int,
+     [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_ulonglong)]),
     ("bitz_diag_gf_peak", ctypes.c_int, [ctypes.c_int, ctypes.POINTER(ctypes.c_double)]),
     ("bitz_diag_round_trip", ctypes.c_int,
      [ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_double)]),

@@ -259,7 +259,7 @@ void blake3_tree_cv(const uint8_t *data, size_t nchunks, const uint32_t key[8], 
   }
   BZ_CUDA(cudaMemcpyAsync(cv_out, a, 32, cudaMemcpyDeviceToHost, s));
   if (extra) BZ_CUDA(cudaMemcpyAsync(extra_out, extra, 16, cudaMemcpyDeviceToHost, s));
-  BZ_CUDA(cudaStreamSynchronize(s));
+  BZ_CUDA(stream_wait(s));
 }
 
 // ----------------------------------------------------------- ring switch

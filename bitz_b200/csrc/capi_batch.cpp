@@ -22,6 +22,7 @@
 #include <vector>
 
 #include "../../include/bitz_b200.h"
+#include "fiber.hpp"
 #include "prover.hpp"
 #include "status.hpp"
 
@@ -70,6 +71,19 @@ class LanePool {
   std::mutex mu_;
   std::unordered_map<int, std::vector<std::unique_ptr<Context>>> idle_;
 };
+
+// Host threads for `lanes` lanes: one per lane up to the host's hardware
+// threads (BITZ_LANE_THREADS overrides the cap); beyond that, lanes share
+// threads as fibers.
+int lane_threads(int lanes) {
+  static const int cap = [] {
+    const char *e = getenv("BITZ_LANE_THREADS");
+    if (e && atoi(e) > 0) return atoi(e);
+    const unsigned hw = std::thread::hardware_concurrency();
+    return (int)std::max(1u, hw);
+  }();
+  return std::max(1, std::min(lanes, cap));
+}
 
 double ms_between(std::chrono::steady_clock::time_point a, std::chrono::steady_clock::time_point b) {
   return std::chrono::duration<double, std::milli>(b - a).count();
@@ -267,7 +281,6 @@ int bitz_batch_prove(bitz_system *const *systems, size_t n, int lanes, uint8_t *
   std::vector<int> status(n, BZ_OK);
   std::vector<std::string> errors(n);
   auto worker = [&](Context *lane) {
-    cudaSetDevice(device);
     for (size_t i; (i = next.fetch_add(1)) < n;) {
       std::vector<uint8_t> proof;
       auto ts = std::chrono::steady_clock::now();
@@ -283,9 +296,24 @@ int bitz_batch_prove(bitz_system *const *systems, size_t n, int lanes, uint8_t *
       }
     }
   };
+  // lane k runs on host thread k mod nt; a thread with several lanes runs
+  // each as a fiber that yields wherever it waits for the device
+  const int nt = lane_threads(nl);
+  auto thread_main = [&](int t) {
+    cudaSetDevice(device);
+    std::vector<Context *> mine;
+    for (int k = t; k < nl; k += nt) mine.push_back(pool[k].get());
+    if (mine.size() == 1) {
+      worker(mine[0]);
+      return;
+    }
+    FiberLoop loop;
+    for (Context *c : mine) loop.add([&worker, c] { worker(c); });
+    loop.run();
+  };
   std::vector<std::thread> threads;
-  for (int k = 1; k < nl; k++) threads.emplace_back(worker, pool[k].get());
-  worker(pool[0].get());
+  for (int t = 1; t < nt; t++) threads.emplace_back(thread_main, t);
+  thread_main(0);
   for (auto &t : threads) t.join();
   LanePool::get().give(device, pool);
   for (size_t i = 0; i < n; i++)
@@ -439,6 +467,18 @@ int bitz_diag_round_trip(int mode, int rounds, double *us_per_round) {
     return BZ_OK;
   } catch (const std::exception &e) {
     return capi_fail(BZ_ERR_CUDA, e.what());
+  }
+}
+
+int bitz_diag_fibers(int threads, int fibers, int yields, unsigned long long *checksum) {
+  if (!checksum || threads < 1 || threads > 64 || fibers < 1 || fibers > 256 || yields < 2)
+    return capi_fail(BZ_ERR_ARGUMENT, "bad argument");
+  try {
+    bool ok = false;
+    *checksum = fiber_selftest(threads, fibers, yields, &ok);
+    return ok ? BZ_OK : capi_fail(BZ_ERR_INTERNAL, "fiber self-test failed");
+  } catch (const std::exception &e) {
+    return capi_fail(BZ_ERR_INTERNAL, e.what());
   }
 }
 

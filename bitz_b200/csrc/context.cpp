@@ -1,5 +1,7 @@
 #include "context.hpp"
 
+#include "fiber.hpp"
+
 #include <immintrin.h>
 
 #include <atomic>
@@ -38,8 +40,11 @@ void RoundChannel::wait(cudaStream_t s, uint64_t *out, int n) {
       if (std::chrono::steady_clock::now() - t0 > std::chrono::seconds(30))
         throw CudaError("timed out waiting for a round result");
     }
-    // spin briefly, then give the core to other lanes' host threads
-    if (spins < 4096)
+    // on a fiber, let the thread's other lanes run; else spin briefly, then
+    // give the core to other lanes' host threads
+    if (in_fiber())
+      fiber_yield();
+    else if (spins < 4096)
       _mm_pause();
     else
       std::this_thread::yield();
@@ -133,17 +138,24 @@ static void lane_bootstrap(Context &lane) {
 
 // ------------------------------------------------------------ DeviceGate
 
-static thread_local int resident_depth = 0;
-static thread_local int alloc_depth = 0;
-
 DeviceGate &DeviceGate::get() {
   static DeviceGate *g = new DeviceGate();
   return *g;
 }
 
+// A fiber must not block its thread in the gate: the thread's other fibers
+// may hold the scopes it waits for. It polls and yields instead.
 void DeviceGate::enter_resident() {
   std::unique_lock<std::mutex> lk(mu_);
-  cv_.wait(lk, [&] { return !alloc_ && allocs_waiting_ == 0; });
+  if (in_fiber()) {
+    while (alloc_ || allocs_waiting_ != 0) {
+      lk.unlock();
+      fiber_yield();
+      lk.lock();
+    }
+  } else {
+    cv_.wait(lk, [&] { return !alloc_ && allocs_waiting_ == 0; });
+  }
   residents_++;
 }
 
@@ -155,7 +167,15 @@ void DeviceGate::leave_resident() {
 void DeviceGate::enter_alloc() {
   std::unique_lock<std::mutex> lk(mu_);
   allocs_waiting_++;
-  cv_.wait(lk, [&] { return !alloc_ && residents_ == 0; });
+  if (in_fiber()) {
+    while (alloc_ || residents_ != 0) {
+      lk.unlock();
+      fiber_yield();
+      lk.lock();
+    }
+  } else {
+    cv_.wait(lk, [&] { return !alloc_ && residents_ == 0; });
+  }
   allocs_waiting_--;
   alloc_ = true;
 }
@@ -167,24 +187,24 @@ void DeviceGate::leave_alloc() {
 }
 
 ResidentScope::ResidentScope(bool on) : on_(on) {
-  if (on_ && resident_depth++ == 0) DeviceGate::get().enter_resident();
+  if (on_ && gate_depth().resident++ == 0) DeviceGate::get().enter_resident();
 }
 
 ResidentScope::~ResidentScope() {
-  if (on_ && --resident_depth == 0) DeviceGate::get().leave_resident();
+  if (on_ && --gate_depth().resident == 0) DeviceGate::get().leave_resident();
 }
 
 AllocScope::AllocScope(bool strict) {
-  if (resident_depth > 0) {
+  if (gate_depth().resident > 0) {
     if (strict) throw CudaError("device allocation while a round kernel of this lane may wait");
     return;  // unwinding out of a resident stretch: free without the gate
   }
   on_ = true;
-  if (alloc_depth++ == 0) DeviceGate::get().enter_alloc();
+  if (gate_depth().alloc++ == 0) DeviceGate::get().enter_alloc();
 }
 
 AllocScope::~AllocScope() {
-  if (on_ && --alloc_depth == 0) DeviceGate::get().leave_alloc();
+  if (on_ && --gate_depth().alloc == 0) DeviceGate::get().leave_alloc();
 }
 
 Context::Context() {

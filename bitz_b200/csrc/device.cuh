@@ -11,6 +11,7 @@
 #include <stdexcept>
 #include <string>
 
+#include "fiber.hpp"
 #include "field.cuh"
 
 namespace bz {

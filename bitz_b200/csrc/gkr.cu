@@ -581,7 +581,7 @@ static void round_read(GkrScratch &sc, const void *src, cudaStream_t s) {
     return;
   }
   BZ_CUDA(cudaMemcpyAsync(sc.host, src, 32, cudaMemcpyDeviceToHost, s));
-  BZ_CUDA(cudaStreamSynchronize(s));
+  BZ_CUDA(stream_wait(s));
 }
 
 void gkr_build(const f128 *cols, int s, const f128 *images, GkrScratch &sc, cudaStream_t st_) {
@@ -806,7 +806,7 @@ f128 gkr_prove(int s, const f128 *zeta, uint32_t grind_bits, Transcript &ts, Gkr
   } catch (...) {
     if (tail) {  // release the waiting kernel before the lane is reused
       ch->abort();
-      cudaStreamSynchronize(st_);
+      stream_wait(st_);
       ch->clear_down();
     }
     throw;

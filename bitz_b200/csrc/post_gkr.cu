@@ -283,7 +283,7 @@ static void round_read(PostGkrScratch &sc, const unsigned long long *d_acc, int 
     return;
   }
   BZ_CUDA(cudaMemcpyAsync(sc.host, d_acc, words * 8, cudaMemcpyDeviceToHost, s));
-  BZ_CUDA(cudaStreamSynchronize(s));
+  BZ_CUDA(stream_wait(s));
 }
 
 // The post-GKR rounds km .. t0-1 in one cooperative launch that stays
@@ -572,7 +572,7 @@ int post_gkr_prove(const PostGkrArgs &a, Transcript &ts, PostGkrScratch &sc, cud
   } catch (...) {
     if (tail) {  // release the waiting kernel before the lane is reused
       ch->abort();
-      cudaStreamSynchronize(s);
+      stream_wait(s);
       ch->clear_down();
     }
     throw;
@@ -586,7 +586,7 @@ int post_gkr_prove(const PostGkrArgs &a, Transcript &ts, PostGkrScratch &sc, cud
   } else {
     BZ_CUDA(cudaMemcpyAsync(fin, w, 16, cudaMemcpyDeviceToHost, s));
     BZ_CUDA(cudaMemcpyAsync(fin + 1, v, 16, cudaMemcpyDeviceToHost, s));
-    BZ_CUDA(cudaStreamSynchronize(s));
+    BZ_CUDA(stream_wait(s));
   }
   *value_out = fin[1];
   ts.prover_f128(fin[1]);

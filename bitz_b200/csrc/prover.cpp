@@ -112,7 +112,7 @@ struct Phases {
   }
   void mark(const char *name) {
     if (!on) return;
-    cudaStreamSynchronize(s);
+    stream_wait(s);
     double wait_ms = ch ? (ch->wait_ns - w0) * 1e-6 : 0.0;
     unsigned long long waits = ch ? ch->waits - n0 : 0;
     fprintf(stderr, "[phase] %-22s %8.3f ms  (%llu round waits, %.3f ms waiting)\n", name,
@@ -184,7 +184,7 @@ std::shared_ptr<DeviceSetup> device_setup(int kind, size_t n_inputs, cudaStream_
   d->tab_which.upload(which.data(), which.size(), s);
   d->ntab = (int)vals.size();
   d->col0_nnz = cnt[1];
-  BZ_CUDA(cudaStreamSynchronize(s));
+  BZ_CUDA(stream_wait(s));
   g_setups[key] = d;
   return d;
 }
@@ -204,7 +204,7 @@ Tables &tables(cudaStream_t s) {
     t->wh_host.resize(kMaxRsDim * kMaxRsDim);
     subspace_table(kMaxRsDim, t->wh_host.data());
     t->wh.upload(t->wh_host.data(), t->wh_host.size(), s);
-    BZ_CUDA(cudaStreamSynchronize(s));
+    BZ_CUDA(stream_wait(s));
   }
   return *t;
 }
@@ -256,7 +256,7 @@ ProofSystem::ProofSystem(int kind, const uint8_t *inputs, size_t n_inputs, const
   serial_ = ++serials;
   BZ_CUDA(cudaEventCreate(&ev_start_));
   BZ_CUDA(cudaEventCreate(&ev_stop_));
-  BZ_CUDA(cudaStreamSynchronize(s));
+  BZ_CUDA(stream_wait(s));
 }
 
 uint64_t ProofSystem::footprint_bytes(int kind, size_t n_inputs) {
@@ -321,7 +321,7 @@ int ProofSystem::witness(cudaStream_t s) {
   witness_generate(a, s);
   int *unsat_h = reinterpret_cast<int *>(W.pin_small.get(kPinSmall) + kPinFlag);
   BZ_CUDA(cudaMemcpyAsync(unsat_h, W.flag.get(), sizeof(int), cudaMemcpyDeviceToHost, s));
-  BZ_CUDA(cudaStreamSynchronize(s));
+  BZ_CUDA(stream_wait(s));
   if (*unsat_h) {
     error = "circuit witness does not satisfy the constraints";
     return BZ_ERR_UNSATISFIED;
@@ -399,7 +399,7 @@ int ProofSystem::commit(cudaStream_t s) {
   } else {
     merkle_build(codeword0_->get(), rows, L0.k, nodes0_->get(), s);
     BZ_CUDA(cudaMemcpyAsync(root_h, nodes0_->get() + 8, 32, cudaMemcpyDeviceToHost, s));
-    BZ_CUDA(cudaStreamSynchronize(s));
+    BZ_CUDA(stream_wait(s));
   }
   memcpy(root_, root_h, 32);
   const char *dom = circuit_name(kind_);
@@ -514,7 +514,7 @@ std::vector<uint8_t> ProofSystem::ligerito(cudaStream_t s, f128 target) {
         }
       } catch (...) {  // release the waiting kernel before the lane is reused
         ch->abort();
-        cudaStreamSynchronize(s);
+        stream_wait(s);
         ch->clear_down();
         throw;
       }
@@ -560,7 +560,7 @@ std::vector<uint8_t> ProofSystem::ligerito(cudaStream_t s, f128 target) {
         merkle_build(next_cw[flip].get(), nrows, N.k, next_nodes[flip].get(), s);
         BZ_CUDA(cudaMemcpyAsync(root_h, next_nodes[flip].get() + 8, 32, cudaMemcpyDeviceToHost,
                                 s));
-        BZ_CUDA(cudaStreamSynchronize(s));
+        BZ_CUDA(stream_wait(s));
       }
       uint8_t root[36];
       uint32_t len = 32;
@@ -583,7 +583,7 @@ std::vector<uint8_t> ProofSystem::ligerito(cudaStream_t s, f128 target) {
     } else {
       f128 *hf = W.pin_f.get(n);
       BZ_CUDA(cudaMemcpyAsync(hf, f, n * 16, cudaMemcpyDeviceToHost, s));
-      BZ_CUDA(cudaStreamSynchronize(s));
+      BZ_CUDA(stream_wait(s));
       uint32_t cnt = (uint32_t)n;
       t.prover_message(&cnt, 4);
       t.prover_message(hf, n * 16);  // one f128 message per entry, no framing between
@@ -605,7 +605,7 @@ std::vector<uint8_t> ProofSystem::ligerito(cudaStream_t s, f128 target) {
     f128 *opened = W.pin_open.get(stride * L.queries);
     BZ_CUDA(cudaMemcpyAsync(opened, W.openings.get(), stride * L.queries * 16,
                             cudaMemcpyDeviceToHost, s));
-    BZ_CUDA(cudaStreamSynchronize(s));
+    BZ_CUDA(stream_wait(s));
     put_u64(proof, (uint64_t)L.queries);
     const uint8_t *ob = reinterpret_cast<const uint8_t *>(opened);
     proof.insert(proof.end(), ob, ob + stride * L.queries * 16);
@@ -646,7 +646,7 @@ std::vector<uint8_t> ProofSystem::ligerito(cudaStream_t s, f128 target) {
   f128 *hf = W.pin_f.get(n), *hb = W.pin_b.get(n);
   BZ_CUDA(cudaMemcpyAsync(hf, f, n * 16, cudaMemcpyDeviceToHost, s));
   BZ_CUDA(cudaMemcpyAsync(hb, b, n * 16, cudaMemcpyDeviceToHost, s));
-  BZ_CUDA(cudaStreamSynchronize(s));
+  BZ_CUDA(stream_wait(s));
   f128 chk = mk(0, 0);
   for (size_t j = 0; j < n; j++) chk = gadd(chk, gmul(hb[j], hf[j]));
   if (!geq(chk, claim)) proof.clear();
@@ -800,7 +800,7 @@ int ProofSystem::prove_after_commit(cudaStream_t s, std::vector<uint8_t> &proof)
     for (auto w : rows_w) put_u128(head, w);
     put_u64(head, ncol);
     t.public_message(head.data(), head.size());
-    BZ_CUDA(cudaEventSynchronize(W.ev_cols));
+    BZ_CUDA(event_wait(W.ev_cols));
     t.public_message(cols_h, ncol * 16);
     std::vector<uint8_t> tail;
     put_u128(tail, target_p);
@@ -808,7 +808,7 @@ int ProofSystem::prove_after_commit(cudaStream_t s, std::vector<uint8_t> &proof)
   }
   t.public_message(pcs_enc_.data(), pcs_enc_.size());
   ph.mark("claim");
-  BZ_CUDA(cudaEventSynchronize(W.ev_folds));
+  BZ_CUDA(event_wait(W.ev_folds));
   t.prover_message(folds_h, ncol * 16);
   std::vector<f128> row_images(row_images_h, row_images_h + 128);
   t.grind("bitz/columns/v1", grinding_bits((uint32_t)security_, (uint64_t)sc_cols));
@@ -907,7 +907,7 @@ int ProofSystem::prove_after_commit(cudaStream_t s, std::vector<uint8_t> &proof)
   ring_claims(pa.packed, W.suffix.get(), np, W.acc.get(), s);
   f128 *claims_h = W.pin_small.get(kPinSmall) + kPinClaims;
   BZ_CUDA(cudaMemcpyAsync(claims_h, W.acc.get(), 128 * 16, cudaMemcpyDeviceToHost, s));
-  BZ_CUDA(cudaStreamSynchronize(s));
+  BZ_CUDA(stream_wait(s));
   std::vector<f128> claims(claims_h, claims_h + 128);
   {
     std::vector<f128> pre(128);
@@ -1046,7 +1046,7 @@ int ProofSystem::split_prove(std::vector<uint8_t> &proof) {
   cudaStream_t s = lane_->stream();
   int rc = prove_after_commit(s, proof);
   BZ_CUDA(cudaEventRecord(ev_stop_, s));
-  BZ_CUDA(cudaEventSynchronize(ev_stop_));
+  BZ_CUDA(event_wait(ev_stop_));
   KernelProbe::get().collect();
   return rc;
 }
@@ -1081,7 +1081,7 @@ int ProofSystem::prove(std::vector<uint8_t> &proof, StageTimes *times, bool rest
   auto t2 = std::chrono::steady_clock::now();
   rc = prove_after_commit(s, proof);
   BZ_CUDA(cudaEventRecord(ev_stop_, s));
-  BZ_CUDA(cudaEventSynchronize(ev_stop_));
+  BZ_CUDA(event_wait(ev_stop_));
   KernelProbe::get().collect();
   if (times) {
     times->witness_ms = tw;
@@ -1106,7 +1106,7 @@ void ProofSystem::download_witness(std::vector<uint32_t> &f, std::vector<uint32_
   f_->download(f.data(), f.size(), s);
   h_->download(h.data(), h.size(), s);
   prod_->download(prod.data(), prod.size(), s);
-  BZ_CUDA(cudaStreamSynchronize(s));
+  BZ_CUDA(stream_wait(s));
 }
 
 }  // namespace bz

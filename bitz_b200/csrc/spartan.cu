@@ -483,7 +483,7 @@ static fp host_partial_sum(const fp *d_partial, int nblocks, int N, fp *d_out, f
     ch->wait(s, reinterpret_cast<uint64_t *>(h_out), 2 * N);
   } else {
     BZ_CUDA(cudaMemcpyAsync(h_out, d_out, N * sizeof(fp), cudaMemcpyDeviceToHost, s));
-    BZ_CUDA(cudaStreamSynchronize(s));
+    BZ_CUDA(stream_wait(s));
   }
   return h_out[0];
 }
@@ -806,13 +806,13 @@ void spartan_prove(const SpartanArgs &a, Transcript &ts, SpartanScratch &sc, cud
     BZ_CUDA(cudaMemcpyAsync(&fin[0], A2, sizeof(fp), cudaMemcpyDeviceToHost, s));
     BZ_CUDA(cudaMemcpyAsync(&fin[1], B2, sizeof(fp), cudaMemcpyDeviceToHost, s));
     BZ_CUDA(cudaMemcpyAsync(&fin[2], C2, sizeof(fp), cudaMemcpyDeviceToHost, s));
-    BZ_CUDA(cudaStreamSynchronize(s));
+    BZ_CUDA(stream_wait(s));
   }
   }
   } catch (...) {
     if (tail) {  // release the waiting kernel before the lane is reused
       ch->abort();
-      cudaStreamSynchronize(s);
+      stream_wait(s);
       ch->clear_down();
     }
     throw;
@@ -967,13 +967,13 @@ void spartan_prove(const SpartanArgs &a, Transcript &ts, SpartanScratch &sc, cud
     BZ_LAUNCH_CHECK();
     BZ_CUDA(cudaMemcpyAsync(&dw[0], D2, sizeof(fp), cudaMemcpyDeviceToHost, s));
     BZ_CUDA(cudaMemcpyAsync(&dw[1], W2, sizeof(fp), cudaMemcpyDeviceToHost, s));
-    BZ_CUDA(cudaStreamSynchronize(s));
+    BZ_CUDA(stream_wait(s));
   }
   }
   } catch (...) {
     if (tail) {
       ch->abort();
-      cudaStreamSynchronize(s);
+      stream_wait(s);
       ch->clear_down();
     }
     throw;
@@ -1025,7 +1025,7 @@ fp spartan_matrix_eval(const SpartanArgs &a, const fp *rx, fp rho, const fp *ry,
   k_fp_finalize<1><<<1, kThreads, 0, s>>>(sc.partial, g, c, sc.sums, Publish{nullptr, nullptr, 0});
   BZ_LAUNCH_CHECK();
   BZ_CUDA(cudaMemcpyAsync(sc.host, sc.sums, sizeof(fp), cudaMemcpyDeviceToHost, s));
-  BZ_CUDA(cudaStreamSynchronize(s));
+  BZ_CUDA(stream_wait(s));
   return sc.host[0];
 }
 

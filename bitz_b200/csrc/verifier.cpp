@@ -346,7 +346,7 @@ int ProofSystem::verify(const uint8_t *proof, size_t proof_len, Context *lane) {
   fp_eq_table(pt.data() + 7, sc_cols, fc, W.cols_fp.get(), sc.eq_scratch, s);
   fp_canonical_device(W.cols_fp.get(), ncol, fc, W.cols_canon.get(), s);
   BZ_CUDA(cudaMemcpyAsync(cols_w.data(), W.cols_canon.get(), ncol * 16, cudaMemcpyDeviceToHost, s));
-  BZ_CUDA(cudaStreamSynchronize(s));
+  BZ_CUDA(stream_wait(s));
   const u128 fin_c = fp_canonical(fin, fc);
   t.public_message("bitz/virtual-statement/v1", 25);
   t.public_message(root, 32);
@@ -404,7 +404,7 @@ int ProofSystem::verify(const uint8_t *proof, size_t proof_len, Context *lane) {
   BZ_CUDA(cudaMemsetAsync(W.acc.get(), 0, 16, s));
   dot(W.u2.get(), W.images.get() + 128, ncol, W.acc.get(), Publish{nullptr, nullptr, 0}, s);
   BZ_CUDA(cudaMemcpyAsync(W.host_acc, W.acc.get(), 16, cudaMemcpyDeviceToHost, s));
-  BZ_CUDA(cudaStreamSynchronize(s));
+  BZ_CUDA(stream_wait(s));
   f128 gclaim = mk(W.host_acc[0], W.host_acc[1]);
   const uint32_t gkr_bits = grinding_bits((uint32_t)security_, 3);
   for (int layer = 0; layer < 7; layer++) {
@@ -503,7 +503,7 @@ int ProofSystem::verify(const uint8_t *proof, size_t proof_len, Context *lane) {
     BZ_CUDA(cudaMemsetAsync(W.acc.get(), 0, 16, s));
     dot(W.eq.get(), W.weights.get(), nbits, W.acc.get(), Publish{nullptr, nullptr, 0}, s);
     BZ_CUDA(cudaMemcpyAsync(W.host_acc, W.acc.get(), 16, cudaMemcpyDeviceToHost, s));
-    BZ_CUDA(cudaStreamSynchronize(s));
+    BZ_CUDA(stream_wait(s));
     const f128 wv = mk(W.host_acc[0], W.host_acc[1]);
     BZ_VERIFY(geq(gmul(wv, v), pclaim), "inner-product sumcheck closing check");
   }
@@ -705,7 +705,7 @@ int ProofSystem::verify(const uint8_t *proof, size_t proof_len, Context *lane) {
   {
     std::vector<f128> hb(n);
     BZ_CUDA(cudaMemcpyAsync(hb.data(), b, n * 16, cudaMemcpyDeviceToHost, s));
-    BZ_CUDA(cudaStreamSynchronize(s));
+    BZ_CUDA(stream_wait(s));
     BZ_VERIFY(f_final.size() == n, "the final vector's length");
     wide chk = wzero();
     for (size_t j = 0; j < n; j++) wacc(chk, gmul_wide(hb[j], f_final[j]));

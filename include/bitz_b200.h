@@ -226,7 +226,10 @@ int bitz_statement_digest(int circuit_kind, const uint8_t *input_bits, size_t n_
  * advances on its own thread. Every proof's bytes are the same as the
  * single-proof call's for the same statement. */
 
-/* Proves systems[0..n) on `lanes` lanes (1..64). proofs[i] (freed with
+/* Proves systems[0..n) on `lanes` lanes (1..64), driven by one host thread
+ * per lane up to the host's hardware threads (BITZ_LANE_THREADS sets the
+ * cap); past it, lanes share threads as cooperative fibers that switch
+ * wherever a lane waits for the device. proofs[i] (freed with
  * bitz_free) and proof_lens[i] receive each proof; latency_ms[i] (may be
  * NULL) that proof's own duration, from its start on a lane to its bytes. Returns
  * the first failure's status after every proof has finished; failed entries
@@ -280,6 +283,12 @@ int bitz_probe_read(const char *kernel, double out[5], unsigned long long *launc
 /* The probed kernels that launched, comma-separated, into out (truncated to
  * cap - 1 characters); returns the full length. */
 size_t bitz_probe_kernels(char *out, size_t cap);
+/* Self-test of the fibers that let one host thread drive several prover
+ * lanes (no GPU): `threads` threads each run `fibers` fibers that yield
+ * `yields` times, throw and catch on their own stacks and keep their own
+ * gate counters. BZ_OK when every check holds; *checksum identifies the
+ * interleaving (the same for the same arguments). */
+int bitz_diag_fibers(int threads, int fibers, int yields, unsigned long long *checksum);
 /* Overwrites a 256 MiB device buffer and waits, evicting the L2 cache. */
 int bitz_l2_flush(void);
 /* Mean microseconds per host<->device round on the default lane: mode 0

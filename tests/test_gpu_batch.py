@@ -57,6 +57,31 @@ def test_batch_matches_alone(alone, lanes):
     assert all(x > 0 for x in lat)
 
 
+def test_lanes_sharing_host_threads_as_fibers(alone):
+    """Eight lanes on two host threads (four fibers each, switching wherever a
+    lane waits for the device): the same proofs. The thread cap is read once
+    per process, so this runs in a child process."""
+    import os
+    import subprocess
+    import sys
+    here = os.path.dirname(os.path.abspath(__file__))
+    code = ("import sys; sys.path[:0] = [%r, %r]\n"
+            "from test_gpu_batch import MIX, statement\n"
+            "import bitz_b200 as bz\n"
+            "systems = [bz.CircuitProofSystem(k, *statement(i, k, b), 100) "
+            "for i, (k, b) in enumerate(MIX)]\n"
+            "proofs, lat = bz.batch_prove(systems, 8)\n"
+            "again, _ = bz.batch_prove(systems, 8)\n"
+            "assert again == proofs\n"
+            "sys.stdout.write(''.join(p.hex() + '\\n' for p in proofs))\n") % (
+                here, os.path.dirname(here))
+    env = dict(os.environ, BITZ_LANE_THREADS="2")
+    r = subprocess.run([sys.executable, "-c", code], env=env, capture_output=True, text=True,
+                       timeout=600, cwd=here)
+    assert r.returncode == 0, r.stderr[-3000:]
+    assert [bytes.fromhex(x) for x in r.stdout.split()] == alone
+
+
 def test_batch_twice_on_the_same_systems(alone):
     systems = [bz.CircuitProofSystem(kind, *statement(i, kind, blocks), 100)
                for i, (kind, blocks) in enumerate(MIX)]
