@@ -169,11 +169,11 @@ def peaks():
         return {"hbm_gbs": FALLBACK_HBM_GBS}, "fallback"
 
 
-def profile_figure(kernel, key):
-    """A figure (e.g. DRAM bytes per launch) from the committed ncu summary of
-    ``kernel`` on this workload, or None: the lines ``key: value`` of
-    profiles/<kernel>_sha256-chain-n64.md."""
-    path = os.path.join(PROFILES, f"{kernel}_sha256-chain-n64.md")
+def profile_figure(summary, key):
+    """A figure (e.g. DRAM bytes per launch) from a committed ncu summary of
+    this workload, or None: the lines ``key: value`` of
+    profiles/<summary>_sha256-chain-n64.md."""
+    path = os.path.join(PROFILES, f"{summary}_sha256-chain-n64.md")
     try:
         for line in open(path):
             if line.startswith(key + ":"):
@@ -211,11 +211,11 @@ def roofline(bz, ps, steps, hbm_gbs, pk_kind):
         rows.append({"kernel": name, "launches": t["launches"] // steps,
                      "us_per_proof": 1e3 * t["ms"] / steps,
                      "avg_launch_us": 1e3 * t["ms"] / t["launches"],
-                     "share_of_device_time": t["ms"] / span_ms, "bound": bound,
+                     "share_of_device_span": t["ms"] / span_ms, "bound": bound,
                      "frac": max(t_hbm, t_int) / secs if secs > 0 else None,
                      "bytes_per_launch": t["bytes"] / t["launches"],
                      "products_per_launch": sum(t[k] for k in peaks) / t["launches"]})
-    rows.sort(key=lambda r: -r["share_of_device_time"])
+    rows.sort(key=lambda r: -r["share_of_device_span"])
     top = rows[0]
     t = table[top["kernel"]]
     secs = t["ms"] / 1e3
@@ -234,12 +234,18 @@ def roofline(bz, ps, steps, hbm_gbs, pk_kind):
     return {"kernel": top["kernel"], "bound": top["bound"], "achieved": achieved, "peak": peak,
             "unit": unit, "frac": achieved / peak, "peak_source": peak_source,
             "traffic": traffic,
-            "traffic_source": (f"ncu dram__bytes_read.sum + dram__bytes_write.sum per launch, "
+            "traffic_source": (f"ncu dram__bytes_read.sum + dram__bytes_write.sum, mean over the "
+                               f"captured launches of the committed summary "
                                f"profiles/{top['kernel']}_sha256-chain-n64.md") if traffic else None,
             "algorithmic_bytes_per_launch": top["bytes_per_launch"],
             "products_per_launch": top["products_per_launch"],
             "launches_per_proof": top["launches"], "avg_launch_us": top["avg_launch_us"],
-            "share_of_device_time": top["share_of_device_time"],
+            "share_of_device_span": top["share_of_device_span"],
+            "share_of_kernel_time_ncu": profile_figure(
+                "launches", f"{top['kernel']}_share_of_kernel_time"),
+            "share_note": "share_of_device_span: this run's CUDA-event kernel time over the proofs' "
+                          "device span (host waits included); share_of_kernel_time_ncu: the "
+                          "committed ncu launch list's share of summed kernel time",
             "mode": "every sumcheck round its own launch (as under ncu), events per launch",
             "kernels": rows[:8]}
 

@@ -1,6 +1,7 @@
 // The extern "C" boundary: argument checks, device staging for the host-buffer
 // variants, and exception-to-status translation. No exception crosses it.
 #include <cuda_runtime.h>
+#include <stdlib.h>
 
 #include <mutex>
 #include <string>
@@ -17,6 +18,16 @@ using namespace bz;
 struct bitz_transcript {
   Transcript t;
 };
+
+// Prover lanes are streams that each keep a round kernel waiting for their
+// host thread; with the CUDA default of 8 hardware work queues, lanes past 8
+// share queues, and a waiting kernel at the head of a queue holds back the
+// other lanes' launches behind it. When the library is loaded before the
+// process creates its CUDA context and the caller has not chosen, ask for 32
+// queues (the most the driver gives). A caller's own setting is kept.
+__attribute__((constructor)) static void bz_default_work_queues() {
+  setenv("CUDA_DEVICE_MAX_CONNECTIONS", "32", 0);
+}
 
 static thread_local std::string g_last_error;
 
