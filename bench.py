@@ -58,7 +58,9 @@ def parse():
     p.add_argument("--blocks", type=int, default=64)
     p.add_argument("--seed", type=int, default=1)
     p.add_argument("--security", type=int, default=100)
-    p.add_argument("--lanes", type=int, default=16)
+    p.add_argument("--lanes", type=int, default=None,
+                   help="prover lanes for the batched and serving workloads (default: the "
+                        "tuned count of bitz_b200/tuning.json, else 16)")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-batch", action="store_true")
     p.add_argument("--serve", action="store_true")
@@ -487,6 +489,7 @@ def serve(args):
     """``--serve``: the full serving sweep, one JSON line per rate, then the summary."""
     import bitz_b200 as bz
     bz.set_device(dist_env()[2])
+    resolve_lanes(args, bz)
     summary = serve_sweep(args, bz, args.serve_requests, 30, emit=True)
     print(json.dumps(dict(summary, metric="SHA-256 blocks proven/sec (serving)")))
 
@@ -499,6 +502,7 @@ def ours(args):
         subprocess.run(["make", "-s", "-C", os.path.join(ROOT, "bitz_b200")], check=True)
     dist = Dist(world)
     bz.set_device(local)
+    resolve_lanes(args, bz)
     inputs, outputs, _ = statement(args)
     blocks = blocks_proven(args, inputs.size)
     ps = bz.CircuitProofSystem(args.circuit, inputs, outputs, args.security)
@@ -583,6 +587,11 @@ def ours(args):
             line["cpu_baseline"] = cpu_baseline(args, inputs, outputs, blocks)
         print(json.dumps(line))
     dist.close()
+
+
+def resolve_lanes(args, bz):
+    if args.lanes is None:
+        args.lanes = int(bz.TUNING.get("lanes", 16))
 
 
 def main():

@@ -18,6 +18,24 @@ import numpy as np
 
 from . import _lib
 
+
+def _tuning():
+    """The batched prover's tuned lane count and host-thread cap
+    (bitz_b200/tuning.json, written by ``python -m bitz_b200.autotune``), or {}."""
+    import json
+    import os
+    try:
+        with open(os.path.join(os.path.dirname(os.path.abspath(__file__)), "tuning.json")) as f:
+            return json.load(f)
+    except (OSError, ValueError):
+        return {}
+
+
+TUNING = _tuning()
+if TUNING.get("lane_threads") and "BITZ_LANE_THREADS" not in __import__("os").environ:
+    # read by the library when its first batch starts
+    __import__("os").environ["BITZ_LANE_THREADS"] = str(int(TUNING["lane_threads"]))
+
 __all__ = ["BitzError", "ProverState", "build_prover", "post_gkr_prove", "gkr_prove",
            "gkr_outputs", "device_count", "CircuitProofSystem", "Witness", "CommittedWitness",
            "wire_decode", "batch_prove", "ProveServer", "probe_kernel", "probe_read", "probe_kernels", "gf_peak",
@@ -309,9 +327,12 @@ def gkr_outputs(row_images, columns):
     return out
 
 
-def batch_prove(systems, lanes: int = 8):
+def batch_prove(systems, lanes=None):
     """Proves every CircuitProofSystem in ``systems`` on ``lanes`` concurrent
-    prover lanes; returns (proofs, each proof's duration in ms)."""
+    prover lanes (the tuned count of bitz_b200/tuning.json when None, else
+    16); returns (proofs, each proof's duration in ms)."""
+    if lanes is None:
+        lanes = int(TUNING.get("lanes", 16))
     lib = _lib.load()
     n = len(systems)
     hs = (ctypes.c_void_p * max(n, 1))(*[s._h.value for s in systems])
