@@ -236,6 +236,9 @@ Context::Context() {
   pg_.channel = &channel_;
   pg_.ctl = gk_ctl_.get();
   gk_.channel = &channel_;
+  gk_.mid_blocks = gkr_mid_blocks(false);
+  sp_mid_blocks_ = ::bz::sp_mid_blocks(false);
+  pg_.mid_blocks = ::bz::pg_mid_blocks(false);
   lane_bootstrap(*this);
 }
 
@@ -255,13 +258,15 @@ std::atomic<unsigned long long> &launch_counter() {
 
 Context &Context::get() {
   // One default lane per process, created on first use on the current device.
-  // It proves one statement at a time with the GPU to itself, so it keeps the
-  // middle GKR rounds in one resident kernel; pool lanes, which share the GPU,
-  // launch them one by one.
+  // It proves one statement at a time with the GPU to itself, so its resident
+  // middle rounds (GKR, Spartan, post-GKR and Ligerito) use grids of 128
+  // blocks; pool lanes, which share the GPU, run those rounds as queued
+  // launches (or 32-block grids with BITZ_POOL_MID=1).
   static Context *ctx = [] {
     Context *c = new Context();
-    c->gk_.resident_middle = true;
-    c->pg_.resident_middle = true;
+    c->gk_.mid_blocks = gkr_mid_blocks(true);
+    c->sp_mid_blocks_ = ::bz::sp_mid_blocks(true);
+    c->pg_.mid_blocks = ::bz::pg_mid_blocks(true);
     return c;
   }();
   return *ctx;

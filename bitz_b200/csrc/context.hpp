@@ -13,6 +13,7 @@
 #include "device.cuh"
 #include "eq.cuh"
 #include "gkr.hpp"
+#include "spartan.hpp"
 #include "post_gkr.hpp"
 
 namespace bz {
@@ -110,8 +111,10 @@ class Context {
   RoundChannel *channel() { return &channel_; }
   // The lane's round controls (kMaxPointGkr entries), used by one phase at a time.
   RoundCtl *round_ctl() { return gk_ctl_.get(); }
-  // The lane proves alone: sumcheck middle rounds may run in resident kernels.
-  bool resident_middle() const { return gk_.resident_middle; }
+  // Grid of the resident Spartan grid rounds on this lane (0: none).
+  int sp_mid_blocks() const { return sp_mid_blocks_; }
+  // Grid of the resident post-GKR and Ligerito folds on this lane (0: none).
+  int pg_mid_blocks() const { return pg_.mid_blocks; }
   // Prover workspace slot, owned by the lane (created by the prover).
   std::shared_ptr<Workspace> workspace;
 
@@ -161,6 +164,7 @@ class Context {
   DeviceBuffer<RoundCtl> gk_ctl_;
   RoundChannel channel_;
   DeviceBuffer<unsigned int> counter_;
+  int sp_mid_blocks_ = 0;
 };
 
 // Loads kernels now (cudaFuncGetAttributes), so no kernel is loaded on its

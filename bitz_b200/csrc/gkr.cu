@@ -293,28 +293,35 @@ __global__ void __launch_bounds__(kMidThreads) gkr_round(
 }
 
 // The middle rounds of a layer (bind r_i for i = i_hi .. i_lo) in one
-// cooperative launch that stays resident, with the layer's live entries in
-// shared memory from the first round to the last. Block b of kMidBlocks owns
-// the positions whose residue mod kMidPeriod lies in [b kMidRuns,
-// (b + 1) kMidRuns); slot m of the block is position
-// kMidPeriod (m / kMidRuns) + b kMidRuns + m % kMidRuns. Every h of these
-// rounds is a multiple of kMidPeriod, so positions y, y + h, y + 2h, y + 3h
-// belong to one block and sit at slots m, m + E, m + 2E, m + 3E (E = h /
-// kMidBlocks elements per block): each round binds slot m < 2E from slots m
-// and m + 2E in place and sums elements j < E from slots j and j + E. Blocks
-// share nothing but the challenge and the sums: block 0 reads r_i from the
-// downbox (publication d0 + n - 1 - i) and relays it through ctl; each block
-// adds its share of the sums into acc and the last one through the round
-// posts them as publication p0 + n - i. The entries the tail kernel reads are
-// written back at the end. All blocks are resident together (cooperative
-// launch), so the relay waits end; each is bounded all the same.
-constexpr int kMidBlocks = 128;
+// cooperative launch of B blocks that stays resident, with the layer's live
+// entries in shared memory from the first round to the last. With the period
+// P = B kMidRuns, block b owns the positions whose residue mod P lies in
+// [b kMidRuns, (b + 1) kMidRuns); slot m of the block is position
+// P (m / kMidRuns) + b kMidRuns + m % kMidRuns. Every h of these rounds is a
+// multiple of P, so positions y, y + h, y + 2h, y + 3h belong to one block and
+// sit at slots m, m + E, m + 2E, m + 3E (E = h / B elements per block): each
+// round binds slot m < 2E from slots m and m + 2E in place and sums elements
+// j < E from slots j and j + E. Blocks share nothing but the challenge and the
+// sums: block 0 reads r_i from the downbox (publication d0 + n - 1 - i) and
+// relays it through ctl; each block adds its share of the sums into acc and
+// the last one through the round posts them as publication p0 + n - i. The
+// entries the tail kernel reads are written back at the end. All blocks are
+// resident together (cooperative launch), so the relay waits end; each is
+// bounded all the same. A lane proving alone uses kMidBlocks blocks; a pooled
+// lane, which shares the GPU with other lanes' kernels, kMidPoolBlocks (each
+// block then holds four times the entries, 192 KB of shared memory at the
+// largest round).
+constexpr int kMidBlocks = 128;      // a lane proving alone
+constexpr int kMidPoolBlocks = 32;   // a pooled lane, sharing the GPU with others
 constexpr int kMidRuns = 4;
-constexpr size_t kMidPeriod = (size_t)kMidBlocks * kMidRuns;
-static_assert(kMidPeriod <= 2 * (size_t)kTailH, "the tail starts below the middle rounds");
+static_assert((size_t)kMidBlocks * kMidRuns <= 2 * (size_t)kTailH,
+              "the tail starts below the middle rounds");
 
+// The period is gridDim.x kMidRuns positions: the grid is kMidBlocks blocks
+// or fewer.
 __device__ __forceinline__ size_t mid_pos(size_t m) {
-  return kMidPeriod * (m / kMidRuns) + (size_t)blockIdx.x * kMidRuns + m % kMidRuns;
+  const size_t period = (size_t)gridDim.x * kMidRuns;
+  return period * (m / kMidRuns) + (size_t)blockIdx.x * kMidRuns + m % kMidRuns;
 }
 
 // Dynamic shared memory for e0 elements: L and R at slots < 2 e0 (lo) and
@@ -329,7 +336,7 @@ __global__ void __launch_bounds__(kMidThreads) gkr_mid(
   extern __shared__ f128 dyn[];
   __shared__ MulTable T;
   const int t = threadIdx.x;
-  const size_t e0 = ((size_t)1 << (i_hi - 1)) / kMidBlocks;
+  const size_t e0 = ((size_t)1 << (i_hi - 1)) / gridDim.x;
   f128 *SL = dyn, *SL1 = dyn + 2 * e0, *SR = dyn + 4 * e0, *SR1 = dyn + 6 * e0;
   f128 *EQ = dyn + 8 * e0, *P = dyn + 10 * e0, *Q = dyn + 11 * e0;
   f128 *L = c, *R = c + n_half;
@@ -349,7 +356,7 @@ __global__ void __launch_bounds__(kMidThreads) gkr_mid(
     unsigned long long rw[2];
     if (!resident_challenge(down, d0 + (n - 1 - i), cl, rw)) return;
     mul_table_build(T, mk(rw[0], rw[1]));
-    const size_t e = ((size_t)1 << (i - 1)) / kMidBlocks;
+    const size_t e = ((size_t)1 << (i - 1)) / gridDim.x;
     const int at_one = (int)((at_one_mask >> (i - 1)) & 1);
     // the upper half of the live slots: separate arrays in the first round,
     // slots [2e, 4e) of the lower ones after it
@@ -411,7 +418,7 @@ __global__ void __launch_bounds__(kMidThreads) gkr_mid(
     }
   }
   // the live entries after round i_lo: L and R below 2 h, eq below h
-  const size_t e = ((size_t)1 << (i_lo - 1)) / kMidBlocks;
+  const size_t e = ((size_t)1 << (i_lo - 1)) / gridDim.x;
   for (size_t m = t; m < 2 * e; m += kMidThreads) {
     const size_t y = mid_pos(m);
     st(L + y, SL[m]);
@@ -604,6 +611,21 @@ static f128 eq_factor(f128 r, f128 z) { return gadd(gadd(mk(1, 0), r), z); }
 
 // One bind round of hh elements per half: by tiles up to kMidMaxH, one
 // element per thread above (issue bound there).
+// Grid of the resident middle rounds for a lane: kMidBlocks for a lane proving
+// alone; for a pooled lane none (every middle round a queued launch), or
+// kMidPoolBlocks with BITZ_POOL_MID=1. On the batched mix the pooled grids cut
+// a proof's launches from 189 to 130 but not its time: at 24 lanes and more
+// the cooperative grids of different lanes compete for SMs and the mix ran
+// 10-20 % slower, so they are off by default.
+int gkr_mid_blocks(bool alone) {
+  if (alone) return kMidBlocks;
+  static const bool pool = [] {
+    const char *e = getenv("BITZ_POOL_MID");
+    return e && e[0] == '1';
+  }();
+  return pool ? kMidPoolBlocks : 0;
+}
+
 // Elements below h whose packed column holds bits of h (the rest are padding).
 static double live_threads(size_t h, size_t colmask, size_t live) {
   return h > colmask ? (double)(h / (colmask + 1)) * (double)live : (double)std::min(h, live);
@@ -622,24 +644,36 @@ static void launch_bind(f128 *c, size_t n_half, size_t hh, f128 r, f128 *eq, int
 }
 
 // gkr_mid over bind rounds i_hi .. i_lo as a cooperative launch of
-// kMidBlocks blocks (every block must be resident together).
+// sc.mid_blocks blocks (every block must be resident together).
 static void launch_mid(f128 *c, size_t n_half, int n, int i_hi, int i_lo, const f128 *point,
                        GkrScratch &sc, unsigned long long p0, unsigned long long d0,
                        size_t colmask, size_t live, cudaStream_t st) {
-  const size_t e0 = ((size_t)1 << (i_hi - 1)) / kMidBlocks;
+  const int nb = sc.mid_blocks;
+  const size_t e0 = ((size_t)1 << (i_hi - 1)) / nb;
   const size_t smem = mid_smem_bytes(e0);
-  static const int capacity = [] {
+  // residency for the largest rounds of each grid size (the kernel's shared
+  // memory limit raised once to the largest, the pooled grid's)
+  static const int capacity[2] = {[] {
     int dev = 0, sms = 0, per_sm = 0;
     BZ_CUDA(cudaGetDevice(&dev));
     BZ_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
     BZ_CUDA(cudaFuncSetAttribute(gkr_mid, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)mid_smem_bytes(kMidMaxH / kMidBlocks)));
+                                 (int)mid_smem_bytes(kMidMaxH / kMidPoolBlocks)));
     BZ_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, gkr_mid, kMidThreads,
                                                           mid_smem_bytes(kMidMaxH / kMidBlocks)));
     return sms * per_sm;
-  }();
-  if (capacity < kMidBlocks) throw CudaError("gkr_mid: the blocks do not fit resident together");
-  if (((size_t)1 << (i_lo - 1)) < kMidPeriod || ((size_t)1 << (i_hi - 1)) > kMidMaxH)
+  }(), [] {
+    int dev = 0, sms = 0, per_sm = 0;
+    BZ_CUDA(cudaGetDevice(&dev));
+    BZ_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    BZ_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+        &per_sm, gkr_mid, kMidThreads, mid_smem_bytes(kMidMaxH / kMidPoolBlocks)));
+    return sms * per_sm;
+  }()};
+  if (nb != kMidBlocks && nb != kMidPoolBlocks) throw CudaError("gkr_mid: unsupported grid");
+  if (capacity[nb == kMidBlocks ? 0 : 1] < nb)
+    throw CudaError("gkr_mid: the blocks do not fit resident together");
+  if (((size_t)1 << (i_lo - 1)) < (size_t)nb * kMidRuns || ((size_t)1 << (i_hi - 1)) > kMidMaxH)
     throw CudaError("gkr_mid: round sizes outside the resident range");
   unsigned long long mask = 0;
   for (int i = i_lo; i <= i_hi; i++) mask |= (unsigned long long)gis_zero(point[i - 1]) << (i - 1);
@@ -651,8 +685,8 @@ static void launch_mid(f128 *c, size_t n_half, int n, int i_hi, int i_lo, const 
   RoundCtl *ctl = sc.ctl;
   void *args[] = {&c,  &n_half, &n,    &i_hi, &i_lo, &eq,      &mask,  &acc,
                   &mb, &p0,     &down, &d0,   &ctl,  &colmask, &live};
-  BZ_CUDA(cudaLaunchCooperativeKernel((const void *)gkr_mid, dim3(kMidBlocks),
-                                      dim3(kMidThreads), args, smem, st));
+  BZ_CUDA(cudaLaunchCooperativeKernel((const void *)gkr_mid, dim3(nb), dim3(kMidThreads), args,
+                                      smem, st));
   BZ_LAUNCH_CHECK();
 }
 
@@ -710,7 +744,7 @@ f128 gkr_prove(int s, const f128 *zeta, uint32_t grind_bits, Transcript &ts, Gkr
     // kMidMaxH; otherwise as a queued launch that reads r_i from ctl, left
     // there by the kernel before it.
     auto in_mid = [&](int i) {
-      return sc.resident_middle && ((size_t)1 << (i - 1)) <= kMidMaxH;
+      return sc.mid_blocks > 0 && ((size_t)1 << (i - 1)) <= kMidMaxH;
     };
     auto link_for = [&](int i) {  // where the kernel before bind round i leaves r_i
       return queued && i > i_tail && !in_mid(i) ? sc.ctl + (n - 1 - i) : nullptr;

@@ -22,11 +22,14 @@ struct GkrScratch {
   // every node of theirs is one in every layer; the kernels skip their
   // products and add their known contribution. 0: every column is live.
   size_t live_cols = 0;
-  // Run the middle rounds of each layer in one cooperative kernel that stays
-  // resident across them (a lane proving alone); otherwise one queued launch
-  // per round.
-  bool resident_middle = false;
+  // Blocks of the cooperative kernel that runs the middle rounds of each
+  // layer, resident across them (128 for a lane proving alone, fewer for a
+  // pooled lane that shares the GPU); 0: one queued launch per round.
+  int mid_blocks = 0;
 };
+
+// The grid of a lane's resident middle rounds (GkrScratch::mid_blocks).
+int gkr_mid_blocks(bool alone);
 
 // Builds every layer from the packed columns (2^s F128, bit b of column c is
 // row b) and the 128 row images. Layer 7 holds the column products.

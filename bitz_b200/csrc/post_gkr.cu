@@ -299,7 +299,8 @@ static void round_read(PostGkrScratch &sc, const unsigned long long *d_acc, int 
 // writes its chunk to (w_out, v_out) for pg_tail. All blocks are resident
 // together (cooperative launch), so the relay waits end; each is bounded all
 // the same.
-constexpr int kPgMidBlocks = 128;
+constexpr int kPgMidBlocks = 128;     // a lane proving alone
+constexpr int kPgMidPoolBlocks = 32;  // a pooled lane, sharing the GPU with others
 constexpr size_t kPgMidMaxChunk = 2048;  // entries per table per block
 
 __global__ void __launch_bounds__(kThreads) pg_mid(const f128 *__restrict__ w_in,
@@ -381,26 +382,34 @@ __global__ void __launch_bounds__(kThreads) pg_mid(const f128 *__restrict__ w_in
 // The first round pg_mid can start at: its input fits the blocks' chunks and
 // the last resident round still sums whole pairs in every block; t0 when
 // there is none.
-bool pg_mid_fits_folds(size_t n, int rounds) {
+bool pg_mid_fits_folds(size_t n, int rounds, int nb) {
   // a fold whose output is still summed needs two entries per block after it
-  return rounds >= 1 && n % kPgMidBlocks == 0 && n / kPgMidBlocks <= kPgMidMaxChunk &&
-         (rounds < 2 || (n >> (rounds - 1)) / kPgMidBlocks >= 2);
+  return nb > 0 && rounds >= 1 && n % nb == 0 && n / nb <= kPgMidMaxChunk &&
+         (rounds < 2 || (n >> (rounds - 1)) / nb >= 2);
 }
 
-int pg_mid_start(size_t n1, int t0) {
+int pg_mid_start(size_t n1, int t0, int nb) {
+  if (nb <= 0) return t0;
   for (int k = 0; k < t0; k++) {
     const size_t n_in = n1 >> k;
-    if (n_in % kPgMidBlocks == 0 && n_in / kPgMidBlocks <= kPgMidMaxChunk &&
-        (n1 >> t0) / kPgMidBlocks >= 2)
-      return k;
+    if (n_in % nb == 0 && n_in / nb <= kPgMidMaxChunk && (n1 >> t0) / nb >= 2) return k;
   }
   return t0;
+}
+
+int pg_mid_blocks(bool alone) {
+  if (alone) return kPgMidBlocks;
+  static const bool pool = [] {
+    const char *e = getenv("BITZ_POOL_MID");
+    return e && e[0] == '1';
+  }();
+  return pool ? kPgMidPoolBlocks : 0;
 }
 
 void launch_pg_mid(const f128 *w_in, const f128 *v_in, size_t n_in, int km, int t0,
                    int emit_last, int acc_off, f128 *w_out, f128 *v_out, unsigned long long *acc,
                    RoundChannel *ch, unsigned long long p0, unsigned long long d0, RoundCtl *ctl,
-                   cudaStream_t s) {
+                   int nb, cudaStream_t s) {
   static const int capacity = [] {
     int dev = 0, sms = 0, per_sm = 0;
     const size_t most = 2 * kPgMidMaxChunk * sizeof(f128);
@@ -410,14 +419,15 @@ void launch_pg_mid(const f128 *w_in, const f128 *v_in, size_t n_in, int km, int 
     BZ_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, pg_mid, kThreads, most));
     return sms * per_sm;
   }();
-  if (capacity < kPgMidBlocks) throw CudaError("pg_mid: the blocks do not fit resident together");
-  const size_t smem = 2 * (n_in / kPgMidBlocks) * sizeof(f128);
+  if (nb < 1 || nb > kPgMidBlocks || capacity < nb)
+    throw CudaError("pg_mid: the blocks do not fit resident together");
+  const size_t smem = 2 * (n_in / nb) * sizeof(f128);
   Mailbox *mb = ch->dev;
   const Mailbox *down = ch->down_dev;
   void *args[] = {&w_in, &v_in, &n_in, &km, &t0, &emit_last, &acc_off, &w_out,
                   &v_out, &acc, &mb,   &p0,   &down, &d0, &ctl};
-  BZ_CUDA(cudaLaunchCooperativeKernel((const void *)pg_mid, dim3(kPgMidBlocks), dim3(kThreads),
-                                      args, smem, s));
+  BZ_CUDA(cudaLaunchCooperativeKernel((const void *)pg_mid, dim3(nb), dim3(kThreads), args, smem,
+                                      s));
   BZ_LAUNCH_CHECK();
 }
 
@@ -474,7 +484,7 @@ int post_gkr_prove(const PostGkrArgs &a, Transcript &ts, PostGkrScratch &sc, cud
       const unsigned long long d0 = queued ? ch->down_next + 1 : 0;
       // rounds km .. t0-1 resident (pg_mid) when the lane proves alone; the
       // rounds before them are queued launches
-      const int km = queued && sc.resident_middle ? pg_mid_start(n1, t0) : t0;
+      const int km = queued ? pg_mid_start(n1, t0, sc.mid_blocks) : t0;
       if (queued) BZ_CUDA(cudaMemsetAsync(sc.ctl, 0, sizeof(RoundCtl) * (rounds + 1), s));
       RoundLink lk{nullptr, queued && km > 0 ? sc.ctl : nullptr, queued ? ch->down_dev : nullptr,
                    d0};
@@ -501,7 +511,7 @@ int post_gkr_prove(const PostGkrArgs &a, Transcript &ts, PostGkrScratch &sc, cud
           f128 *const *in = set[km % 2];
           f128 *const *to = set[(km + 1) % 2];
           launch_pg_mid(in[0], in[1], n1 >> km, km, t0, 1, 2, to[0], to[1], acc, ch, p0, d0, sc.ctl,
-                        s);
+                        sc.mid_blocks, s);
           cur_set = (km + 1) % 2;
         }
         f128 *const *cur = set[cur_set];

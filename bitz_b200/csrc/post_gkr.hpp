@@ -30,24 +30,32 @@ struct PostGkrScratch {
   f128 claim_seen{0, 0};              // the weighted sum found when a claim fails
   RoundChannel *channel = nullptr;    // mailbox for round results; null: copy + sync
   RoundCtl *ctl = nullptr;            // round controls for queued rounds; null: none
-  bool resident_middle = false;       // rounds above the tail in one resident kernel
+  // blocks of the cooperative kernel that runs the rounds above the tail
+  // resident (128 for a lane proving alone, fewer for a pooled lane); 0: queued
+  // launches
+  int mid_blocks = 0;
 };
 
 // Folds k = km .. t0-1 of a quadratic sumcheck over <W, V> (n_in entries
-// each) in one resident cooperative launch (a lane that proves alone): fold
+// each) in one resident cooperative launch of nb blocks: fold
 // k takes its challenge from downbox publication d0 + k (relayed through
 // ctl[k], which must start zeroed), XORs the next message into
 // acc + 8 (k + acc_off) and posts it as publication p0 + k + 1 (the last fold
 // only with emit_last); the folded tables end in (w_out, v_out).
 // pg_mid_start gives the first fold it can take (t0 when none).
-int pg_mid_start(size_t n1, int t0);
-// All `rounds` folds of n-entry tables fit launch_pg_mid (the last without a
-// message).
-bool pg_mid_fits_folds(size_t n, int rounds);
+// nb is the grid (0: none fits).
+int pg_mid_start(size_t n1, int t0, int nb);
+// All `rounds` folds of n-entry tables fit launch_pg_mid with nb blocks (the
+// last without a message).
+bool pg_mid_fits_folds(size_t n, int rounds, int nb);
 void launch_pg_mid(const f128 *w_in, const f128 *v_in, size_t n_in, int km, int t0,
                    int emit_last, int acc_off, f128 *w_out, f128 *v_out, unsigned long long *acc,
                    RoundChannel *ch, unsigned long long p0, unsigned long long d0, RoundCtl *ctl,
-                   cudaStream_t s);
+                   int nb, cudaStream_t s);
+// The grid of a lane's resident post-GKR and Ligerito folds
+// (PostGkrScratch::mid_blocks): 128 for a lane proving alone; for a pooled
+// lane none, or 32 with BITZ_POOL_MID=1 (as for the GKR middle rounds).
+int pg_mid_blocks(bool alone);
 
 // The quadratic sumcheck round of <W, V> (shared with the Ligerito folds):
 // quad_sums accumulates (a0, a2) over the pairs as they are; quad_fold folds

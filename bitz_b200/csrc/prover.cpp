@@ -488,7 +488,8 @@ std::vector<uint8_t> ProofSystem::ligerito(cudaStream_t s, f128 target) {
     BZ_CUDA(cudaMemsetAsync(acc, 0, 8 * sizeof(unsigned long long) * (L.k + 1), s));
     // kernels that wait for the host follow the sumchecks' mode
     const bool resident = resident_rounds_enabled();
-    if (resident && lane_->resident_middle() && pg_mid_fits_folds(n, L.k)) {
+    const int pg_nb = lane_->pg_mid_blocks();
+    if (resident && pg_mid_fits_folds(n, L.k, pg_nb)) {
       // the level's folds in one resident kernel: fold r takes its challenge
       // from the downbox and posts the next message itself
       RoundCtl *ctl = lane_->round_ctl();
@@ -497,7 +498,7 @@ std::vector<uint8_t> ProofSystem::ligerito(cudaStream_t s, f128 target) {
       ResidentScope gate(true);
       const unsigned long long d0 = ch->down_next + 1;
       quad_sums(b, f, n, acc, ch->arm(), s);
-      launch_pg_mid(b, f, n, 0, L.k, 0, 1, b2, f2, acc, ch, ch->next, d0, ctl, s);
+      launch_pg_mid(b, f, n, 0, L.k, 0, 1, b2, f2, acc, ch, ch->next, d0, ctl, pg_nb, s);
       try {
         for (int r = 0; r < L.k; r++) {
           ch->wait(s, W.host_acc, 4);
@@ -707,7 +708,7 @@ int ProofSystem::prove_after_commit(cudaStream_t s, std::vector<uint8_t> &proof)
   sc.host = W.host_fp;
   sc.channel = ctx.channel();
   sc.ctl = ctx.round_ctl();
-  sc.resident_middle = ctx.resident_middle();
+  sc.mid_blocks = ctx.sp_mid_blocks();
   SpartanArgs sa;
   sa.ctx = fc;
   sa.q = q;

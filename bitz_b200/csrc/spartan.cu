@@ -529,7 +529,8 @@ static fp round_message(Transcript &ts, const FpCtx &c, fp &claim, const fp *wl,
 // them and posts publication p0 + k). At the end each block writes its chunk
 // to `out` for the tail kernel. All blocks are resident together
 // (cooperative launch), so the relay waits end; each is bounded all the same.
-constexpr int kSpMidBlocks = 128;
+constexpr int kSpMidBlocks = 128;     // a lane proving alone
+constexpr int kSpMidPoolBlocks = 32;  // a pooled lane, sharing the GPU with others
 constexpr size_t kSpMidMaxChunk = 2048;  // entries per table per block
 struct SpTabs {
   fp *t[4];
@@ -602,13 +603,14 @@ __global__ void __launch_bounds__(kThreads) sp_mid(SpTabs in, SpTabs out, size_t
     for (int t = 0; t < T; t++) out.t[t][ob + i] = tab[t][i];
 }
 
-// sp_mid over rounds k0 .. k1-1 as a cooperative launch of kSpMidBlocks
+// sp_mid over rounds k0 .. k1-1 as a cooperative launch of sc.mid_blocks
 // blocks; n_in entries per input table.
 template <int T, int N>
 static void launch_sp_mid(const SpTabs &in, const SpTabs &out, size_t n_in, int k0, int k1,
                           const FpCtx &c, const SpartanScratch &sc, unsigned long long p0,
                           unsigned long long d0, cudaStream_t s) {
-  const size_t smem = T * (n_in / kSpMidBlocks) * sizeof(fp);
+  const int nb = sc.mid_blocks;
+  const size_t smem = T * (n_in / nb) * sizeof(fp);
   static const int capacity = [] {
     int dev = 0, sms = 0, per_sm = 0;
     const size_t most = T * kSpMidMaxChunk * sizeof(fp);
@@ -619,7 +621,8 @@ static void launch_sp_mid(const SpTabs &in, const SpTabs &out, size_t n_in, int 
     BZ_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, sp_mid<T, N>, kThreads, most));
     return sms * per_sm;
   }();
-  if (capacity < kSpMidBlocks) throw CudaError("sp_mid: the blocks do not fit resident together");
+  if (nb < 1 || nb > kSpMidBlocks || capacity < nb)
+    throw CudaError("sp_mid: the blocks do not fit resident together");
   RoundChannel *ch = sc.channel;
   SpTabs a = in, b = out;
   FpCtx cc = c;
@@ -628,21 +631,34 @@ static void launch_sp_mid(const SpTabs &in, const SpTabs &out, size_t n_in, int 
   const Mailbox *down = ch->down_dev;
   RoundCtl *ctl = sc.ctl;
   void *args[] = {&a, &b, &n_in, &k0, &k1, &cc, &partial, &mb, &p0, &down, &d0, &ctl};
-  BZ_CUDA(cudaLaunchCooperativeKernel((const void *)sp_mid<T, N>, dim3(kSpMidBlocks),
-                                      dim3(kThreads), args, smem, s));
+  BZ_CUDA(cudaLaunchCooperativeKernel((const void *)sp_mid<T, N>, dim3(nb), dim3(kThreads), args,
+                                      smem, s));
   BZ_LAUNCH_CHECK();
 }
 
 // The first round (>= kmin) from which sp_mid can run the rounds up to t0:
 // its input fits the blocks' chunks, and the last resident round still sums
 // whole pairs in every block. t0 when there is none.
-static int sp_mid_start(size_t n0, int kmin, int t0) {
+static int sp_mid_start(size_t n0, int kmin, int t0, int nb) {
+  if (nb <= 0) return t0;
   for (int k = kmin; k < t0; k++) {
     const size_t n_in = k == 0 ? n0 : n0 >> (k - 1);
-    const size_t last = (n0 >> (t0 - 1)) / kSpMidBlocks;  // per block after the last fold
-    if (n_in % kSpMidBlocks == 0 && n_in / kSpMidBlocks <= kSpMidMaxChunk && last >= 2) return k;
+    const size_t last = (n0 >> (t0 - 1)) / nb;  // per block after the last fold
+    if (n_in % nb == 0 && n_in / nb <= kSpMidMaxChunk && last >= 2) return k;
   }
   return t0;
+}
+
+// Grid of the resident grid rounds for a lane: kSpMidBlocks for a lane proving
+// alone; for a pooled lane none, or kSpMidPoolBlocks with BITZ_POOL_MID=1 (as
+// for the GKR middle rounds, gkr.cu).
+int sp_mid_blocks(bool alone) {
+  if (alone) return kSpMidBlocks;
+  static const bool pool = [] {
+    const char *e = getenv("BITZ_POOL_MID");
+    return e && e[0] == '1';
+  }();
+  return pool ? kSpMidPoolBlocks : 0;
 }
 
 void spartan_prove(const SpartanArgs &a, Transcript &ts, SpartanScratch &sc, cudaStream_t s,
@@ -700,10 +716,10 @@ void spartan_prove(const SpartanArgs &a, Transcript &ts, SpartanScratch &sc, cud
     const unsigned long long p0 = ch->next + 1, d0 = ch->down_next + 1;
     tail = true;  // from here a kernel of the lane may wait for this thread
     fp *set[2][4] = {{E, A, B, C}, {E2, A2, B2, C2}};
-    // rounds km .. t0-1 resident (sp_mid) when the lane proves alone and a
-    // round's input fits the blocks' shared memory; the rounds before them
+    // rounds km .. t0-1 resident (sp_mid, a grid of sc.mid_blocks blocks) when
+    // a round's input fits the blocks' shared memory; the rounds before them
     // are queued launches
-    const int km = sc.resident_middle ? sp_mid_start(R, 0, t0) : t0;
+    const int km = sp_mid_start(R, 0, t0, sc.mid_blocks);
     BZ_CUDA(cudaMemsetAsync(sc.ctl, 0, sizeof(RoundCtl) * (nr + 1), s));
     for (int k = 0; k < km; k++) {
       const int fold = k > 0;
@@ -864,7 +880,7 @@ void spartan_prove(const SpartanArgs &a, Transcript &ts, SpartanScratch &sc, cud
     fp *set[2][2] = {{D, W}, {D2, W2}};
     // W is read from the packed bits of h through round 1: resident rounds
     // start at 2 at the earliest
-    const int km = sc.resident_middle ? sp_mid_start(Cn, 2, t0) : t0;
+    const int km = sp_mid_start(Cn, 2, t0, sc.mid_blocks);
     BZ_CUDA(cudaMemsetAsync(sc.ctl, 0, sizeof(RoundCtl) * (nc + 1), s));
     for (int k = 0; k < km; k++) {
       const int fold = k > 0;

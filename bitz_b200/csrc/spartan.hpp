@@ -43,7 +43,9 @@ struct SpartanScratch {
   fp *host;        // pinned, 4 entries
   RoundChannel *channel = nullptr;  // mailbox for round results; null: copy + sync
   RoundCtl *ctl = nullptr;          // the lane's round controls (queued rounds)
-  bool resident_middle = false;     // the grid rounds in one resident kernel (a lone lane)
+  // blocks of the cooperative kernel that runs the grid rounds resident (128
+  // for a lane proving alone, fewer for a pooled lane); 0: queued launches
+  int mid_blocks = 0;
 };
 
 struct SpartanOut {
@@ -53,6 +55,8 @@ struct SpartanOut {
   bool ok = false;
 };
 
+// The grid of a lane's resident Spartan rounds (SpartanScratch::mid_blocks).
+int sp_mid_blocks(bool alone);
 FpCtx make_fp_ctx(u128 q);
 u128 fp_canonical(fp mont, const FpCtx &c);
 // out[k] = canonical value of in[k] (as two LE words), on the device.

@@ -57,10 +57,9 @@ def test_batch_matches_alone(alone, lanes):
     assert all(x > 0 for x in lat)
 
 
-def test_lanes_sharing_host_threads_as_fibers(alone):
-    """Eight lanes on two host threads (four fibers each, switching wherever a
-    lane waits for the device): the same proofs. The thread cap is read once
-    per process, so this runs in a child process."""
+def _batch_in_child(env_updates):
+    """The MIX proved twice on eight lanes in a child process with the given
+    environment (the library reads these settings once per process)."""
     import os
     import subprocess
     import sys
@@ -75,11 +74,24 @@ def test_lanes_sharing_host_threads_as_fibers(alone):
             "assert again == proofs\n"
             "sys.stdout.write(''.join(p.hex() + '\\n' for p in proofs))\n") % (
                 here, os.path.dirname(here))
-    env = dict(os.environ, BITZ_LANE_THREADS="2")
+    env = dict(os.environ, **env_updates)
     r = subprocess.run([sys.executable, "-c", code], env=env, capture_output=True, text=True,
                        timeout=600, cwd=here)
     assert r.returncode == 0, r.stderr[-3000:]
-    assert [bytes.fromhex(x) for x in r.stdout.split()] == alone
+    return [bytes.fromhex(x) for x in r.stdout.split()]
+
+
+def test_lanes_sharing_host_threads_as_fibers(alone):
+    """Eight lanes on two host threads (four fibers each, switching wherever a
+    lane waits for the device): the same proofs."""
+    assert _batch_in_child({"BITZ_LANE_THREADS": "2"}) == alone
+
+
+def test_pooled_lanes_with_resident_middle_rounds(alone):
+    """Pooled lanes with their GKR, Spartan and post-GKR middle rounds in
+    32-block resident grids (BITZ_POOL_MID=1) instead of queued launches: the
+    same proofs."""
+    assert _batch_in_child({"BITZ_POOL_MID": "1"}) == alone
 
 
 def test_batch_twice_on_the_same_systems(alone):
