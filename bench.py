@@ -171,11 +171,10 @@ def peaks():
         return {"hbm_gbs": FALLBACK_HBM_GBS}, "fallback"
 
 
-def profile_figure(summary, key):
+def profile_figure(summary, key, tag="sha256-chain-n64"):
     """A figure (e.g. DRAM bytes per launch) from a committed ncu summary of
-    this workload, or None: the lines ``key: value`` of
-    profiles/<summary>_sha256-chain-n64.md."""
-    path = os.path.join(PROFILES, f"{summary}_sha256-chain-n64.md")
+    a workload, or None: the lines ``key: value`` of profiles/<summary>_<tag>.md."""
+    path = os.path.join(PROFILES, f"{summary}_{tag}.md")
     try:
         for line in open(path):
             if line.startswith(key + ":"):
@@ -185,7 +184,7 @@ def profile_figure(summary, key):
     return None
 
 
-def roofline(bz, ps, steps, hbm_gbs, pk_kind):
+def roofline(bz, ps, steps, hbm_gbs, pk_kind, tag="sha256-chain-n64"):
     """Times every launch of the instrumented kernels with CUDA events over
     ``steps`` proofs (every round its own launch, as under a kernel profiler),
     picks the kernel with the largest share of the proofs' device time, and
@@ -232,19 +231,19 @@ def roofline(bz, ps, steps, hbm_gbs, pk_kind):
         peak_source = ("measured GF(2^128) product throughput of this GPU (bitz_diag_gf_peak: "
                        + ", ".join(f"{k} {v / 1e9:.1f} G/s" for k, v in peaks.items())
                        + "), weighted by the kernel's product mix")
-    traffic = profile_figure(top["kernel"], "traffic_bytes_per_launch")
+    traffic = profile_figure(top["kernel"], "traffic_bytes_per_launch", tag)
     return {"kernel": top["kernel"], "bound": top["bound"], "achieved": achieved, "peak": peak,
             "unit": unit, "frac": achieved / peak, "peak_source": peak_source,
             "traffic": traffic,
             "traffic_source": (f"ncu dram__bytes_read.sum + dram__bytes_write.sum, mean over the "
                                f"captured launches of the committed summary "
-                               f"profiles/{top['kernel']}_sha256-chain-n64.md") if traffic else None,
+                               f"profiles/{top['kernel']}_{tag}.md") if traffic else None,
             "algorithmic_bytes_per_launch": top["bytes_per_launch"],
             "products_per_launch": top["products_per_launch"],
             "launches_per_proof": top["launches"], "avg_launch_us": top["avg_launch_us"],
             "share_of_device_span": top["share_of_device_span"],
             "share_of_kernel_time_ncu": profile_figure(
-                "launches", f"{top['kernel']}_share_of_kernel_time"),
+                "launches", f"{top['kernel']}_share_of_kernel_time", tag),
             "share_note": "share_of_device_span: this run's CUDA-event kernel time over the proofs' "
                           "device span (host waits included); share_of_kernel_time_ncu: the "
                           "committed ncu launch list's share of summed kernel time",
@@ -363,7 +362,8 @@ def batched(args, bz):
 def large(args, bz, steps=5, warmup=2):
     """sha256-chain n=1024 (64 KiB, SplitMix64 seed 2) at PCS security 128 (unique
     decoding, no OOD): one proof per step, device time by CUDA events on the
-    prover's stream, L2 flushed before each."""
+    prover's stream, L2 flushed before each; then the roofline of its dominant
+    kernel, as for the main workload."""
     from bitz_b200 import statements
     inp, out, _ = statements.instance("sha256-chain", 1024, 2)
     ps = bz.CircuitProofSystem("sha256-chain", inp, out, 128)
@@ -379,7 +379,10 @@ def large(args, bz, steps=5, warmup=2):
         t0 = time.perf_counter()
         ps.prove(restage=True)
         e2e.append(1e3 * (time.perf_counter() - t0))
+    pk, pk_kind = peaks()
+    roof = roofline(bz, ps, 2, pk["hbm_gbs"], pk_kind, tag="sha256-chain-n1024")
     return {"workload": "sha256-chain n=1024 pcs-security-bits 128 (seed 2)", "blocks": 1024,
+            "roofline": roof,
             "steps": steps, "value": 1024 * steps / (sum(spans) / 1e3), "unit": "blocks/s",
             "latency_ms": {"p50": statistics.median(spans), "p99": pct(spans, 0.99)},
             "e2e": {"value": 1024 * steps / (sum(e2e) / 1e3), "unit": "blocks/s",
