@@ -251,6 +251,12 @@ def roofline(bz, ps, steps, hbm_gbs, pk_kind, tag="sha256-chain-n64"):
             "kernels": rows[:8]}
 
 
+def replica_value(world, blocks, steps, slowest_ms):
+    """Whole-job blocks/s of `world` replicas, each proving `steps` proofs of
+    `blocks` blocks: every rank's blocks over the slowest rank's time."""
+    return world * blocks * steps / (slowest_ms / 1000.0)
+
+
 def pct(xs, q):
     xs = sorted(xs)
     return xs[min(len(xs) - 1, int(q * len(xs)))]
@@ -538,7 +544,7 @@ def ours(args):
         e2e_s += time.perf_counter() - t1
     e2e_s = dist.max(e2e_s)
     dist.barrier()
-    value = world * blocks * args.steps / (dev_total_ms / 1000.0)
+    value = replica_value(world, blocks, args.steps, dev_total_ms)
     e2e = world * blocks * args.steps / e2e_s
     stats = ps.stats()
     h2d = 4 * (8 + 16) * stats["compressions"] + 8 * stats["compressions"] + (inputs.size + 7) // 8 \
