@@ -82,7 +82,7 @@ void RoundChannel::clear_down() {
   for (int k = 0; k < 2 * kMailboxWords; k++) s[k] = 0;
 }
 
-// The probe's verdict, set when the process's first lane is made: -1 not
+// The probe's result, set when the process's first lane is made: -1 not
 // yet probed, 0 the host cannot reach a running kernel, 1 it can.
 static std::atomic<int> g_host_reaches_kernel{-1};
 
