@@ -89,6 +89,17 @@ def round_wait_stats():
     return out[0] * 1e-9, int(out[1])
 
 
+def gate_stats():
+    """The device gate since the process started: lanes whose kernels may wait
+    for their host thread hold it as resident stretches; device and pinned
+    allocations wait until none is held. Returns a dict of the allocation and
+    resident stretch counts and the seconds each kind waited."""
+    out = (ctypes.c_ulonglong * 4)()
+    _check(_lib.load().bitz_gate_stats(out))
+    return {"allocs": int(out[0]), "alloc_wait_s": out[1] * 1e-9,
+            "residents": int(out[2]), "resident_wait_s": out[3] * 1e-9}
+
+
 class ProverState:
     """The prover transcript (crates/transcript/src/prover.rs:10)."""
 

@@ -61,6 +61,7 @@ SIGNATURES = [
     ("bitz_launch_count", ctypes.c_ulonglong, []),
     ("bitz_resident_rounds", ctypes.c_int, []),
     ("bitz_round_wait_stats", ctypes.c_int, [ctypes.POINTER(ctypes.c_ulonglong)]),
+    ("bitz_gate_stats", ctypes.c_int, [ctypes.POINTER(ctypes.c_ulonglong)]),
     ("bitz_system_witness", ctypes.c_int,
      [_vp, _vp, ctypes.c_size_t, _vp, ctypes.c_size_t, _vp, ctypes.c_size_t]),
     ("bitz_circuit_layout", ctypes.c_int,

@@ -17,6 +17,7 @@
 #include <map>
 #include <memory>
 #include <mutex>
+#include <numeric>
 #include <thread>
 #include <unordered_map>
 #include <vector>
@@ -277,11 +278,28 @@ int bitz_batch_prove(bitz_system *const *systems, size_t n, int lanes, uint8_t *
   } catch (const std::exception &e) {
     return capi_fail(BZ_ERR_CUDA, e.what());
   }
+  // Largest statements first. A lane's first proof is then the largest it
+  // proves in the batch, so its scratch grows at most once per batch (a
+  // growth allocation waits until no lane has a kernel waiting for its host
+  // thread and holds every lane back meanwhile), and the batch ends on its
+  // shortest proofs. The proofs come back in the callers' order.
+  std::vector<size_t> order(n);
+  std::iota(order.begin(), order.end(), (size_t)0);
+  {
+    std::vector<std::pair<uint64_t, size_t>> key(n);
+    for (size_t i = 0; i < n; i++) {
+      const ProofSystem &ps = *systems[i]->ps;
+      key[i] = {ProofSystem::footprint_bytes(ps.kind(), ps.n_inputs()), ps.n_inputs()};
+    }
+    std::stable_sort(order.begin(), order.end(),
+                     [&](size_t a, size_t b) { return key[a] > key[b]; });
+  }
   std::atomic<size_t> next{0};
   std::vector<int> status(n, BZ_OK);
   std::vector<std::string> errors(n);
   auto worker = [&](Context *lane) {
-    for (size_t i; (i = next.fetch_add(1)) < n;) {
+    for (size_t k; (k = next.fetch_add(1)) < n;) {
+      const size_t i = order[k];
       std::vector<uint8_t> proof;
       auto ts = std::chrono::steady_clock::now();
       status[i] = prove_on(*systems[i]->ps, *lane, proof, errors[i]);

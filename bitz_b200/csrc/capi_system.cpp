@@ -137,6 +137,12 @@ int bitz_round_wait_stats(unsigned long long out[2]) {
   }
 }
 
+int bitz_gate_stats(unsigned long long out[4]) {
+  if (!out) return capi_fail(BZ_ERR_ARGUMENT, "null argument");
+  DeviceGate::get().stats(out);
+  return BZ_OK;
+}
+
 int bitz_system_witness(bitz_system *sys, uint32_t *f_words, size_t f_cap, uint32_t *h_words,
                         size_t h_cap, int64_t *products, size_t prod_cap) {
   if (!sys) return capi_fail(BZ_ERR_ARGUMENT, "null argument");

@@ -145,16 +145,27 @@ DeviceGate &DeviceGate::get() {
 
 // A fiber must not block its thread in the gate: the thread's other fibers
 // may hold the scopes it waits for. It polls and yields instead.
+static unsigned long long ns_since(std::chrono::steady_clock::time_point t0) {
+  return (unsigned long long)std::chrono::duration_cast<std::chrono::nanoseconds>(
+             std::chrono::steady_clock::now() - t0)
+      .count();
+}
+
 void DeviceGate::enter_resident() {
   std::unique_lock<std::mutex> lk(mu_);
-  if (in_fiber()) {
-    while (alloc_ || allocs_waiting_ != 0) {
-      lk.unlock();
-      fiber_yield();
-      lk.lock();
+  resident_n_++;
+  if (alloc_ || allocs_waiting_ != 0) {
+    const auto t0 = std::chrono::steady_clock::now();
+    if (in_fiber()) {
+      while (alloc_ || allocs_waiting_ != 0) {
+        lk.unlock();
+        fiber_yield();
+        lk.lock();
+      }
+    } else {
+      cv_.wait(lk, [&] { return !alloc_ && allocs_waiting_ == 0; });
     }
-  } else {
-    cv_.wait(lk, [&] { return !alloc_ && allocs_waiting_ == 0; });
+    resident_wait_ns_ += ns_since(t0);
   }
   residents_++;
 }
@@ -166,15 +177,20 @@ void DeviceGate::leave_resident() {
 
 void DeviceGate::enter_alloc() {
   std::unique_lock<std::mutex> lk(mu_);
+  alloc_n_++;
   allocs_waiting_++;
-  if (in_fiber()) {
-    while (alloc_ || residents_ != 0) {
-      lk.unlock();
-      fiber_yield();
-      lk.lock();
+  if (alloc_ || residents_ != 0) {
+    const auto t0 = std::chrono::steady_clock::now();
+    if (in_fiber()) {
+      while (alloc_ || residents_ != 0) {
+        lk.unlock();
+        fiber_yield();
+        lk.lock();
+      }
+    } else {
+      cv_.wait(lk, [&] { return !alloc_ && residents_ == 0; });
     }
-  } else {
-    cv_.wait(lk, [&] { return !alloc_ && residents_ == 0; });
+    alloc_wait_ns_ += ns_since(t0);
   }
   allocs_waiting_--;
   alloc_ = true;
@@ -184,6 +200,13 @@ void DeviceGate::leave_alloc() {
   std::lock_guard<std::mutex> lk(mu_);
   alloc_ = false;
   cv_.notify_all();
+}
+
+void DeviceGate::stats(unsigned long long out[4]) const {
+  out[0] = alloc_n_.load();
+  out[1] = alloc_wait_ns_.load();
+  out[2] = resident_n_.load();
+  out[3] = resident_wait_ns_.load();
 }
 
 ResidentScope::ResidentScope(bool on) : on_(on) {

@@ -287,12 +287,17 @@ class DeviceGate {
   void leave_resident();
   void enter_alloc();
   void leave_alloc();
+  // Since the process started: allocation stretches and the nanoseconds they
+  // waited for the gate, resident stretches and the nanoseconds they waited.
+  void stats(unsigned long long out[4]) const;
 
  private:
   std::mutex mu_;
   std::condition_variable cv_;
   int residents_ = 0, allocs_waiting_ = 0;
   bool alloc_ = false;
+  std::atomic<unsigned long long> alloc_n_{0}, alloc_wait_ns_{0}, resident_n_{0},
+      resident_wait_ns_{0};
 };
 
 class ResidentScope {

@@ -98,6 +98,8 @@ class ProofSystem {
 
   const CircuitSetup &setup() const { return *dev_->host; }
   int security() const { return security_; }
+  int kind() const { return kind_; }
+  size_t n_inputs() const { return inputs_.size(); }
   std::string error;
 
   // CircuitProofSystem::verify (end_to_end.rs:339-377) on proof bytes (root

@@ -194,6 +194,13 @@ int bitz_resident_rounds(void);
  * such waits. The rest of a proof's host time is the host's own transcript
  * work. */
 int bitz_round_wait_stats(unsigned long long out[2]);
+/* Diagnostic (no reference counterpart): the process's device gate since it
+ * started. A lane whose kernels may wait for its host thread holds the gate
+ * as a resident stretch; a device or pinned allocation (a lane's scratch
+ * growing, a new circuit shape) waits until no stretch is held and holds new
+ * ones back meanwhile. out[0] allocation stretches, out[1] nanoseconds they
+ * waited, out[2] resident stretches, out[3] nanoseconds they waited. */
+int bitz_gate_stats(unsigned long long out[4]);
 /* Diagnostic (no reference counterpart): the last proof's packed witness f,
  * packed h = M (1 || f) and the exact products (A h, B h, C h per row). */
 int bitz_system_witness(bitz_system *sys, uint32_t *f_words, size_t f_cap, uint32_t *h_words,
@@ -231,7 +238,9 @@ int bitz_statement_digest(int circuit_kind, const uint8_t *input_bits, size_t n_
  * cap); past it, lanes share threads as cooperative fibers that switch
  * wherever a lane waits for the device. proofs[i] (freed with
  * bitz_free) and proof_lens[i] receive each proof; latency_ms[i] (may be
- * NULL) that proof's own duration, from its start on a lane to its bytes. Returns
+ * NULL) that proof's own duration, from its start on a lane to its bytes. The
+ * lanes take the statements largest first (a lane's scratch then grows at
+ * most once per call); results come back in the callers' order. Returns
  * the first failure's status after every proof has finished; failed entries
  * get a NULL proof. The systems must be distinct. */
 int bitz_batch_prove(bitz_system *const *systems, size_t n, int lanes, uint8_t **proofs,
