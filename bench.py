@@ -347,10 +347,11 @@ def batched(args, bz):
     res["plain"] = (blocks / (time.perf_counter() - t0), lat, plain)
     for name, lanes in (("pool_lane", 1), ("batched", args.lanes)):
         bz.l2_flush()
+        g0 = bz.gate_stats()
         t0 = time.perf_counter()
         proofs, lat = bz.batch_prove(systems, lanes)
         wall = time.perf_counter() - t0
-        res[name] = (blocks / wall, lat, proofs)
+        res[name] = (blocks / wall, lat, proofs, gate_delta(g0, bz.gate_stats()))
     same = res["plain"][2] == res["batched"][2] == res["pool_lane"][2]
     return {"workload": "256 x sha256-block-aligned, k ~ U{0..32} blocks (SplitMix64 seed 3), "
                         f"pcs-security-bits {args.security}",
@@ -362,7 +363,17 @@ def batched(args, bz):
             "latency_ms": {"p50": pct(res["batched"][1], 0.5), "p99": pct(res["batched"][1], 0.99)},
             "sequential_plain_latency_ms": {"p50": pct(res["plain"][1], 0.5),
                                             "p99": pct(res["plain"][1], 0.99)},
-            "proofs_identical_to_alone": same}
+            "proofs_identical_to_alone": same,
+            "gate": res["batched"][3]}
+
+
+def gate_delta(g0, g1):
+    """Device-gate activity between two gate_stats() readings: allocations
+    (scratch growth) and the seconds allocations and resident stretches
+    waited for each other."""
+    return {"allocs": g1["allocs"] - g0["allocs"],
+            "alloc_wait_s": round(g1["alloc_wait_s"] - g0["alloc_wait_s"], 6),
+            "resident_wait_s": round(g1["resident_wait_s"] - g0["resident_wait_s"], 6)}
 
 
 def large(args, bz, steps=5, warmup=2):
@@ -446,6 +457,7 @@ def serve_sweep(args, bz, requests, max_rates, emit=False):
         rate = 1000.0 / statistics.mean(alone_served)  # one request at a time
         for _ in range(max_rates):
             gaps = [rng.expovariate(rate) for _ in mix]
+            g0 = bz.gate_stats()
             tickets, t0 = [], time.perf_counter()
             due = t0
             for (kind, inp, out), g in zip(mix, gaps):
@@ -467,6 +479,7 @@ def serve_sweep(args, bz, requests, max_rates, emit=False):
             point = {"rate_rps": rate, "value": sum(blocks) / wall, "unit": "blocks/s",
                      "latency_ms": {"p50": pct(lat, 0.5), "p99": p99},
                      "peak_in_flight": srv.stats()["peak_in_flight"],
+                     "gate": gate_delta(g0, bz.gate_stats()),
                      "proofs_identical_to_alone": same}
             sweep.append(point)
             if emit:
@@ -483,7 +496,7 @@ def serve_sweep(args, bz, requests, max_rates, emit=False):
                         "k = floor(2^U(0,9)) in 1..512 (seed 4)",
             "requests": len(mix), "blocks": sum(blocks), "lanes": args.lanes,
             "rate_rps": best["rate_rps"], "value": best["value"], "unit": "blocks/s",
-            "latency_ms": best["latency_ms"],
+            "latency_ms": best["latency_ms"], "gate": best["gate"],
             "single_request_latency_ms": {"p50": pct(alone_served, 0.5), "p99": single},
             "plain_sequential_value": plain_bps,
             "speedup_vs_plain_sequential": best["value"] / plain_bps,

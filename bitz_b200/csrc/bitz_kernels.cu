@@ -14,6 +14,11 @@
 #include "device.cuh"
 #include "hash.cuh"
 #include "context.hpp"
+#include "tma.cuh"
+
+#include <cudaTypedefs.h>
+
+#include <algorithm>
 
 namespace bz {
 
@@ -355,55 +360,140 @@ void dot(const f128 *a, const f128 *b, size_t n, unsigned long long *acc, Publis
 }
 
 // ----------------------------------------------------- Reed-Solomon encode
+//
+// The codeword is 2^d rows of 2^k columns (row-major, 16-byte entries); the
+// message is its first 2^l rows, repeated across the 2^(d-l) row blocks
+// before the additive FFT's levels t = l-1 .. 0 run. Level t takes rows q
+// and q + 2^t of each 2^(t+1)-row block based at q0 to
+// (u + lam w, u + (lam + 1) w), lam = Wh_t(x_q0), the sum of the basis
+// table's wh[t][sb] = Wh_t(X^sb) over the set bits sb > t of the row index.
 
-// Copies the message into every 2^l-row repetition of the codeword: levels
-// t >= l of the additive FFT only copy, the upper coefficients being zero.
-__global__ void k_rs_spread(const f128 *__restrict__ msg, int k, int l, int d,
-                            f128 *__restrict__ cw) {
-  size_t total = (size_t)1 << (d + k);
-  size_t mmask = ((size_t)1 << (l + k)) - 1;
-  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < total;
-       i += (size_t)gridDim.x * blockDim.x)
-    st(cw + i, ld(msg + (i & mmask)));
+// lam of level t for a row whose bits above t are those of `row`; wt is
+// level t's row of the basis table (wt[sb] = Wh_t(X^sb)).
+__device__ __forceinline__ f128 rs_lambda(const f128 *wt, int t, int d, size_t row) {
+  f128 lam = mk(0, 0);
+  for (int sb = t + 1; sb < d; sb++)
+    if ((row >> sb) & 1) lam = gadd(lam, wt[sb]);
+  return lam;
 }
 
-// One additive-FFT level t over every column: rows q and q + 2^t of a block
-// based at q0 become (u + lam w, u + (lam + 1) w), lam = Wh_t(x_q0) summed from
-// the basis table wh[t][s] = Wh_t(X^s).
-__global__ void k_rs_level(f128 *__restrict__ cw, int k, int d, int t,
-                           const f128 *__restrict__ wh) {
-  size_t pairs = (size_t)1 << (d - 1 + k);
-  size_t cmask = ((size_t)1 << k) - 1;
-  size_t half = (size_t)1 << t;
-  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < pairs;
-       i += (size_t)gridDim.x * blockDim.x) {
-    size_t c = i & cmask, p = i >> k;
-    size_t base = (p >> t) << (t + 1);
-    size_t j = p & (half - 1);
-    f128 lam = mk(0, 0);
-    for (int sb = t + 1; sb < d; sb++)
-      if ((base >> sb) & 1) lam = gadd(lam, wh[t * kMaxRsDim + sb]);
-    size_t iu = ((base + j) << k) + c, iw = ((base + half + j) << k) + c;
-    f128 u = ld(cw + iu), w = ld(cw + iw);
-    f128 u2 = gadd(u, gmul(lam, w));
-    st(cw + iu, u2);
-    st(cw + iw, gadd(u2, w));
+// Levels [s, s + r) of the FFT, top down, on a shared-memory tile of 2^r rows
+// (row y of the tile is codeword row ((z0 + y) << s) | lo) by C = 2^cshift
+// columns; whs holds the basis table's rows s .. s + r - 1 (kMaxRsDim each).
+__device__ __forceinline__ void rs_tile_levels(f128 *tile, int s, int r, int cshift, int d,
+                                               size_t z0, size_t lo, const f128 *whs) {
+  const int pairs = 1 << (r - 1 + cshift);
+  const int cmask = (1 << cshift) - 1;
+  for (int t = s + r - 1; t >= s; t--) {
+    const int ht = t - s;  // the level's half-distance in tile rows: 2^ht
+    for (int q = threadIdx.x; q < pairs; q += blockDim.x) {
+      const int c = q & cmask, p = q >> cshift;
+      const int yu = ((p >> ht) << (ht + 1)) | (p & ((1 << ht) - 1));
+      const int yw = yu + (1 << ht);
+      const f128 lam = rs_lambda(whs + (t - s) * kMaxRsDim, t, d, ((z0 + (size_t)yu) << s) | lo);
+      const f128 u = tile[(yu << cshift) + c], w = tile[(yw << cshift) + c];
+      const f128 u2 = gadd(u, gmul(lam, w));
+      tile[(yu << cshift) + c] = u2;
+      tile[(yw << cshift) + c] = gadd(u2, w);
+    }
+    __syncthreads();
   }
 }
 
-// The whole encode of a codeword that fits one block's shared memory: the
-// spread, then every level of k_rs_level in place, one launch instead of
-// l + 1 (the Ligerito levels' codewords are 2^8 .. 2^13 entries).
+// One pass of the FFT over levels [s, s + r), one tile per block: the tile
+// (the 2^r rows whose row bits [s, s + r) vary, the others fixed, by C
+// columns) arrives by one TMA tensor copy, its r levels run in shared memory
+// and it leaves by one TMA tensor copy. Tensor maps see a codeword of 2^rows
+// rows as (u64 words of a row, row bits below s, row bits from s up); a box
+// is (2C, 1, 2^r). The first pass (`first`) reads the message (rows = l) and
+// writes repetition `rep` of the codeword (its row bits from l up), so the
+// spread costs no pass of its own; later passes read and write the codeword.
+// A copy that has not landed within its time limit sets *err and the block
+// returns.
+constexpr int kRsTileEntries = 1024;  // 16 KiB tiles
+constexpr int kRsPassLevels = 6;      // levels per pass at most
+__global__ void __launch_bounds__(512) k_rs_pass(const __grid_constant__ CUtensorMap src,
+                                                 const __grid_constant__ CUtensorMap dst, int d,
+                                                 int l, int s, int r, int cshift, int ncc,
+                                                 int first, const f128 *__restrict__ wh,
+                                                 unsigned int *err) {
+  __shared__ __align__(128) f128 tile[kRsTileEntries];
+  __shared__ f128 whs[kRsPassLevels * kMaxRsDim];
+  __shared__ uint64_t bar;
+  const int src_rows = first ? l : d;
+  // block -> (column chunk, row bits below s, row bits above s + r, repetition)
+  unsigned b = blockIdx.x;
+  const int cc = (int)(b % (unsigned)ncc);
+  b /= (unsigned)ncc;
+  const size_t lo = b & (((size_t)1 << s) - 1);
+  b >>= s;
+  const size_t nhi = (size_t)1 << (src_rows - s - r);
+  const size_t hi = b % nhi;
+  const size_t rep = b / nhi;
+  const int x = 2 * (cc << cshift);
+  const size_t zs = hi << r;                            // tile's first row group, source
+  const size_t zd = (first ? rep << (l - s) : 0) + zs;  // and destination
+  const uint32_t bytes = (uint32_t)(16u << (r + cshift));
+  if (threadIdx.x == 0) {
+    mbar_init(&bar);
+    mbar_expect(&bar, bytes);
+    tensor_load_3d(tile, &src, x, (int)lo, (int)zs, &bar);
+  }
+  // the pass's rows of the basis table while the tile is in flight
+  for (int i = threadIdx.x; i < r * d; i += blockDim.x)
+    whs[(i / d) * kMaxRsDim + i % d] = wh[(s + i / d) * kMaxRsDim + i % d];
+  __syncthreads();
+  if (!mbar_wait(&bar, 0)) {
+    if (threadIdx.x == 0) {
+      if (err) *reinterpret_cast<volatile unsigned int *>(err) = 1u;
+      mbar_wait(&bar, 0);  // the copy may still land: give it one more limit
+    }
+    return;
+  }
+  rs_tile_levels(tile, s, r, cshift, d, zd, lo, whs);
+  fence_async_shared();
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    tensor_store_3d(&dst, x, (int)lo, (int)zd, tile);
+    bulk_store_drain();
+  }
+}
+
+// The whole encode of a small codeword (at most 2^10 entries) in one block:
+// the message arrives by one bulk copy, is repeated across the row blocks in
+// shared memory, every level runs in place and the codeword leaves by one
+// bulk copy. Larger codewords go through k_rs_pass, whose tiles spread a
+// level over 128 or more blocks.
 constexpr int kRsBlockThreads = 1024;
-constexpr size_t kRsBlockMax = (size_t)1 << 13;  // 128 KiB of shared memory
+constexpr int kRsBlockLog = 10;
+constexpr size_t kRsBlockMax = (size_t)1 << kRsBlockLog;  // 16 KiB of shared memory
 __global__ void __launch_bounds__(kRsBlockThreads) k_rs_encode_block(const f128 *__restrict__ msg,
                                                                      int k, int l, int d,
                                                                      const f128 *__restrict__ wh,
-                                                                     f128 *__restrict__ cw) {
-  extern __shared__ f128 sm[];
+                                                                     f128 *__restrict__ cw,
+                                                                     unsigned int *err) {
+  __shared__ __align__(128) f128 sm[kRsBlockMax];
+  __shared__ f128 whs[kRsBlockLog * kRsBlockLog];
+  __shared__ uint64_t bar;
   const size_t total = (size_t)1 << (d + k);
-  const size_t mmask = ((size_t)1 << (l + k)) - 1;
-  for (size_t i = threadIdx.x; i < total; i += blockDim.x) sm[i] = ld(msg + (i & mmask));
+  const size_t mlen = (size_t)1 << (l + k);
+  if (threadIdx.x == 0) {
+    mbar_init(&bar);
+    mbar_expect(&bar, (uint32_t)(mlen * sizeof(f128)));
+    bulk_load(sm, msg, (uint32_t)(mlen * sizeof(f128)), &bar);
+  }
+  // the basis table's rows t < l, columns sb < d, while the message is in flight
+  for (int i = threadIdx.x; i < l * d; i += blockDim.x)
+    whs[(i / d) * kRsBlockLog + i % d] = wh[(i / d) * kMaxRsDim + i % d];
+  __syncthreads();
+  if (!mbar_wait(&bar, 0)) {
+    if (threadIdx.x == 0) {
+      if (err) *reinterpret_cast<volatile unsigned int *>(err) = 1u;
+      mbar_wait(&bar, 0);
+    }
+    return;
+  }
+  for (size_t i = mlen + threadIdx.x; i < total; i += blockDim.x) sm[i] = sm[i & (mlen - 1)];
   __syncthreads();
   const size_t cmask = ((size_t)1 << k) - 1;
   for (int t = l - 1; t >= 0; t--) {
@@ -412,9 +502,7 @@ __global__ void __launch_bounds__(kRsBlockThreads) k_rs_encode_block(const f128 
       const size_t c = i & cmask, p = i >> k;
       const size_t base = (p >> t) << (t + 1);
       const size_t j = p & (half - 1);
-      f128 lam = mk(0, 0);
-      for (int sb = t + 1; sb < d; sb++)
-        if ((base >> sb) & 1) lam = gadd(lam, wh[t * kMaxRsDim + sb]);
+      const f128 lam = rs_lambda(whs + t * kRsBlockLog, t, d, base);
       const size_t iu = ((base + j) << k) + c, iw = ((base + half + j) << k) + c;
       const f128 u = sm[iu], w = sm[iw];
       const f128 u2 = gadd(u, gmul(lam, w));
@@ -423,29 +511,81 @@ __global__ void __launch_bounds__(kRsBlockThreads) k_rs_encode_block(const f128 
     }
     __syncthreads();
   }
-  for (size_t i = threadIdx.x; i < total; i += blockDim.x) st(cw + i, sm[i]);
+  fence_async_shared();
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    bulk_store(cw, sm, (uint32_t)(total * sizeof(f128)));
+    bulk_store_drain();
+  }
 }
 
+namespace {
+
+PFN_cuTensorMapEncodeTiled tensor_map_encoder() {
+  static PFN_cuTensorMapEncodeTiled fn = [] {
+    void *p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    BZ_CUDA(cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q));
+    if (!p || q != cudaDriverEntryPointSuccess)
+      throw CudaError("cuTensorMapEncodeTiled is not available");
+    return reinterpret_cast<PFN_cuTensorMapEncodeTiled>(p);
+  }();
+  return fn;
+}
+
+// The 3-D view of a codeword of 2^rows rows x 2^k columns that k_rs_pass
+// copies: (2^(k+1) u64 words of a row, 2^s rows below bit s, 2^(rows-s) row
+// groups), box (2C, 1, 2^r).
+CUtensorMap rows_map(const f128 *base, int rows, int k, int s, int r, int cshift) {
+  CUtensorMap m;
+  const cuuint64_t row_bytes = (cuuint64_t)16 << k;
+  const cuuint64_t dim[3] = {(cuuint64_t)2 << k, (cuuint64_t)1 << s, (cuuint64_t)1 << (rows - s)};
+  const cuuint64_t stride[2] = {row_bytes, row_bytes << s};
+  const cuuint32_t box[3] = {(cuuint32_t)2 << cshift, 1, (cuuint32_t)1 << r};
+  const cuuint32_t estride[3] = {1, 1, 1};
+  const CUresult rc = tensor_map_encoder()(
+      &m, CU_TENSOR_MAP_DATA_TYPE_UINT64, 3, const_cast<f128 *>(base), dim, stride, box, estride,
+      CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+      CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (rc != CUDA_SUCCESS) throw CudaError("cuTensorMapEncodeTiled failed for a codeword view");
+  return m;
+}
+
+}  // namespace
+
 void rs_encode(const f128 *msg, int log_n, int k, int rate, const f128 *wh, f128 *cw,
-               cudaStream_t s) {
-  int l = log_n - k, d = l + rate;
-  size_t total = (size_t)1 << (d + k);
+               unsigned int *err, cudaStream_t s) {
+  const int l = log_n - k, d = l + rate;
+  const size_t total = (size_t)1 << (d + k);
   if (total <= kRsBlockMax) {
-    static const bool attr = [] {
-      BZ_CUDA(cudaFuncSetAttribute(k_rs_encode_block, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                   (int)(kRsBlockMax * sizeof(f128))));
-      return true;
-    }();
-    (void)attr;
-    k_rs_encode_block<<<1, kRsBlockThreads, total * sizeof(f128), s>>>(msg, k, l, d, wh, cw);
+    k_rs_encode_block<<<1, kRsBlockThreads, 0, s>>>(msg, k, l, d, wh, cw, err);
     BZ_LAUNCH_CHECK();
     return;
   }
-  k_rs_spread<<<grid_for(total), kThreads, 0, s>>>(msg, k, l, d, cw);
-  BZ_LAUNCH_CHECK();
-  for (int t = l - 1; t >= 0; t--) {
-    k_rs_level<<<grid_for(total / 2), kThreads, 0, s>>>(cw, k, d, t, wh);
+  if (l < 1) throw CudaError("rs_encode: a codeword of one message row");
+  // the levels split into passes of at most 6, top down, the first from the
+  // message; a pass of r levels takes tiles of 2^r rows by C = 2^cshift
+  // columns, C as wide as keeps 128 or more tiles (blocks) per pass and a
+  // tile within kRsTileEntries (a pass has 2^(d + k - r - cshift) tiles)
+  const int npass = (l + kRsPassLevels - 1) / kRsPassLevels;
+  int top = l;  // levels [0, top) remain
+  bool first = true;
+  for (int pass = 0; pass < npass; pass++) {
+    const int r = (top + (npass - pass) - 1) / (npass - pass);
+    const int sb = top - r;
+    int cshift = std::min(std::min(k, 6), 10 - r);
+    cshift = std::max(0, std::min(cshift, d + k - 7 - r));
+    const int ncc = 1 << (k - cshift);
+    const int src_rows = first ? l : d;
+    const CUtensorMap src = rows_map(first ? msg : cw, src_rows, k, sb, r, cshift);
+    const CUtensorMap dst = rows_map(cw, d, k, sb, r, cshift);
+    const size_t blocks = (size_t)ncc << (src_rows - r) << (first ? d - l : 0);
+    const int threads = std::min(512, 1 << (r - 1 + cshift));
+    k_rs_pass<<<(unsigned)blocks, threads, 0, s>>>(src, dst, d, l, sb, r, cshift, ncc,
+                                                   first ? 1 : 0, wh, err);
     BZ_LAUNCH_CHECK();
+    top = sb;
+    first = false;
   }
 }
 
@@ -641,8 +781,7 @@ void preload_pcs_kernels() {
                 (const void *)k_packed_basis,
                 (const void *)k_dot,
                 (const void *)k_axpy,
-                (const void *)k_rs_spread,
-                (const void *)k_rs_level,
+                (const void *)k_rs_pass,
                 (const void *)k_rs_encode_block,
                 (const void *)k_merkle_leaves,
                 (const void *)k_merkle_parents,

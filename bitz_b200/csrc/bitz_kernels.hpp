@@ -31,8 +31,12 @@ void packed_basis(const f128 *suffix, size_t n, const f128 *bw, const f128 *eq_o
 void axpy(f128 *y, f128 a, const f128 *x, size_t n, cudaStream_t s);
 void dot(const f128 *a, const f128 *b, size_t n, unsigned long long *acc, Publish pub,
          cudaStream_t s);
+// Interleaved Reed-Solomon encode of msg (2^log_n entries, 2^k columns) at
+// rate 2^-rate into cw, staged through shared memory by TMA copies; err (a
+// word the host reads; null: no report) is set when a copy did not land
+// within its time limit.
 void rs_encode(const f128 *msg, int log_n, int k, int rate, const f128 *wh, f128 *cw,
-               cudaStream_t s);
+               unsigned int *err, cudaStream_t s);
 void merkle_build(const f128 *cw, size_t rows, int k, uint32_t *nodes, cudaStream_t s);
 // A small tree (at most kMerkleBlockMaxRows rows) in one launch that posts
 // the root (node 1, 32 bytes) as four mailbox words of publication pub; false

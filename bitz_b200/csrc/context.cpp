@@ -71,6 +71,15 @@ void RoundChannel::send(const uint64_t *words, int n) {
   std::atomic_thread_fence(std::memory_order_release);
 }
 
+void RoundChannel::check_device_error(const char *stage) {
+  if (!err_host) return;
+  volatile unsigned int *e = err_host;
+  if (*e) {
+    *e = 0;
+    throw CudaError(std::string(stage) + ": a TMA copy did not land within its time limit");
+  }
+}
+
 void RoundChannel::abort() {
   volatile unsigned long long *s = down_host->slot;
   for (int k = 0; k < 2 * kMailboxWords; k++) s[k] = 0xffffffffull << 32;
@@ -253,6 +262,8 @@ Context::Context() {
   channel_.dev = (Mailbox *)mbd;
   channel_.down_host = (Mailbox *)((char *)mb + 512);
   channel_.down_dev = (Mailbox *)((char *)mbd + 512);
+  channel_.err_host = (unsigned int *)((char *)mb + 1024);
+  channel_.err_dev = (unsigned int *)((char *)mbd + 1024);
   counter_.resize(1);
   BZ_CUDA(cudaMemset(counter_.get(), 0, sizeof(unsigned int)));
   channel_.counter = counter_.get();

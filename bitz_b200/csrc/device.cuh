@@ -221,6 +221,11 @@ struct RoundChannel {
   unsigned long long down_next = 0;
   // host time spent inside wait() and the number of waits (phase timer)
   unsigned long long wait_ns = 0, waits = 0;
+  // A word in the same mapped page that the lane's kernels set when a bounded
+  // wait of theirs ran out (a TMA copy that did not land); check_device_error
+  // throws (and clears it) when it is set.
+  unsigned int *err_host = nullptr, *err_dev = nullptr;
+  void check_device_error(const char *stage);
   Publish arm() { return Publish{counter, dev, ++next}; }
   // Waits for the publication armed last; copies n payload words.
   void wait(cudaStream_t s, uint64_t *out, int n);

@@ -389,9 +389,9 @@ int ProofSystem::commit(cudaStream_t s) {
   codeword0_->resize(rows << L0.k);
   nodes0_->resize(16 * rows);
   const f128 *fpk = reinterpret_cast<const f128 *>(f_->get());
-  rs_encode(fpk, log_n, L0.k, L0.log_inv_rate, T.wh.get(), codeword0_->get(), s);
-  f128 *root_h = W.pin_small.get(kPinSmall) + kPinRoot;
   RoundChannel *lch = lane_->channel();
+  rs_encode(fpk, log_n, L0.k, L0.log_inv_rate, T.wh.get(), codeword0_->get(), lch->err_dev, s);
+  f128 *root_h = W.pin_small.get(kPinSmall) + kPinRoot;
   if (rows <= kMerkleBlockMaxRows &&
       merkle_build_posted(codeword0_->get(), rows, L0.k, nodes0_->get(), lch->arm(), s)) {
     // a small tree in one launch that posts its root
@@ -401,6 +401,7 @@ int ProofSystem::commit(cudaStream_t s) {
     BZ_CUDA(cudaMemcpyAsync(root_h, nodes0_->get() + 8, 32, cudaMemcpyDeviceToHost, s));
     BZ_CUDA(stream_wait(s));
   }
+  lch->check_device_error("commit");
   memcpy(root_, root_h, 32);
   const char *dom = circuit_name(kind_);
   ts_.reset(new Transcript((const uint8_t *)"bitz/circuit-e2e/v2", 19, (const uint8_t *)dom,
@@ -551,7 +552,7 @@ std::vector<uint8_t> ProofSystem::ligerito(cudaStream_t s, f128 target) {
       nrows = (size_t)1 << (l - N.k + N.log_inv_rate);
       next_cw[flip].resize(nrows << N.k);
       next_nodes[flip].resize(16 * nrows);
-      rs_encode(f, l, N.k, N.log_inv_rate, T.wh.get(), next_cw[flip].get(), s);
+      rs_encode(f, l, N.k, N.log_inv_rate, T.wh.get(), next_cw[flip].get(), ch->err_dev, s);
       f128 *root_h = W.pin_small.get(kPinSmall) + kPinLevelRoot;
       if (nrows <= kMerkleBlockMaxRows &&
           merkle_build_posted(next_cw[flip].get(), nrows, N.k, next_nodes[flip].get(), ch->arm(),
@@ -563,6 +564,7 @@ std::vector<uint8_t> ProofSystem::ligerito(cudaStream_t s, f128 target) {
                                 s));
         BZ_CUDA(stream_wait(s));
       }
+      ch->check_device_error("ligerito");
       uint8_t root[36];
       uint32_t len = 32;
       memcpy(root, &len, 4);
