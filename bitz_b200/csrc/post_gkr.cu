@@ -16,6 +16,17 @@
 
 namespace bz {
 
+// One pair's share of the next round's (a0, a2) = (w0 v0, (w0 + w1)(v0 + v1)).
+// A product whose V factor is zero is skipped: it adds nothing, and the
+// committed bits past the witness's last one are zero padding (most of f for
+// small statements), so whole stretches of V stay zero round after round.
+__device__ __forceinline__ void pair_sums(wide &a0, wide &a2, f128 w0, f128 w1, f128 v0,
+                                          f128 v1) {
+  if (!gis_zero(v0)) wacc(a0, gmul_wide(w0, v0));
+  const f128 dv = gadd(v0, v1);
+  if (!gis_zero(dv)) wacc(a2, gmul_wide(gadd(w0, w1), dv));
+}
+
 // Round 1 message and the claim check, one warp per packed element: lane l
 // owns bit pairs l and l + 32, so the warp reads the element's 128 row
 // weights as one contiguous 2 KiB run.
@@ -30,6 +41,7 @@ __global__ void pg_first_message(const f128 *__restrict__ rows, int log_rows,
   wide a0 = wzero(), a2 = wzero(), ws = wzero();
   for (size_t e = warp; e < npacked; e += nwarps) {
     f128 word = ld(packed + e);
+    if (gis_zero(word)) continue;  // no set bit: nothing to add (the warp's whole element)
     const f128 *rw = rows + ((e & per_col_mask) << 7);
     f128 s0 = mk(0, 0), s2 = mk(0, 0), sw = mk(0, 0);
     // Branch-free: each lane's two bits become all-ones / all-zero masks.
@@ -103,8 +115,7 @@ __global__ void pg_first_fold(const f128 *__restrict__ rows, int log_rows,
     st(w_out + i0 + 1, w1);
     st(v_out + i0, v0);
     st(v_out + i0 + 1, v1);
-    wacc(a0, gmul_wide(w0, v0));
-    wacc(a2, gmul_wide(gadd(w0, w1), gadd(v0, v1)));
+    pair_sums(a0, a2, w0, w1, v0, v1);
   }
   f128 r0 = greduce(a0), r2 = greduce(a2);
   uint64_t v[4] = {r0.lo, r0.hi, r2.lo, r2.hi};
@@ -143,10 +154,7 @@ __global__ void pg_round(const f128 *__restrict__ w_in, const f128 *__restrict__
       f128 fv1 = gadd(v2, mul_table(T, gadd(v2, v3)));
       st(w_out + o + 1, fw1);
       st(v_out + o + 1, fv1);
-      if (emit) {
-        wacc(a0, gmul_wide(fw0, fv0));
-        wacc(a2, gmul_wide(gadd(fw0, fw1), gadd(fv0, fv1)));
-      }
+      if (emit) pair_sums(a0, a2, fw0, fw1, fv0, fv1);
     }
   }
   if (emit) {
@@ -164,8 +172,7 @@ __global__ void pg_sums(const f128 *__restrict__ w, const f128 *__restrict__ v, 
   for (size_t j = blockIdx.x * (size_t)blockDim.x + threadIdx.x; j < n / 2;
        j += (size_t)gridDim.x * blockDim.x) {
     f128 w0 = ld(w + 2 * j), w1 = ld(w + 2 * j + 1), v0 = ld(v + 2 * j), v1 = ld(v + 2 * j + 1);
-    wacc(a0, gmul_wide(w0, v0));
-    wacc(a2, gmul_wide(gadd(w0, w1), gadd(v0, v1)));
+    pair_sums(a0, a2, w0, w1, v0, v1);
   }
   f128 r0 = greduce(a0), r2 = greduce(a2);
   uint64_t o[4] = {r0.lo, r0.hi, r2.lo, r2.hi};
@@ -261,8 +268,7 @@ __global__ void __launch_bounds__(kThreads) pg_tail(const f128 *__restrict__ w_i
     wide a0 = wzero(), a2 = wzero();
     for (int j = threadIdx.x; j < len / 2; j += blockDim.x) {
       f128 w0 = W[2 * j], w1 = W[2 * j + 1], v0 = V[2 * j], v1 = V[2 * j + 1];
-      wacc(a0, gmul_wide(w0, v0));
-      wacc(a2, gmul_wide(gadd(w0, w1), gadd(v0, v1)));
+      pair_sums(a0, a2, w0, w1, v0, v1);
     }
     f128 s0 = greduce(a0), s2 = greduce(a2);
     uint64_t vv[4] = {s0.lo, s0.hi, s2.lo, s2.hi};
@@ -355,8 +361,7 @@ __global__ void __launch_bounds__(kThreads) pg_mid(const f128 *__restrict__ w_in
     wide a0 = wzero(), a2 = wzero();
     for (size_t j = threadIdx.x; j < len / 2; j += blockDim.x) {
       const f128 w0 = W[2 * j], w1 = W[2 * j + 1], v0 = V[2 * j], v1 = V[2 * j + 1];
-      wacc(a0, gmul_wide(w0, v0));
-      wacc(a2, gmul_wide(gadd(w0, w1), gadd(v0, v1)));
+      pair_sums(a0, a2, w0, w1, v0, v1);
     }
     const f128 r0 = greduce(a0), r2 = greduce(a2);
     uint64_t v[4] = {r0.lo, r0.hi, r2.lo, r2.hi};
