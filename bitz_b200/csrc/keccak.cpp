@@ -1,8 +1,12 @@
 // Keccak-f[1600] (FIPS 202 section 3.3) for the host transcript sponge, each
 // round fully unrolled over the 25 lanes held in registers: theta, then rho
 // and pi folded into one lane permutation (lane (x, y) moves to
-// (y, 2x + 3y) rotated by its rho offset), then chi and iota.
+// (y, 2x + 3y) rotated by its rho offset), then chi and iota. Three builds of
+// the same round: AVX-512VL (one lane per vector register), BMI1/BMI2 and
+// plain x86-64, the first the host supports (BITZ_HOST_SIMD=0 skips AVX-512).
 #include "transcript.hpp"
+
+#include <immintrin.h>
 
 namespace bz {
 
@@ -99,9 +103,101 @@ static void keccak_generic(uint64_t st[25]) { KECCAK_BODY }
 // third faster where the CPU has them.
 __attribute__((target("bmi,bmi2"))) static void keccak_bmi(uint64_t st[25]) { KECCAK_BODY }
 
+// The same round with every lane in its own 128-bit vector register (32 of
+// them with AVX-512VL, so the state stays out of memory): three-input XORs
+// and chi as one ternary-logic instruction each, rotations by VPROLQ. Lane
+// (x, y) ^ D[x] is formed as lane ^ C[x-1] ^ rot(C[x+1], 1) in one step.
+#define XOR3(a, b, c) _mm_ternarylogic_epi64(a, b, c, 0x96)
+#define CHI(a, b, c) _mm_ternarylogic_epi64(a, b, c, 0xD2) /* a ^ (~b & c) */
+#define KECCAK_ROUND_VL(RC) \
+  { \
+    const __m128i c0 = XOR3(XOR3(a0, a5, a10), a15, a20); \
+    const __m128i c1 = XOR3(XOR3(a1, a6, a11), a16, a21); \
+    const __m128i c2 = XOR3(XOR3(a2, a7, a12), a17, a22); \
+    const __m128i c3 = XOR3(XOR3(a3, a8, a13), a18, a23); \
+    const __m128i c4 = XOR3(XOR3(a4, a9, a14), a19, a24); \
+    const __m128i r0 = _mm_rol_epi64(c0, 1); \
+    const __m128i r1 = _mm_rol_epi64(c1, 1); \
+    const __m128i r2 = _mm_rol_epi64(c2, 1); \
+    const __m128i r3 = _mm_rol_epi64(c3, 1); \
+    const __m128i r4 = _mm_rol_epi64(c4, 1); \
+    const __m128i b0 = XOR3(a0, c4, r1); \
+    const __m128i b1 = _mm_rol_epi64(XOR3(a6, c0, r2), 44); \
+    const __m128i b2 = _mm_rol_epi64(XOR3(a12, c1, r3), 43); \
+    const __m128i b3 = _mm_rol_epi64(XOR3(a18, c2, r4), 21); \
+    const __m128i b4 = _mm_rol_epi64(XOR3(a24, c3, r0), 14); \
+    const __m128i b5 = _mm_rol_epi64(XOR3(a3, c2, r4), 28); \
+    const __m128i b6 = _mm_rol_epi64(XOR3(a9, c3, r0), 20); \
+    const __m128i b7 = _mm_rol_epi64(XOR3(a10, c4, r1), 3); \
+    const __m128i b8 = _mm_rol_epi64(XOR3(a16, c0, r2), 45); \
+    const __m128i b9 = _mm_rol_epi64(XOR3(a22, c1, r3), 61); \
+    const __m128i b10 = _mm_rol_epi64(XOR3(a1, c0, r2), 1); \
+    const __m128i b11 = _mm_rol_epi64(XOR3(a7, c1, r3), 6); \
+    const __m128i b12 = _mm_rol_epi64(XOR3(a13, c2, r4), 25); \
+    const __m128i b13 = _mm_rol_epi64(XOR3(a19, c3, r0), 8); \
+    const __m128i b14 = _mm_rol_epi64(XOR3(a20, c4, r1), 18); \
+    const __m128i b15 = _mm_rol_epi64(XOR3(a4, c3, r0), 27); \
+    const __m128i b16 = _mm_rol_epi64(XOR3(a5, c4, r1), 36); \
+    const __m128i b17 = _mm_rol_epi64(XOR3(a11, c0, r2), 10); \
+    const __m128i b18 = _mm_rol_epi64(XOR3(a17, c1, r3), 15); \
+    const __m128i b19 = _mm_rol_epi64(XOR3(a23, c2, r4), 56); \
+    const __m128i b20 = _mm_rol_epi64(XOR3(a2, c1, r3), 62); \
+    const __m128i b21 = _mm_rol_epi64(XOR3(a8, c2, r4), 55); \
+    const __m128i b22 = _mm_rol_epi64(XOR3(a14, c3, r0), 39); \
+    const __m128i b23 = _mm_rol_epi64(XOR3(a15, c4, r1), 41); \
+    const __m128i b24 = _mm_rol_epi64(XOR3(a21, c0, r2), 2); \
+    a0 = CHI(b0, b1, b2); \
+    a1 = CHI(b1, b2, b3); \
+    a2 = CHI(b2, b3, b4); \
+    a3 = CHI(b3, b4, b0); \
+    a4 = CHI(b4, b0, b1); \
+    a5 = CHI(b5, b6, b7); \
+    a6 = CHI(b6, b7, b8); \
+    a7 = CHI(b7, b8, b9); \
+    a8 = CHI(b8, b9, b5); \
+    a9 = CHI(b9, b5, b6); \
+    a10 = CHI(b10, b11, b12); \
+    a11 = CHI(b11, b12, b13); \
+    a12 = CHI(b12, b13, b14); \
+    a13 = CHI(b13, b14, b10); \
+    a14 = CHI(b14, b10, b11); \
+    a15 = CHI(b15, b16, b17); \
+    a16 = CHI(b16, b17, b18); \
+    a17 = CHI(b17, b18, b19); \
+    a18 = CHI(b18, b19, b15); \
+    a19 = CHI(b19, b15, b16); \
+    a20 = CHI(b20, b21, b22); \
+    a21 = CHI(b21, b22, b23); \
+    a22 = CHI(b22, b23, b24); \
+    a23 = CHI(b23, b24, b20); \
+    a24 = CHI(b24, b20, b21); \
+    a0 = _mm_xor_si128(a0, _mm_cvtsi64_si128((long long)(RC))); \
+  }
+
+__attribute__((target("avx512f,avx512vl"))) static void keccak_vl(uint64_t st[25]) {
+  __m128i a0, a1, a2, a3, a4, a5, a6, a7, a8, a9, a10, a11, a12, a13, a14, a15, a16, a17, a18, a19, a20, a21, a22, a23, a24;
+#define LOAD(i) a##i = _mm_cvtsi64_si128((long long)st[i])
+  LOAD(0); LOAD(1); LOAD(2); LOAD(3); LOAD(4); LOAD(5); LOAD(6); LOAD(7); LOAD(8); LOAD(9); LOAD(10); LOAD(11); LOAD(12); LOAD(13); LOAD(14); LOAD(15); LOAD(16); LOAD(17); LOAD(18); LOAD(19); LOAD(20); LOAD(21); LOAD(22); LOAD(23); LOAD(24);
+#undef LOAD
+  for (int round = 0; round < 24; round++) KECCAK_ROUND_VL(KRC[round]);
+#define STORE(i) st[i] = (uint64_t)_mm_cvtsi128_si64(a##i)
+  STORE(0); STORE(1); STORE(2); STORE(3); STORE(4); STORE(5); STORE(6); STORE(7); STORE(8); STORE(9); STORE(10); STORE(11); STORE(12); STORE(13); STORE(14); STORE(15); STORE(16); STORE(17); STORE(18); STORE(19); STORE(20); STORE(21); STORE(22); STORE(23); STORE(24);
+#undef STORE
+}
+#undef KECCAK_ROUND_VL
+#undef CHI
+#undef XOR3
+
 void keccak_f1600(uint64_t st[25]) {
-  static const bool bmi = __builtin_cpu_supports("bmi") && __builtin_cpu_supports("bmi2");
-  if (bmi)
+  static const int path = [] {
+    if (host_simd_enabled() && __builtin_cpu_supports("avx512f") &&
+        __builtin_cpu_supports("avx512vl"))
+      return 2;
+    return __builtin_cpu_supports("bmi") && __builtin_cpu_supports("bmi2") ? 1 : 0;
+  }();
+  if (path == 2)
+    keccak_vl(st);
+  else if (path == 1)
     keccak_bmi(st);
   else
     keccak_generic(st);

@@ -101,15 +101,17 @@ __attribute__((target("avx512f"))) static uint64_t pow_search16(const uint32_t w
 }
 #undef BZ_B3_G16
 
-// The AVX-512 paths (grinding, the prime's strong rounds) run where the host
-// has the instructions, unless BITZ_HOST_SIMD=0 selects the scalar ones.
-static bool host_simd() {
+// The AVX-512 paths (grinding, the prime's strong rounds, the Keccak
+// permutation) run where the host has the instructions, unless
+// BITZ_HOST_SIMD=0 selects the scalar ones.
+bool host_simd_enabled() {
   static const bool on = [] {
     const char *v = getenv("BITZ_HOST_SIMD");
     return !(v && v[0] == '0');
   }();
   return on;
 }
+static bool host_simd() { return host_simd_enabled(); }
 
 uint64_t pow_search(const uint8_t seed[16], uint32_t bits) {
   if (bits == 0) return 0;

@@ -24,6 +24,9 @@ namespace bz {
 typedef unsigned __int128 u128;
 
 void keccak_f1600(uint64_t st[25]);
+// False when BITZ_HOST_SIMD=0: the host paths then avoid AVX-512 (grinding,
+// the prime's strong rounds, the Keccak permutation).
+bool host_simd_enabled();
 
 class Transcript {
  public:

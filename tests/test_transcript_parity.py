@@ -109,13 +109,14 @@ def test_hints_bypass_the_sponge():
 
 @pytest.mark.skipif(os.environ.get("BITZ_HOST_SIMD") == "0", reason="already the scalar paths")
 def test_scalar_host_paths_agree_too():
-    # BITZ_HOST_SIMD=0 selects the one-nonce-at-a-time grind and the
-    # thread-pool strong rounds (the paths of hosts without AVX-512); the
-    # grinding and prime tests above rerun on them in a fresh process.
+    # BITZ_HOST_SIMD=0 selects the one-nonce-at-a-time grind, the
+    # thread-pool strong rounds and the general-register Keccak permutation
+    # (the paths of hosts without AVX-512); the event-sequence, grinding and
+    # prime tests above rerun on them in a fresh process.
     env = dict(os.environ, BITZ_HOST_SIMD="0")
     r = subprocess.run(
         [sys.executable, "-m", "pytest", "-q", "-p", "no:cacheprovider", __file__,
-         "-k", "grinding or prime"],
+         "-k", "event_sequence or grinding or prime"],
         env=env, capture_output=True, text=True, timeout=600)
     assert r.returncode == 0, r.stdout[-2000:] + r.stderr[-2000:]
 
