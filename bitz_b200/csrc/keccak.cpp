@@ -174,16 +174,38 @@ __attribute__((target("bmi,bmi2"))) static void keccak_bmi(uint64_t st[25]) { KE
     a0 = _mm_xor_si128(a0, _mm_cvtsi64_si128((long long)(RC))); \
   }
 
-__attribute__((target("avx512f,avx512vl"))) static void keccak_vl(uint64_t st[25]) {
-  __m128i a0, a1, a2, a3, a4, a5, a6, a7, a8, a9, a10, a11, a12, a13, a14, a15, a16, a17, a18, a19, a20, a21, a22, a23, a24;
-#define LOAD(i) a##i = _mm_cvtsi64_si128((long long)st[i])
-  LOAD(0); LOAD(1); LOAD(2); LOAD(3); LOAD(4); LOAD(5); LOAD(6); LOAD(7); LOAD(8); LOAD(9); LOAD(10); LOAD(11); LOAD(12); LOAD(13); LOAD(14); LOAD(15); LOAD(16); LOAD(17); LOAD(18); LOAD(19); LOAD(20); LOAD(21); LOAD(22); LOAD(23); LOAD(24);
-#undef LOAD
-  for (int round = 0; round < 24; round++) KECCAK_ROUND_VL(KRC[round]);
-#define STORE(i) st[i] = (uint64_t)_mm_cvtsi128_si64(a##i)
-  STORE(0); STORE(1); STORE(2); STORE(3); STORE(4); STORE(5); STORE(6); STORE(7); STORE(8); STORE(9); STORE(10); STORE(11); STORE(12); STORE(13); STORE(14); STORE(15); STORE(16); STORE(17); STORE(18); STORE(19); STORE(20); STORE(21); STORE(22); STORE(23); STORE(24);
-#undef STORE
+#define VL_LANES(M)                                                                        \
+  M(0) M(1) M(2) M(3) M(4) M(5) M(6) M(7) M(8) M(9) M(10) M(11) M(12) M(13) M(14) M(15) M(16) \
+  M(17) M(18) M(19) M(20) M(21) M(22) M(23) M(24)
+#define VL_RATE_LANES(M) \
+  M(0) M(1) M(2) M(3) M(4) M(5) M(6) M(7) M(8) M(9) M(10) M(11) M(12) M(13) M(14) M(15) M(16)
+#define VL_DECL(i) __m128i a##i = _mm_cvtsi64_si128((long long)st[i]);
+#define VL_STORE(i) st[i] = (uint64_t)_mm_cvtsi128_si64(a##i);
+#define VL_XOR_IN(i) \
+  a##i = _mm_xor_si128(a##i, _mm_loadl_epi64(reinterpret_cast<const __m128i *>(in + 8 * (i))));
+
+// nblocks == 0: one permutation. Otherwise, per block of the rate (136 bytes
+// of `in`): the permutation, then the block XORed into the rate, the state
+// staying in registers from the first block to the last.
+__attribute__((target("avx512f,avx512vl"))) static void keccak_vl(uint64_t st[25],
+                                                                  const uint8_t *in,
+                                                                  size_t nblocks) {
+  VL_LANES(VL_DECL)
+  size_t b = 0;
+  do {
+    for (int round = 0; round < 24; round++) KECCAK_ROUND_VL(KRC[round]);
+    if (nblocks) {
+      VL_RATE_LANES(VL_XOR_IN)
+      in += Transcript::RATE;
+    }
+  } while (++b < nblocks);
+  VL_LANES(VL_STORE)
 }
+#undef VL_XOR_IN
+#undef VL_STORE
+#undef VL_DECL
+#undef VL_RATE_LANES
+#undef VL_LANES
 #undef KECCAK_ROUND_VL
 #undef CHI
 #undef XOR3
@@ -196,11 +218,29 @@ void keccak_f1600(uint64_t st[25]) {
     return __builtin_cpu_supports("bmi") && __builtin_cpu_supports("bmi2") ? 1 : 0;
   }();
   if (path == 2)
-    keccak_vl(st);
+    keccak_vl(st, nullptr, 0);
   else if (path == 1)
     keccak_bmi(st);
   else
     keccak_generic(st);
+}
+void keccak_absorb_blocks(uint64_t st[25], const uint8_t *in, size_t nblocks) {
+  static_assert(__BYTE_ORDER__ == __ORDER_LITTLE_ENDIAN__, "lanes read as memory bytes");
+  if (nblocks == 0) return;
+  static const bool vl = host_simd_enabled() && __builtin_cpu_supports("avx512f") &&
+                         __builtin_cpu_supports("avx512vl");
+  if (vl) {
+    keccak_vl(st, in, nblocks);
+    return;
+  }
+  for (size_t b = 0; b < nblocks; b++, in += Transcript::RATE) {
+    keccak_f1600(st);
+    for (int i = 0; i < Transcript::RATE / 8; i++) {
+      uint64_t v;
+      memcpy(&v, in + 8 * i, 8);
+      st[i] ^= v;
+    }
+  }
 }
 #undef KECCAK_BODY
 #undef KECCAK_ROUND

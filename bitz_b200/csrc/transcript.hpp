@@ -24,6 +24,9 @@ namespace bz {
 typedef unsigned __int128 u128;
 
 void keccak_f1600(uint64_t st[25]);
+// For each 136-byte block of `in`: the permutation, then the block XORed into
+// the rate (the sponge's absorb of whole blocks once its rate is full).
+void keccak_absorb_blocks(uint64_t st[25], const uint8_t *in, size_t nblocks);
 // False when BITZ_HOST_SIMD=0: the host paths then avoid AVX-512 (grinding,
 // the prime's strong rounds, the Keccak permutation).
 bool host_simd_enabled();
@@ -117,6 +120,13 @@ class Transcript {
   // little-endian lanes go in eight bytes at a time once aligned.
   void absorb(const uint8_t *in, size_t n) {
     while (n) {
+      if (absorb_pos_ == RATE && n >= RATE) {  // whole blocks, the state kept in registers
+        const size_t blocks = n / RATE;
+        keccak_absorb_blocks(st_, in, blocks);
+        in += blocks * RATE;
+        n -= blocks * RATE;
+        continue;
+      }
       if (absorb_pos_ == RATE) {
         keccak_f1600(st_);
         absorb_pos_ = 0;
