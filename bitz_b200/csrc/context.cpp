@@ -13,28 +13,29 @@
 namespace bz {
 
 // True once the first 2n slots all carry the tag of publication `want`.
-static bool mailbox_ready(const Mailbox *mb, unsigned long long want, int n) {
-  const volatile unsigned long long *s = mb->slot;
+static bool slots_ready(const unsigned long long *slots, unsigned long long want, int n) {
+  const volatile unsigned long long *s = slots;
   const unsigned long long tag = (want << 32) >> 32;
   for (int k = 0; k < 2 * n; k++)
     if ((s[k] >> 32) != tag) return false;
   return true;
 }
 
-void RoundChannel::wait(cudaStream_t s, uint64_t *out, int n) {
-  if (n > kMailboxWords) throw CudaError("mailbox read too long");
-  const unsigned long long want = next;
+// Waits until n tagged words of publication `want` are in `slots`, surfacing
+// a failed or finished stream instead of spinning; copies the payload.
+static void wait_slots(RoundChannel &ch, cudaStream_t s, const unsigned long long *slots,
+                       unsigned long long want, uint64_t *out, int n) {
   auto t0 = std::chrono::steady_clock::now();
   uint64_t spins = 0;
-  while (!mailbox_ready(host, want, n)) {
+  while (!slots_ready(slots, want, n)) {
     if ((++spins & 0x3ff) == 0) {
       cudaError_t e = cudaStreamQuery(s);
       if (e != cudaSuccess && e != cudaErrorNotReady)
         throw CudaError(std::string("round kernel failed: ") + cudaGetErrorString(e));
-      if (e == cudaSuccess && !mailbox_ready(host, want, n)) {
+      if (e == cudaSuccess && !slots_ready(slots, want, n)) {
         // the stream is idle: its writes land within microseconds
         std::this_thread::sleep_for(std::chrono::milliseconds(2));
-        if (!mailbox_ready(host, want, n))
+        if (!slots_ready(slots, want, n))
           throw CudaError("round kernel finished without publishing its result");
       }
       if (std::chrono::steady_clock::now() - t0 > std::chrono::seconds(30))
@@ -50,12 +51,22 @@ void RoundChannel::wait(cudaStream_t s, uint64_t *out, int n) {
       std::this_thread::yield();
   }
   std::atomic_thread_fence(std::memory_order_acquire);
-  const volatile unsigned long long *p = host->slot;
+  const volatile unsigned long long *p = slots;
   for (int k = 0; k < n; k++) out[k] = (p[2 * k] & 0xffffffffull) | (p[2 * k + 1] << 32);
-  wait_ns += (unsigned long long)std::chrono::duration_cast<std::chrono::nanoseconds>(
-                 std::chrono::steady_clock::now() - t0)
-                 .count();
-  waits++;
+  ch.wait_ns += (unsigned long long)std::chrono::duration_cast<std::chrono::nanoseconds>(
+                    std::chrono::steady_clock::now() - t0)
+                    .count();
+  ch.waits++;
+}
+
+void RoundChannel::wait(cudaStream_t s, uint64_t *out, int n) {
+  if (n > kMailboxWords) throw CudaError("mailbox read too long");
+  wait_slots(*this, s, host->slot, next, out, n);
+}
+
+void RoundChannel::wait_handover(cudaStream_t s, unsigned long long seq, uint64_t *out, int n) {
+  if (!handover_host || n > kHandoverWords) throw CudaError("handover read too long");
+  wait_slots(*this, s, handover_host, seq, out, n);
 }
 
 void RoundChannel::send(const uint64_t *words, int n) {
@@ -254,8 +265,11 @@ Context::Context() {
   gk_.ctl = gk_ctl_.get();
   // the round mailbox: one mapped pinned page and a device block counter
   void *mb = nullptr;
-  BZ_CUDA(cudaHostAlloc(&mb, 4096, cudaHostAllocMapped));
-  memset(mb, 0, 4096);
+  // one mapped allocation: mailbox (0), downbox (512), error word (1024),
+  // handover area (4096, 16 bytes per word)
+  const size_t mapped = 4096 + 16 * (size_t)kHandoverWords;
+  BZ_CUDA(cudaHostAlloc(&mb, mapped, cudaHostAllocMapped));
+  memset(mb, 0, mapped);
   channel_.host = (Mailbox *)mb;
   void *mbd = nullptr;
   BZ_CUDA(cudaHostGetDevicePointer(&mbd, mb, 0));
@@ -264,6 +278,8 @@ Context::Context() {
   channel_.down_dev = (Mailbox *)((char *)mbd + 512);
   channel_.err_host = (unsigned int *)((char *)mb + 1024);
   channel_.err_dev = (unsigned int *)((char *)mbd + 1024);
+  channel_.handover_host = (unsigned long long *)((char *)mb + 4096);
+  channel_.handover_dev = (unsigned long long *)((char *)mbd + 4096);
   counter_.resize(1);
   BZ_CUDA(cudaMemset(counter_.get(), 0, sizeof(unsigned int)));
   channel_.counter = counter_.get();

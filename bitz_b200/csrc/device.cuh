@@ -56,6 +56,7 @@ inline int grid_for(size_t work, int per_block = kThreads, int max_blocks = kSMs
 // so the host accepts the result once every slot shows the current tag, and
 // the device needs no system-scope fence to order data before a flag.
 constexpr int kMailboxWords = 8;  // 64-bit data words per publication
+constexpr int kHandoverWords = 512;  // 64-bit data words of a handover
 struct Mailbox {
   unsigned long long slot[2 * kMailboxWords];
 };
@@ -67,6 +68,15 @@ __device__ __forceinline__ void mailbox_post(Mailbox *mb, unsigned long long seq
   const unsigned long long tag = seq << 32;
   unsigned long long *p = mb->slot + 2 * k;
   asm volatile("st.volatile.global.v2.u64 [%0], {%1, %2};" ::"l"(p),
+               "l"(tag | (v & 0xffffffffull)), "l"(tag | (v >> 32))
+               : "memory");
+}
+
+// Word k of a handover (tagged like a mailbox word) into the mapped area.
+__device__ __forceinline__ void handover_post(unsigned long long *slots, unsigned long long seq,
+                                              int k, unsigned long long v) {
+  const unsigned long long tag = seq << 32;
+  asm volatile("st.volatile.global.v2.u64 [%0], {%1, %2};" ::"l"(slots + 2 * k),
                "l"(tag | (v & 0xffffffffull)), "l"(tag | (v >> 32))
                : "memory");
 }
@@ -226,6 +236,12 @@ struct RoundChannel {
   // throws (and clears it) when it is set.
   unsigned int *err_host = nullptr, *err_dev = nullptr;
   void check_device_error(const char *stage);
+  // A larger tagged area in the same mapped allocation (kHandoverWords words,
+  // one 16-byte slot each as in the mailbox) for a kernel that hands a
+  // sumcheck's last small tables to the host instead of waiting for its
+  // challenges; wait_handover reads publication `seq` of n words.
+  unsigned long long *handover_host = nullptr, *handover_dev = nullptr;
+  void wait_handover(cudaStream_t s, unsigned long long seq, uint64_t *out, int n);
   Publish arm() { return Publish{counter, dev, ++next}; }
   // Waits for the publication armed last; copies n payload words.
   void wait(cudaStream_t s, uint64_t *out, int n);

@@ -14,8 +14,10 @@
 // down to round i's (eq_i[x] = eq_{i+1}[x] + eq_{i+1}[x + 2^i], summing out
 // coordinate i), and accumulates round i's two sums from the freshly bound
 // values; 32 bytes leave the device per round.
+#include <algorithm>
 #include <chrono>
 #include <cstdio>
+#include <vector>
 
 #include "context.hpp"
 #include "eq.cuh"
@@ -454,6 +456,9 @@ __global__ void gkr_final_bind(const f128 *__restrict__ c, size_t n_half, f128 r
 // and sums exactly as gkr_bind_sums / gkr_final_bind, and posts the round's
 // four words to the mailbox (publication seq0 + i0 - i). A missing challenge
 // ends the kernel without a post, which the host reads as a failed round.
+// At iteration i_host (-1: none) the block hands its tables to the host
+// instead and ends: rounds whose tables are that small cost the host about a
+// microsecond each, against a PCIe round trip and a device step per round.
 //
 // A round is a chain of three dependent products per element (the bind,
 // e * L, then * R); with few elements one thread per element leaves the
@@ -470,7 +475,9 @@ __global__ void __launch_bounds__(kTailThreads) gkr_tail(const f128 *__restrict_
                                                          unsigned long long seq0,
                                                          const Mailbox *down,
                                                          unsigned long long dseq0, size_t colmask,
-                                                         size_t live_cols) {
+                                                         size_t live_cols, int i_host,
+                                                         unsigned long long *handover,
+                                                         unsigned long long hseq) {
   __shared__ f128 L[4 * kTailH], R[4 * kTailH], E[2 * kTailH];
   __shared__ uint64_t red[4][kTailThreads / 32];
   __shared__ unsigned long long chal[2];
@@ -483,6 +490,18 @@ __global__ void __launch_bounds__(kTailThreads) gkr_tail(const f128 *__restrict_
   }
   for (int k = threadIdx.x; k < 2 * h0 && i0 > 0; k += blockDim.x) E[k] = ld(eq + k);
   for (int i = i0; i >= 0; i--) {
+    if (i == i_host) {
+      // the layer's last rounds run on the host: the tables as they stand
+      // before r_i's bind (L and R: 4h entries each, then E: 2h) go out as
+      // handover publication hseq, two words per entry, and the block ends
+      const int h = 1 << (i - 1), nl = 4 * h;
+      for (int k = threadIdx.x; k < 2 * nl + 2 * h; k += blockDim.x) {
+        const f128 v = k < nl ? L[k] : k < 2 * nl ? R[k - nl] : E[k - 2 * nl];
+        handover_post(handover, hseq, 2 * k, v.lo);
+        handover_post(handover, hseq, 2 * k + 1, v.hi);
+      }
+      return;
+    }
     if (threadIdx.x == 0) ok = mailbox_wait_device(down, dseq0 + (i0 - i), 2, chal, kTailWaitNs);
     __syncthreads();
     if (!ok) return;
@@ -690,6 +709,48 @@ static void launch_mid(f128 *c, size_t n_half, int n, int i_hi, int i_lo, const 
   BZ_LAUNCH_CHECK();
 }
 
+// The rounds from this iteration down run on the host once gkr_tail has
+// handed over its tables (h <= 2^(kHostTailI - 1) = 16 pairs).
+constexpr int kHostTailI = 5;
+
+// One iteration of gkr_tail on the host, with the same arithmetic: bind the
+// tables (L, R: 4h entries, E: 2h, h = 2^(i-1)) at r and leave the sums of
+// the next round in out, or, at i == 0, the bound pair (lr, rr).
+static void host_tail_round(std::vector<f128> &L, std::vector<f128> &R, std::vector<f128> &E,
+                            int i, f128 r, uint32_t at_one_mask, size_t colmask, size_t live,
+                            f128 out[2]) {
+  if (i == 0) {
+    out[0] = gadd(L[0], gmul(r, gadd(L[1], L[0])));
+    out[1] = gadd(R[0], gmul(r, gadd(R[1], R[0])));
+    return;
+  }
+  const size_t h = (size_t)1 << (i - 1), h2 = 2 * h;
+  const bool at_one = (at_one_mask >> (i - 1)) & 1;
+  for (size_t x = 0; x < h; x++) {
+    E[x] = gadd(E[x], E[x + h]);
+    if ((x & colmask) >= live) continue;  // a padded column stays one
+    for (int q = 0; q < 4; q++) {
+      std::vector<f128> &T = q < 2 ? L : R;
+      const size_t at = x + (q & 1) * h;
+      T[at] = gadd(T[at], gmul(r, gadd(T[at + h2], T[at])));
+    }
+  }
+  f128 s0 = mk(0, 0), s1 = mk(0, 0);
+  for (size_t x = 0; x < h; x++) {
+    const f128 e = E[x];
+    if ((x & colmask) >= live) {  // e * 1 * 1 and e * 0 * 0
+      s0 = gadd(s0, e);
+      continue;
+    }
+    const f128 p = gmul(e, at_one ? L[x + h] : L[x]);
+    const f128 q = gmul(e, gadd(L[x + h], L[x]));
+    s0 = gadd(s0, gmul(p, at_one ? R[x + h] : R[x]));
+    s1 = gadd(s1, gmul(q, gadd(R[x + h], R[x])));
+  }
+  out[0] = s0;
+  out[1] = s1;
+}
+
 f128 gkr_prove(int s, const f128 *zeta, uint32_t grind_bits, Transcript &ts, GkrScratch &sc,
                cudaStream_t st_, f128 *point_out) {
   f128 point[kMaxPoint], next[kMaxPoint];
@@ -738,6 +799,15 @@ f128 gkr_prove(int s, const f128 *zeta, uint32_t grind_bits, Transcript &ts, Gkr
     while (i_tail > 0 && ((size_t)1 << (i_tail - 1)) > (size_t)kTailH) i_tail--;
     const Publish top = arm(sc);
     const unsigned long long p0 = top.seq, d0 = ch ? ch->down_next + 1 : 0;
+    // Queued mode: the tail hands its tables over at iteration i_host and the
+    // host runs the rounds from there down (handover publication hseq).
+    const int i_host =
+        queued && ch->handover_host && i_tail >= 1 ? std::min(kHostTailI, i_tail) : -1;
+    const unsigned long long hseq = p0 + (n - i_host);
+    uint32_t tail_mask = 0;
+    for (int k = 1; k <= i_tail; k++) tail_mask |= (uint32_t)gis_zero(point[k - 1]) << (k - 1);
+    std::vector<f128> HL, HR, HE;
+    f128 host_out[2] = {mk(0, 0), mk(0, 0)};  // sums (or the pair) the host computed
     RoundLink none{nullptr, nullptr, nullptr, 0};
     // Bind round i > i_tail runs in gkr_mid (which reads r_i from the downbox
     // itself) when the lane keeps the middle rounds resident and 2^(i-1) <=
@@ -775,18 +845,24 @@ f128 gkr_prove(int s, const f128 *zeta, uint32_t grind_bits, Transcript &ts, Gkr
                     sc.acc + 4 * (n - i), pub, lk, colmask, live, st_);
       }
       if (i > i_tail) launch_mid(c, n_half, n, i, i_tail + 1, point, sc, p0, d0, colmask, live, st_);
-      uint32_t mask = 0;
-      for (int k = 1; k <= i_tail; k++) mask |= (uint32_t)gis_zero(point[k - 1]) << (k - 1);
-      gkr_tail<<<1, kTailThreads, 0, st_>>>(c, n_half, i_tail, sc.eq, mask, ch->dev,
+      gkr_tail<<<1, kTailThreads, 0, st_>>>(c, n_half, i_tail, sc.eq, tail_mask, ch->dev,
                                             p0 + (n - i_tail), ch->down_dev,
-                                            d0 + (n - 1 - i_tail), colmask, live);
+                                            d0 + (n - 1 - i_tail), colmask, live, i_host,
+                                            ch->handover_dev, hseq);
       BZ_LAUNCH_CHECK();
       tail = true;
     }
     f128 eq_bound = mk(1, 0);
     for (int i = n - 1; i >= 0; i--) {
       unsigned long long *acc = sc.acc + 4 * (n - 1 - i);
-      round_read(sc, acc, st_);
+      if (i_host >= 0 && i < i_host) {  // the host's own round
+        sc.host[0] = host_out[0].lo;
+        sc.host[1] = host_out[0].hi;
+        sc.host[2] = host_out[1].lo;
+        sc.host[3] = host_out[1].hi;
+      } else {
+        round_read(sc, acc, st_);
+      }
       if (trace) {
         const auto now = std::chrono::steady_clock::now();
         fprintf(stderr, "[gkr] layer %d round %2d h %8zu %s %7.2f us\n", j, i, (size_t)1 << i,
@@ -802,7 +878,23 @@ f128 gkr_prove(int s, const f128 *zeta, uint32_t grind_bits, Transcript &ts, Gkr
       next[i] = r;
       eq_bound = gmul(eq_bound, eq_factor(r, point[i]));
       const uint64_t rw[2] = {r.lo, r.hi};
-      if (queued) {
+      if (queued && i_host >= 0 && i <= i_host) {
+        if (i == i_host) {  // the tail's tables, as it stood before binding r_i
+          const int h = 1 << (i - 1), nl = 4 * h;
+          std::vector<uint64_t> w(2 * (2 * nl + 2 * h));
+          ch->wait_handover(st_, hseq, w.data(), (int)w.size());
+          tail = false;  // the tail kernel ends after the handover
+          auto take = [&](std::vector<f128> &v, int at, int cnt) {
+            v.resize(cnt);
+            for (int k = 0; k < cnt; k++) v[k] = mk(w[2 * (at + k)], w[2 * (at + k) + 1]);
+          };
+          take(HL, 0, nl);
+          take(HR, nl, nl);
+          take(HE, 2 * nl, 2 * h);
+        }
+        host_tail_round(HL, HR, HE, i, r, tail_mask, colmask, live, host_out);
+        ch->arm();  // publication numbering as if the device had posted
+      } else if (queued) {
         ch->send(rw, 2);
         ch->arm();
       } else if (i > 0) {
@@ -827,9 +919,14 @@ f128 gkr_prove(int s, const f128 *zeta, uint32_t grind_bits, Transcript &ts, Gkr
       }
     }
     f128 lr[2];
-    round_read(sc, sc.pair, st_);
-    tail = false;  // the tail kernel ends after posting the pair
-    memcpy(lr, sc.host, 32);
+    if (i_host >= 0) {
+      lr[0] = host_out[0];
+      lr[1] = host_out[1];
+    } else {
+      round_read(sc, sc.pair, st_);
+      tail = false;  // the tail kernel ends after posting the pair
+      memcpy(lr, sc.host, 32);
+    }
     ts.prover_message(lr, 32);
     f128 t = ts.challenge_f128();
     next[n] = t;
