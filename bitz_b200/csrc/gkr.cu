@@ -495,6 +495,7 @@ __global__ void __launch_bounds__(kTailThreads) gkr_tail(const f128 *__restrict_
       // before r_i's bind (L and R: 4h entries each, then E: 2h) go out as
       // handover publication hseq, two words per entry, and the block ends
       const int h = 1 << (i - 1), nl = 4 * h;
+      __syncthreads();  // the tables as loaded (a first iteration has no barrier yet)
       for (int k = threadIdx.x; k < 2 * nl + 2 * h; k += blockDim.x) {
         const f128 v = k < nl ? L[k] : k < 2 * nl ? R[k - nl] : E[k - 2 * nl];
         handover_post(handover, hseq, 2 * k, v.lo);
@@ -710,8 +711,8 @@ static void launch_mid(f128 *c, size_t n_half, int n, int i_hi, int i_lo, const 
 }
 
 // The rounds from this iteration down run on the host once gkr_tail has
-// handed over its tables (h <= 2^(kHostTailI - 1) = 16 pairs).
-constexpr int kHostTailI = 5;
+// handed over its tables (h <= 2^(kHostTailI - 1) = 32 pairs).
+constexpr int kHostTailI = 6;
 
 // One iteration of gkr_tail on the host, with the same arithmetic: bind the
 // tables (L, R: 4h entries, E: 2h, h = 2^(i-1)) at r and leave the sums of

@@ -10,6 +10,8 @@
 // sums leave the device as 32 bytes. Round 1 reads the bits directly: its
 // coefficients are XOR sums of weights with no multiplication
 // (lib.rs:189-239).
+#include <vector>
+
 #include "device.cuh"
 #include "context.hpp"
 #include "post_gkr.hpp"
@@ -214,6 +216,37 @@ static f128 advance(f128 claim, f128 a0, f128 a2, f128 r) {
 
 // A round's result words: through the mailbox when the scratch has a
 // channel, else by a copy and a stream sync.
+// The tail hands its tables to the host at the first round whose input is at
+// most this long (the host then folds and sums in a few microseconds a round).
+constexpr size_t kPgHostLen = 64;
+
+// One pg_tail round on the host: fold W and V at r (entry o = t0 + r (t0 +
+// t1)); then the next round's (a0, a2) into sums, or, once one entry is left,
+// the closing pair into pair. Returns true when the pair is formed.
+static bool host_pg_round(std::vector<f128> &W, std::vector<f128> &V, f128 r, f128 sums[2],
+                          f128 pair[2]) {
+  const size_t n = W.size() / 2;
+  for (size_t o = 0; o < n; o++) {
+    W[o] = gadd(W[2 * o], gmul(r, gadd(W[2 * o], W[2 * o + 1])));
+    V[o] = gadd(V[2 * o], gmul(r, gadd(V[2 * o], V[2 * o + 1])));
+  }
+  W.resize(n);
+  V.resize(n);
+  if (n == 1) {
+    pair[0] = W[0];
+    pair[1] = V[0];
+    return true;
+  }
+  f128 a0 = mk(0, 0), a2 = mk(0, 0);
+  for (size_t j = 0; j < n / 2; j++) {
+    a0 = gadd(a0, gmul(W[2 * j], V[2 * j]));
+    a2 = gadd(a2, gmul(gadd(W[2 * j], W[2 * j + 1]), gadd(V[2 * j], V[2 * j + 1])));
+  }
+  sums[0] = a0;
+  sums[1] = a2;
+  return false;
+}
+
 // The last rounds in one resident block, fed through the lane's downbox like
 // the GKR tail: the tables (at most 2 * kPgTailN entries each) sit in shared
 // memory; each round waits (bounded) for the host's challenge, folds both
@@ -225,7 +258,9 @@ constexpr unsigned long long kPgWaitNs = 2000000000ull;
 __global__ void __launch_bounds__(kThreads) pg_tail(const f128 *__restrict__ w_in,
                                                     const f128 *__restrict__ v_in, int len0,
                                                     Mailbox *mb, unsigned long long seq0,
-                                                    const Mailbox *down, unsigned long long dseq0) {
+                                                    const Mailbox *down, unsigned long long dseq0,
+                                                    int hand_round, unsigned long long *handover,
+                                                    unsigned long long hseq) {
   __shared__ f128 W[2 * kPgTailN], V[2 * kPgTailN];
   __shared__ unsigned long long chal[2];
   __shared__ int ok;
@@ -235,6 +270,15 @@ __global__ void __launch_bounds__(kThreads) pg_tail(const f128 *__restrict__ w_i
   }
   int len = len0;
   for (int round = 0; len > 1; round++) {
+    if (round == hand_round) {  // the remaining rounds run on the host: W, then V
+      __syncthreads();
+      for (int k = threadIdx.x; k < 2 * len; k += blockDim.x) {
+        const f128 x = k < len ? W[k] : V[k - len];
+        handover_post(handover, hseq, 2 * k, x.lo);
+        handover_post(handover, hseq, 2 * k + 1, x.hi);
+      }
+      return;
+    }
     if (threadIdx.x == 0) ok = mailbox_wait_device(down, dseq0 + round, 2, chal, kPgWaitNs);
     __syncthreads();
     if (!ok) return;
@@ -479,6 +523,10 @@ int post_gkr_prove(const PostGkrArgs &a, Transcript &ts, PostGkrScratch &sc, cud
   const bool queued = ch && resident && sc.ctl && rounds >= 1;
   int t0 = 0;  // the loop iteration at which the tail takes over
   while (t0 < rounds && (n1 >> t0) > (size_t)2 * kPgTailN) t0++;
+  int kh = -1;                   // queued: the host runs iterations kh .. rounds-1
+  unsigned long long hseq = 0;   // the tail's handover publication
+  bool host_fin = false;         // the closing pair came from the host's rounds
+  f128 fin_host[2] = {mk(0, 0), mk(0, 0)};
   // no other thread's device allocation while a round kernel waits for this one
   ResidentScope gate(ch && resident);
   try {
@@ -520,15 +568,29 @@ int post_gkr_prove(const PostGkrArgs &a, Transcript &ts, PostGkrScratch &sc, cud
           cur_set = (km + 1) % 2;
         }
         f128 *const *cur = set[cur_set];
+        // iterations kh .. rounds-1 on the host, from the tail's handover
+        for (int k = t0; k < rounds && kh < 0 && ch->handover_host; k++)
+          if ((n1 >> k) <= kPgHostLen) kh = k;
+        hseq = p0 + (kh >= 0 ? kh : 0) + 1;
         pg_tail<<<1, kThreads, 0, s>>>(cur[0], cur[1], (int)(n1 >> t0), ch->dev, p0 + t0 + 1,
-                                       ch->down_dev, d0 + t0);
+                                       ch->down_dev, d0 + t0, kh >= 0 ? kh - t0 : -1,
+                                       ch->handover_dev, hseq);
         BZ_LAUNCH_CHECK();
       }
     }
   }
   if (queued) {
+    std::vector<f128> HW, HV;
+    f128 hsums[2];
     for (int k = 0; k < rounds; k++) {
-      round_read(sc, nullptr, 4, s);
+      if (kh >= 0 && k > kh) {  // the host's own round
+        sc.host[0] = hsums[0].lo;
+        sc.host[1] = hsums[0].hi;
+        sc.host[2] = hsums[1].lo;
+        sc.host[3] = hsums[1].hi;
+      } else {
+        round_read(sc, nullptr, 4, s);
+      }
       f128 m0 = mk(sc.host[0], sc.host[1]), m2 = mk(sc.host[2], sc.host[3]);
       uint64_t mm[4] = {m0.lo, m0.hi, m2.lo, m2.hi};
       ts.prover_message(mm, 32);
@@ -536,6 +598,23 @@ int post_gkr_prove(const PostGkrArgs &a, Transcript &ts, PostGkrScratch &sc, cud
       f128 rr = ts.challenge_f128();
       claim = advance(claim, m0, m2, rr);
       point_out[1 + k] = rr;
+      if (kh >= 0 && k >= kh) {
+        if (k == kh) {  // the tail's W and V as they stood before folding at rr
+          const size_t len = n1 >> k;
+          std::vector<uint64_t> words(4 * len);
+          ch->wait_handover(s, hseq, words.data(), (int)words.size());
+          tail = false;  // the tail kernel ends after the handover
+          HW.resize(len);
+          HV.resize(len);
+          for (size_t i = 0; i < len; i++) {
+            HW[i] = mk(words[2 * i], words[2 * i + 1]);
+            HV[i] = mk(words[2 * (len + i)], words[2 * (len + i) + 1]);
+          }
+        }
+        host_fin = host_pg_round(HW, HV, rr, hsums, fin_host);
+        ch->arm();  // publication numbering as if the device had posted
+        continue;
+      }
       const uint64_t rw[2] = {rr.lo, rr.hi};
       ch->send(rw, 2);
       ch->arm();
@@ -553,7 +632,7 @@ int post_gkr_prove(const PostGkrArgs &a, Transcript &ts, PostGkrScratch &sc, cud
     point_out[1 + k] = rr;
     if (!tail && ch && resident && len <= (size_t)2 * kPgTailN) {
       pg_tail<<<1, kThreads, 0, s>>>(w, v, (int)len, ch->dev, ch->next + 1, ch->down_dev,
-                                     ch->down_next + 1);
+                                     ch->down_next + 1, -1, nullptr, 0);
       BZ_LAUNCH_CHECK();
       tail = true;
     }
@@ -593,7 +672,10 @@ int post_gkr_prove(const PostGkrArgs &a, Transcript &ts, PostGkrScratch &sc, cud
     throw;
   }
   f128 fin[2];
-  if (tail) {
+  if (host_fin) {
+    fin[0] = fin_host[0];
+    fin[1] = fin_host[1];
+  } else if (tail) {
     // the tail's last publication is the closing pair
     ch->wait(s, sc.host, 4);
     fin[0] = mk(sc.host[0], sc.host[1]);

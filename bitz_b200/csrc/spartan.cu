@@ -84,13 +84,13 @@ __global__ void k_products_to_fp(const int64_t *__restrict__ prod, size_t rows, 
   }
 }
 
-__device__ __forceinline__ fp interp(fp a, fp b, fp r, const FpCtx &c) {
+BZ_HD fp interp(fp a, fp b, fp r, const FpCtx &c) {
   return fp_add(a, fp_mul(r, fp_sub(b, a, c), c), c);
 }
 
 // cubic_contribution (sumcheck.rs:724-746): [e0 r0, e0 rq + ed rl, ed rq]
-__device__ __forceinline__ void cubic(fp e0, fp e1, fp a0, fp a1, fp b0, fp b1, fp c0, fp c1,
-                                      const FpCtx &c, fp (&acc)[3]) {
+BZ_HD void cubic(fp e0, fp e1, fp a0, fp a1, fp b0, fp b1, fp c0, fp c1, const FpCtx &c,
+                 fp (&acc)[3]) {
   fp ed = fp_sub(e1, e0, c), ad = fp_sub(a1, a0, c), bd = fp_sub(b1, b0, c), cd = fp_sub(c1, c0, c);
   fp r0 = fp_sub(fp_mul(a0, b0, c), c0, c);
   fp rl = fp_sub(fp_add(fp_mul(a0, bd, c), fp_mul(ad, b0, c), c), cd, c);
@@ -374,6 +374,19 @@ __device__ __forceinline__ bool sp_challenge(const Mailbox *down, unsigned long 
   return good;
 }
 
+// The T tables (len entries each, one after another) as handover
+// publication seq: the host runs the sumcheck's remaining rounds.
+template <int T>
+__device__ __forceinline__ void sp_handover(fp (*tab)[kSpTailN], int len,
+                                            unsigned long long *handover,
+                                            unsigned long long seq) {
+  for (int k = threadIdx.x; k < T * len; k += blockDim.x) {
+    const fp v = tab[k / len][k % len];
+    handover_post(handover, seq, 2 * k, v.lo);
+    handover_post(handover, seq, 2 * k + 1, v.hi);
+  }
+}
+
 template <int N>
 __device__ __forceinline__ void sp_post(fp (&acc)[N], const FpCtx &c, Mailbox *mb,
                                         unsigned long long seq) {
@@ -393,7 +406,10 @@ __global__ void __launch_bounds__(kThreads) sp_outer_tail(const fp *E, const fp 
                                                           int nrounds, FpCtx c, Mailbox *mb,
                                                           unsigned long long seq0,
                                                           const Mailbox *down,
-                                                          unsigned long long dseq0) {
+                                                          unsigned long long dseq0,
+                                                          int hand_round,
+                                                          unsigned long long *handover,
+                                                          unsigned long long hseq) {
   __shared__ fp tab[4][kSpTailN];
   for (int k = threadIdx.x; k < len0; k += blockDim.x) {
     tab[0][k] = E[k];
@@ -404,6 +420,10 @@ __global__ void __launch_bounds__(kThreads) sp_outer_tail(const fp *E, const fp 
   __syncthreads();
   int len = len0, nd = 0, np = 0;
   for (int round = 0; round < nrounds; round++) {
+    if (round == hand_round) {  // the remaining rounds run on the host
+      sp_handover<4>(tab, len, handover, hseq);
+      return;
+    }
     if (round > 0 || fold0) {
       fp r;
       if (!sp_challenge(down, dseq0 + nd++, c, r)) return;
@@ -432,7 +452,10 @@ __global__ void __launch_bounds__(kThreads) sp_inner_tail(const fp *D, const fp 
                                                           FpCtx c, Mailbox *mb,
                                                           unsigned long long seq0,
                                                           const Mailbox *down,
-                                                          unsigned long long dseq0) {
+                                                          unsigned long long dseq0,
+                                                          int hand_round,
+                                                          unsigned long long *handover,
+                                                          unsigned long long hseq) {
   __shared__ fp tab[2][kSpTailN];
   for (int k = threadIdx.x; k < len0; k += blockDim.x) {
     tab[0][k] = D[k];
@@ -441,6 +464,10 @@ __global__ void __launch_bounds__(kThreads) sp_inner_tail(const fp *D, const fp 
   __syncthreads();
   int len = len0, nd = 0, np = 0;
   for (int round = 0; round < nrounds; round++) {
+    if (round == hand_round) {  // the remaining rounds run on the host
+      sp_handover<2>(tab, len, handover, hseq);
+      return;
+    }
     if (round > 0 || fold0) {
       fp r;
       if (!sp_challenge(down, dseq0 + nd++, c, r)) return;
@@ -466,6 +493,63 @@ __global__ void __launch_bounds__(kThreads) sp_inner_tail(const fp *D, const fp 
 }
 
 // ------------------------------------------------------------------- host
+
+// The tail hands its tables to the host at the first round whose input is at
+// most this long; each round after that costs the host a few microseconds,
+// against a PCIe round trip and a device step.
+constexpr size_t kSpHostLen = 64;
+
+// The first round (at or after the tail's first, t0) whose input of
+// n0 >> (k - 1) entries (n0 at k = 0) is at most kSpHostLen; -1 without a
+// handover area or a round that small.
+static int sp_host_round(const RoundChannel *ch, size_t n0, int t0, int nrounds) {
+  if (!ch->handover_host) return -1;
+  for (int k = t0; k < nrounds; k++)
+    if ((k == 0 ? n0 : n0 >> (k - 1)) <= kSpHostLen) return k;
+  return -1;
+}
+
+// The handover's T tables of len entries each.
+static void sp_take_handover(RoundChannel *ch, cudaStream_t s, unsigned long long seq, int T,
+                             size_t len, std::vector<fp> *tab) {
+  std::vector<uint64_t> w(2 * T * len);
+  ch->wait_handover(s, seq, w.data(), (int)w.size());
+  for (int t = 0; t < T; t++) {
+    tab[t].resize(len);
+    for (size_t k = 0; k < len; k++)
+      tab[t][k] = fp{w[2 * (t * len + k)], w[2 * (t * len + k) + 1]};
+  }
+}
+
+// sp_fold on the host: each table folded at r in place (entry o from 2o and
+// 2o + 1, read before it is overwritten).
+static void host_sp_fold(std::vector<fp> *tab, int T, fp r, const FpCtx &c) {
+  for (int t = 0; t < T; t++) {
+    const size_t n = tab[t].size() / 2;
+    for (size_t o = 0; o < n; o++) tab[t][o] = interp(tab[t][2 * o], tab[t][2 * o + 1], r, c);
+    tab[t].resize(n);
+  }
+}
+
+// The outer and inner rounds' sums, as the tail kernels form them.
+static void host_outer_sums(const std::vector<fp> *tab, const FpCtx &c, fp *out) {
+  fp acc[3] = {fp_zero(), fp_zero(), fp_zero()};
+  for (size_t j = 0; j < tab[0].size() / 2; j++)
+    cubic(tab[0][2 * j], tab[0][2 * j + 1], tab[1][2 * j], tab[1][2 * j + 1], tab[2][2 * j],
+          tab[2][2 * j + 1], tab[3][2 * j], tab[3][2 * j + 1], c, acc);
+  for (int k = 0; k < 3; k++) out[k] = acc[k];
+}
+
+static void host_inner_sums(const std::vector<fp> *tab, const FpCtx &c, fp *out) {
+  fp acc[2] = {fp_zero(), fp_zero()};
+  for (size_t j = 0; j < tab[0].size() / 2; j++) {
+    const fp d0 = tab[0][2 * j], d1 = tab[0][2 * j + 1], w0 = tab[1][2 * j], w1 = tab[1][2 * j + 1];
+    acc[0] = fp_add(acc[0], fp_mul(d0, w0, c), c);
+    acc[1] = fp_add(acc[1], fp_mul(fp_sub(d1, d0, c), fp_sub(w1, w0, c), c), c);
+  }
+  out[0] = acc[0];
+  out[1] = acc[1];
+}
 
 static fp host_partial_sum(const fp *d_partial, int nblocks, int N, fp *d_out, fp *h_out,
                            const FpCtx &c, cudaStream_t s, RoundChannel *ch) {
@@ -743,35 +827,57 @@ void spartan_prove(const SpartanArgs &a, Transcript &ts, SpartanScratch &sc, cud
                           n_in, km, t0, c, sc, p0, d0, s);
       cur_set = 1 - si;
     }
+    // rounds kh .. nr-1 on the host, from the tail's handover
+    const int kh = sp_host_round(ch, R, t0, nr);
+    const unsigned long long hseq = p0 + (kh >= 0 ? kh : 0);
+    std::vector<fp> host_tab[4];
     {
       fp *const *cur = set[cur_set];
       const size_t n = t0 == 0 ? R : R >> (t0 - 1);
       sp_outer_tail<<<1, kThreads, 0, s>>>(cur[0], cur[1], cur[2], cur[3], (int)n, t0 > 0,
                                            nr - t0, c, ch->dev, p0 + t0, ch->down_dev,
-                                           d0 + (t0 > 0 ? t0 - 1 : 0));
+                                           d0 + (t0 > 0 ? t0 - 1 : 0), kh >= 0 ? kh - t0 : -1,
+                                           ch->handover_dev, hseq);
       BZ_LAUNCH_CHECK();
       tail = true;
     }
     for (int round = 0; round < nr; round++) {
-      if (round > 0) send_r(r);
-      ch->arm();
-      ch->wait(s, reinterpret_cast<uint64_t *>(sc.host), 6);
+      if (kh >= 0 && round >= kh) {
+        if (round == kh) {
+          sp_take_handover(ch, s, hseq, 4, round == 0 ? R : R >> (round - 1), host_tab);
+          tail = false;  // the tail kernel ends after the handover
+        }
+        if (round > 0) host_sp_fold(host_tab, 4, r, c);
+        host_outer_sums(host_tab, c, sc.host);
+        ch->arm();  // publication numbering as if the device had posted
+      } else {
+        if (round > 0) send_r(r);
+        ch->arm();
+        ch->wait(s, reinterpret_cast<uint64_t *>(sc.host), 6);
+      }
       trace_round("outer", round, round < t0);
       fp co[4];
       r = round_message(ts, c, claim, sc.host, 4, a.q, co);
       for (int i = 0; i < 4; i++) out.outer[4 * round + i] = co[i];
       out.rx[round] = r;
     }
-    // the tail's last publication: the single entries of A, B and C
-    send_r(r);
-    ch->arm();
-    ch->wait(s, reinterpret_cast<uint64_t *>(fin), 6);
+    if (kh >= 0) {  // the last fold leaves one entry per table
+      host_sp_fold(host_tab, 4, r, c);
+      for (int k = 0; k < 3; k++) fin[k] = host_tab[k + 1][0];
+      ch->arm();
+    } else {
+      // the tail's last publication: the single entries of A, B and C
+      send_r(r);
+      ch->arm();
+      ch->wait(s, reinterpret_cast<uint64_t *>(fin), 6);
+    }
   } else {
   for (int round = 0; round < nr; round++) {
     int fold = round > 0;
     if (!tail && ch && resident && len <= (size_t)kSpTailN) {
       sp_outer_tail<<<1, kThreads, 0, s>>>(E, A, B, C, (int)len, fold, nr - round, c, ch->dev,
-                                           ch->next + 1, ch->down_dev, ch->down_next + 1);
+                                           ch->next + 1, ch->down_dev, ch->down_next + 1, -1,
+                                           nullptr, 0);
       BZ_LAUNCH_CHECK();
       tail = true;
     }
@@ -903,35 +1009,57 @@ void spartan_prove(const SpartanArgs &a, Transcript &ts, SpartanScratch &sc, cud
                           Cn >> (km - 1), km, t0, c, sc, p0, d0, s);
       cur_set = 1 - si;
     }
+    // rounds kh .. nc-1 on the host, from the tail's handover
+    const int kh = sp_host_round(ch, Cn, t0, nc);
+    const unsigned long long hseq = p0 + (kh >= 0 ? kh : 0);
+    std::vector<fp> host_tab[2];
     {
       fp *const *cur = set[cur_set];
       const size_t n = t0 == 0 ? Cn : Cn >> (t0 - 1);
       sp_inner_tail<<<1, kThreads, 0, s>>>(cur[0], cur[1], a.hbits, t0 <= 1 ? 1 : 0, (int)n,
                                            t0 > 0, nc - t0, c, ch->dev, p0 + t0, ch->down_dev,
-                                           d0 + (t0 > 0 ? t0 - 1 : 0));
+                                           d0 + (t0 > 0 ? t0 - 1 : 0), kh >= 0 ? kh - t0 : -1,
+                                           ch->handover_dev, hseq);
       BZ_LAUNCH_CHECK();
       tail = true;
     }
     for (int round = 0; round < nc; round++) {
-      if (round > 0) send_r(r);
-      ch->arm();
-      ch->wait(s, reinterpret_cast<uint64_t *>(sc.host), 4);
+      if (kh >= 0 && round >= kh) {
+        if (round == kh) {
+          sp_take_handover(ch, s, hseq, 2, round == 0 ? Cn : Cn >> (round - 1), host_tab);
+          tail = false;  // the tail kernel ends after the handover
+        }
+        if (round > 0) host_sp_fold(host_tab, 2, r, c);
+        host_inner_sums(host_tab, c, sc.host);
+        ch->arm();  // publication numbering as if the device had posted
+      } else {
+        if (round > 0) send_r(r);
+        ch->arm();
+        ch->wait(s, reinterpret_cast<uint64_t *>(sc.host), 4);
+      }
       trace_round("inner", round, round < t0);
       fp co[3];
       r = round_message(ts, c, claim, sc.host, 3, a.q, co);
       for (int i = 0; i < 3; i++) out.inner[3 * round + i] = co[i];
       out.ry[round] = r;
     }
-    send_r(r);
-    ch->arm();
-    ch->wait(s, reinterpret_cast<uint64_t *>(dw), 4);
+    if (kh >= 0) {  // the last fold leaves one entry per table
+      host_sp_fold(host_tab, 2, r, c);
+      dw[0] = host_tab[0][0];
+      dw[1] = host_tab[1][0];
+      ch->arm();
+    } else {
+      send_r(r);
+      ch->arm();
+      ch->wait(s, reinterpret_cast<uint64_t *>(dw), 4);
+    }
   } else {
   for (int round = 0; round < nc; round++) {
     int fold = round > 0;
     if (!tail && ch && resident && len <= (size_t)kSpTailN) {
       sp_inner_tail<<<1, kThreads, 0, s>>>(D, W, a.hbits, w_bits, (int)len, fold, nc - round, c,
                                            ch->dev, ch->next + 1, ch->down_dev,
-                                           ch->down_next + 1);
+                                           ch->down_next + 1, -1, nullptr, 0);
       BZ_LAUNCH_CHECK();
       tail = true;
     }
