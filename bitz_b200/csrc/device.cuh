@@ -56,7 +56,7 @@ inline int grid_for(size_t work, int per_block = kThreads, int max_blocks = kSMs
 // so the host accepts the result once every slot shows the current tag, and
 // the device needs no system-scope fence to order data before a flag.
 constexpr int kMailboxWords = 8;  // 64-bit data words per publication
-constexpr int kHandoverWords = 1024;  // 64-bit data words of a handover
+constexpr int kHandoverWords = 1280;  // 64-bit data words of a handover
 struct Mailbox {
   unsigned long long slot[2 * kMailboxWords];
 };

@@ -106,7 +106,11 @@ inline bool host_has_pclmul() {
 BZ_HD wide gmul_wide_portable(f128 a, f128 b);
 BZ_HD wide gmul_wide(f128 a, f128 b) {
 #if !defined(__CUDA_ARCH__)
+#if defined(__PCLMUL__) && defined(__SSE4_1__)
+  return gmul_wide_pclmul(a, b);  // compiled for it: no run-time check, inlined
+#else
   if (host_has_pclmul()) return gmul_wide_pclmul(a, b);
+#endif
 #endif
   return gmul_wide_portable(a, b);
 }

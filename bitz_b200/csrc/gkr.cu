@@ -711,8 +711,8 @@ static void launch_mid(f128 *c, size_t n_half, int n, int i_hi, int i_lo, const 
 }
 
 // The rounds from this iteration down run on the host once gkr_tail has
-// handed over its tables (h <= 2^(kHostTailI - 1) = 32 pairs).
-constexpr int kHostTailI = 6;
+// handed over its tables (h <= 2^(kHostTailI - 1) = 64 pairs).
+constexpr int kHostTailI = 7;
 
 // One iteration of gkr_tail on the host, with the same arithmetic: bind the
 // tables (L, R: 4h entries, E: 2h, h = 2^(i-1)) at r and leave the sums of
