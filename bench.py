@@ -65,8 +65,10 @@ def parse():
     p.add_argument("--no-batch", action="store_true")
     p.add_argument("--serve", action="store_true")
     p.add_argument("--serve-requests", type=int, default=96)
-    p.add_argument("--serving-requests", type=int, default=32,
+    p.add_argument("--serving-requests", type=int, default=96,
                    help="requests in the default line's serving sweep")
+    p.add_argument("--serving-rates", type=int, default=10,
+                   help="arrival rates at most in the default line's serving sweep")
     p.add_argument("--no-large", action="store_true")
     p.add_argument("--no-serving", action="store_true")
     return p.parse_args()
@@ -570,7 +572,7 @@ def ours(args):
     if world == 1 and not args.no_large:
         big = large(args, bz)
     if world == 1 and not args.no_serving:
-        serving = serve_sweep(args, bz, args.serving_requests, 6)
+        serving = serve_sweep(args, bz, args.serving_requests, args.serving_rates)
     line = None
     if rank == 0:
         line = {
