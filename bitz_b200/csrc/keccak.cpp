@@ -193,7 +193,15 @@ __attribute__((target("avx512f,avx512vl"))) static void keccak_vl(uint64_t st[25
   VL_LANES(VL_DECL)
   size_t b = 0;
   do {
-    for (int round = 0; round < 24; round++) KECCAK_ROUND_VL(KRC[round]);
+    // the 24 rounds written out: no loop-carried register shuffling between them
+    KECCAK_ROUND_VL(KRC[0]) KECCAK_ROUND_VL(KRC[1]) KECCAK_ROUND_VL(KRC[2])
+    KECCAK_ROUND_VL(KRC[3]) KECCAK_ROUND_VL(KRC[4]) KECCAK_ROUND_VL(KRC[5])
+    KECCAK_ROUND_VL(KRC[6]) KECCAK_ROUND_VL(KRC[7]) KECCAK_ROUND_VL(KRC[8])
+    KECCAK_ROUND_VL(KRC[9]) KECCAK_ROUND_VL(KRC[10]) KECCAK_ROUND_VL(KRC[11])
+    KECCAK_ROUND_VL(KRC[12]) KECCAK_ROUND_VL(KRC[13]) KECCAK_ROUND_VL(KRC[14])
+    KECCAK_ROUND_VL(KRC[15]) KECCAK_ROUND_VL(KRC[16]) KECCAK_ROUND_VL(KRC[17])
+    KECCAK_ROUND_VL(KRC[18]) KECCAK_ROUND_VL(KRC[19]) KECCAK_ROUND_VL(KRC[20])
+    KECCAK_ROUND_VL(KRC[21]) KECCAK_ROUND_VL(KRC[22]) KECCAK_ROUND_VL(KRC[23])
     if (nblocks) {
       VL_RATE_LANES(VL_XOR_IN)
       in += Transcript::RATE;
